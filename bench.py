@@ -1,0 +1,354 @@
+#!/usr/bin/env python
+"""E+F+stress throughput of the FourierD3 dispersion path on B200.
+
+Workload: the seeded 648-atom SiO2 box (216 Si + 432 O, L = 21.4 A) replicated 6x6x6 with
+N(0, 0.05 A) jitter = 139,968 atoms; PBE-BJ, CN cutoff 6 A, SPME order 5, mesh spacing
+1.2 A (256^3 mesh), default c6tol. One step = device cell-list neighbour search + CN + C6
+factors + spread + FFT + filter + inverse FFT + gather + CN adjoint: energy, forces and
+stress all produced. Synthetic inputs; the C6^ref table is the seeded synthetic stand-in
+unless FD3_C6REF points at the real file.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl fd3|reference]
+
+With N > 1 (torchrun, one rank per GPU) each rank runs an independent replica of the box
+(the path does not shard a single box): value = N * atoms / max-over-ranks step time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+import torch
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "E+F+stress atoms/s, 140k-atom SiO2: mixed/batched vs plain FP64, same B200"
+WORKLOAD = "sio2_139968_spme_p5_h1.2_E+F+stress"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="fd3", choices=["fd3", "reference"])
+    ap.add_argument("--reps", type=int, default=6)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return ws, rank, local
+
+
+def barrier(ws):
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(x: float, ws: int, device) -> float:
+    if ws == 1:
+        return x
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [v.strip() for v in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx.append(float(f[2]))
+                except ValueError:
+                    continue
+                for k, v in zip(names, f[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(k)
+        except Exception:
+            pass
+        finally:
+            try:
+                os.remove(self.path)
+            except Exception:
+                pass
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(max(mx)), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def stage_bytes(stage: str, n: int, mesh, C: int, R: int, b: int) -> float:
+    """Algorithmic HBM bytes of one launch of a pipeline stage (Roofline)."""
+    M = mesh[0] * mesh[1] * mesh[2]
+    Mh = mesh[0] * mesh[1] * (mesh[2] // 2 + 1)
+    if stage == "spread":
+        return C * M * b + n * (24 + 4 + 8 * R)
+    if stage == "filter":
+        return 2 * C * Mh * 2 * b + Mh * 4
+    if stage == "gather":
+        return C * M * b + n * (24 + 4 + 16 * R + 8 + 24)
+    if stage in ("fft_r2c", "fft_c2r"):
+        return C * M * b + C * Mh * 2 * b
+    if stage == "cn_c6":
+        return n * (32 + 16 + 8 + 16 * R)
+    if stage == "cn_adjoint":
+        return n * (32 + 16 + 8 + 24 + 24)
+    if stage == "cell_list":
+        return n * (24 + 4 + 16 + 32 + 16 + 4 * 4)
+    return 0.0
+
+
+def cpu_baseline_port(threads: int, reps: int = 2):
+    """The oracle (CPU float64 restatement of the reference) on a bounded sample."""
+    from fourierd3_b200 import structures as st
+    from oracle.reference_port import OracleFourierD3
+
+    torch.set_num_threads(threads)
+    p, c, z = st.sio2_scaled(reps)
+    o = OracleFourierD3(z, c, method="spme", mesh_spacing=1.2, interpolation_nodes=5, c6tol=1.0, r_cut=6.0)
+    o.calculate(p, c)                      # warm-up (decomposition cache, allocator)
+    t0 = time.perf_counter()
+    o.calculate(p, c)
+    dt = time.perf_counter() - t0
+    return len(z) / dt, dt, len(z)
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    from fourierd3_b200 import structures as st
+    from oracle.reference_port import OracleFourierD3
+
+    torch.set_num_threads(threads)
+    p, c, z = st.sio2_scaled(2)
+    o = OracleFourierD3(z, c, method="spme", mesh_spacing=1.2, interpolation_nodes=5, c6tol=1.0, r_cut=6.0)
+    for _ in range(args.warmup):
+        o.calculate(p, c)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.calculate(p, c)
+    dt = (time.perf_counter() - t0) / args.steps
+    val = len(z) / dt
+    sample = f"one E+F+stress evaluation per step of the 5,184-atom 2x2x2 replica of the same SiO2 box (128^3 mesh)"
+    line = {
+        "metric": METRIC, "value": val, "unit": "atoms/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": WORKLOAD, "sample": sample, "method": "spme", "order": 5},
+        "cpu_baseline": {"value": val, "unit": "atoms/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": val, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def time_steps(fn, steps, warmup, ws, device):
+    for _ in range(warmup):
+        fn()
+    barrier(ws)
+    torch.cuda.synchronize(device)
+    s = torch.cuda.Event(enable_timing=True)
+    e = torch.cuda.Event(enable_timing=True)
+    s.record()
+    for _ in range(steps):
+        fn()
+    e.record()
+    torch.cuda.synchronize(device)
+    barrier(ws)
+    return s.elapsed_time(e) / steps
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+    from fourierd3_b200 import _native, tables, structures as st
+    from fourierd3_b200.functional import D3Model
+
+    device = torch.device("cuda", local)
+    pos, cell, nums = st.sio2_scaled(args.reps)
+    n = len(nums)
+    models = {prec: D3Model(nums, cell, precision=prec, device=device, method="spme", mesh_spacing=1.2,
+                            interpolation_nodes=5, c6tol=1.0, r_cut=6.0) for prec in ("mixed", "fp64")}
+    mesh = models["mixed"].mesh
+    R = models["mixed"].setup.n_rank
+    S = models["mixed"].setup.n_species
+    C = S * R
+    pos_dev = torch.tensor(pos, dtype=torch.float64, device=device)
+    cell_dev = torch.tensor(cell, dtype=torch.float64, device=device)
+    outs = {k: (torch.empty((), dtype=torch.float64, device=device),
+                torch.empty((n, 3), dtype=torch.float64, device=device),
+                torch.empty((3, 3), dtype=torch.float64, device=device)) for k in models}
+
+    def step(prec):
+        models[prec].engine.energy_forces_stress(pos_dev, cell, 6.0, cell_dev=cell_dev, out=outs[prec])
+
+    res = {}
+    clocks = None
+    for prec in ("fp64", "mixed"):
+        if prec == "mixed":
+            with ClockSampler(torch.cuda.current_device()) as cs:
+                l0 = _native.launch_count()
+                ms = time_steps(lambda: step(prec), args.steps, args.warmup, ws, device)
+                launches = (_native.launch_count() - l0) // (args.steps + args.warmup)
+            clocks = cs.summary()
+        else:
+            ms = time_steps(lambda: step(prec), args.steps, args.warmup, ws, device)
+        ms = max_over_ranks(ms, ws, device)
+        res[prec] = ms
+
+    # per-stage CUDA-event times on the launching stream (separate, profiled steps)
+    stages = {}
+    for prec in ("mixed", "fp64"):
+        eng = models[prec].engine
+        eng.profile(True)
+        acc: dict = {}
+        nprof = max(3, min(args.steps, 10))
+        for _ in range(nprof):
+            step(prec)
+            for k, v in eng.stage_times().items():
+                acc[k] = acc.get(k, 0.0) + v / nprof
+        eng.profile(False)
+        stages[prec] = acc
+
+    # end-to-end through the public API with host buffers (H2D positions, D2H E/F/stress)
+    pos_h = torch.tensor(pos, dtype=torch.float64).pin_memory()
+    e_h = torch.empty((), dtype=torch.float64).pin_memory()
+    f_h = torch.empty((n, 3), dtype=torch.float64).pin_memory()
+    s_h = torch.empty((3, 3), dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        pd = pos_h.to(device, non_blocking=True)
+        e, f, s = models["mixed"](pd, cell, out=outs["mixed"])
+        e_h.copy_(e, non_blocking=True)
+        f_h.copy_(f, non_blocking=True)
+        s_h.copy_(s, non_blocking=True)
+
+    e2e_ms = max_over_ranks(time_steps(e2e_step, args.steps, args.warmup, ws, device), ws, device)
+
+    b = 4
+    st_mixed = stages["mixed"]
+    ours = {k: v for k, v in st_mixed.items() if not k.startswith("fft")}
+    dom = max(ours, key=ours.get)
+    peak, peak_kind = measured_peaks()
+    dom_bytes = stage_bytes(dom, n, mesh, C, R, b if dom in ("spread", "filter", "gather") else 8)
+    achieved = dom_bytes / (ours[dom] * 1e-3) / 1e9
+    roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+            "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+            "bytes_per_launch": dom_bytes, "ms_per_launch": ours[dom]}
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        v, dt, natoms = cpu_baseline_port(threads)
+        cpu = {"value": v, "unit": "atoms/s", "cores": threads, "kind": "port",
+               "sample": f"oracle (CPU float64 restatement) one E+F+stress of the {natoms}-atom 2x2x2 replica, "
+                         f"{dt:.1f} s"}
+
+    ms = res["mixed"]
+    line = {
+        "metric": METRIC, "value": ws * n / (ms * 1e-3), "unit": "atoms/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32-mesh+f64-accum", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "n_atoms": n, "mesh": list(mesh), "method": "spme", "order": 5,
+                   "species": S, "c6_rank": R, "precision": "mixed", "parallelism": f"replicas{ws}",
+                   "l2": "inputs larger than L2 (mesh channels %.2f GB)" % (C * mesh[0] * mesh[1] * mesh[2] * 4 / 1e9),
+                   "c6_source": tables.c6_source()},
+        "plain_fp64": {"value": ws * n / (res["fp64"] * 1e-3), "ms_per_step": res["fp64"],
+                       "stages_ms": stages["fp64"]},
+        "mixed_over_fp64": res["fp64"] / ms,
+        "stages_ms": stages["mixed"],
+        "roofline": roof,
+        "cpu_baseline": cpu,
+        "e2e": {"value": ws * n / (e2e_ms * 1e-3), "unit": "atoms/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": n * 3 * 8, "d2h_bytes_per_step": 8 + n * 3 * 8 + 9 * 8},
+        "gpu_launches": int(launches) * args.steps,
+        "clocks": clocks,
+    }
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,558 @@
+// C ABI of libfd3: plan setup (host), workspace layout and the stream-ordered pipelines.
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <atomic>
+#include <new>
+
+#include "fd3_internal.h"
+
+using namespace fd3;
+
+struct fd3_plan {
+  int S = 0, R = 0, method = 0, P = 0, precision = 0;
+  MeshGeom mg{};
+  int ens[3] = {0, 0, 0};
+  Tables h_tab{};
+  Tables* d_tab = nullptr;
+  double* d_eigvecs = nullptr;
+  GreenPair* d_green = nullptr;
+  float* d_deconv = nullptr;
+  cufftHandle fwd = 0, inv = 0;
+  bool has_fft = false;
+  size_t fft_ws = 0;
+  // optional per-stage CUDA-event timing (fd3_profile_enable / fd3_profile_read)
+  static constexpr int kMaxMarks = 24;
+  bool prof = false;
+  cudaEvent_t ev[kMaxMarks] = {};
+  const char* mark_name[kMaxMarks] = {};
+  int n_marks = 0;
+};
+
+// Record a stage boundary on the launching stream when profiling is on.
+static void prof_begin(fd3_plan* p, cudaStream_t s) {
+  p->n_marks = 0;
+  if (!p->prof) return;
+  cudaEventRecord(p->ev[0], s);
+  p->mark_name[0] = "start";
+  p->n_marks = 1;
+}
+static void prof_mark(fd3_plan* p, cudaStream_t s, const char* name) {
+  if (!p->prof || p->n_marks >= fd3_plan::kMaxMarks) return;
+  cudaEventRecord(p->ev[p->n_marks], s);
+  p->mark_name[p->n_marks++] = name;
+}
+
+// ------------------------------------------------------------------ errors / counters
+namespace fd3 {
+static thread_local char g_err[512] = "";
+void set_error(const char* where, const char* what) { snprintf(g_err, sizeof(g_err), "%s: %s", where, what); }
+static std::atomic<int64_t> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+}  // namespace fd3
+
+extern "C" const char* fd3_last_error(void) { return g_err; }
+extern "C" int64_t fd3_launch_count(void) { return g_launches.load(); }
+
+#define FD3_CUFFT(call)                                       \
+  do {                                                        \
+    cufftResult r_ = (call);                                  \
+    if (r_ != CUFFT_SUCCESS) {                                \
+      char b_[64];                                            \
+      snprintf(b_, sizeof(b_), "cufft status %d", (int)r_);   \
+      set_error(#call, b_);                                   \
+      return FD3_ECUFFT;                                      \
+    }                                                         \
+  } while (0)
+#define FD3_TRY(x)          \
+  do {                      \
+    int rc_ = (x);          \
+    if (rc_) return rc_;    \
+  } while (0)
+
+// ------------------------------------------------------------------ plan
+static int largest_divisor_le(int n, int cap) {
+  for (int t = cap; t >= 1; --t)
+    if (n % t == 0) return t;
+  return 1;
+}
+
+extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
+  if (!d || !out) return FD3_EINVAL;
+  *out = nullptr;
+  const int S = d->n_species, R = d->n_rank;
+  if (S < 1 || S > FD3_MAX_SPECIES || R < 1 || R > FD3_MAX_RANK) {
+    set_error("fd3_plan_create", "n_species must be 1..64 and n_rank 1..32");
+    return FD3_EINVAL;
+  }
+  if (d->method != FD3_METHOD_SPME && d->method != FD3_METHOD_PME && d->method != FD3_METHOD_EWALD) return FD3_EINVAL;
+  if (d->precision != FD3_PREC_FP64 && d->precision != FD3_PREC_MIXED) return FD3_EINVAL;
+  const bool mesh = d->method != FD3_METHOD_EWALD;
+  if (mesh) {
+    if (d->order < 1 || d->order > FD3_MAX_ORDER) {
+      set_error("fd3_plan_create", "interpolation order must be 1..8");
+      return FD3_EINVAL;
+    }
+    for (int a = 0; a < 3; ++a)
+      if (d->mesh[a] < 1) return FD3_EINVAL;
+    if (S > 8) {
+      set_error("fd3_plan_create", "mesh filter kernel supports up to 8 species");
+      return FD3_EINVAL;
+    }
+  }
+  fd3_plan* p = new (std::nothrow) fd3_plan();
+  if (!p) return FD3_EINVAL;
+  p->S = S;
+  p->R = R;
+  p->method = d->method;
+  p->P = d->order;
+  p->precision = d->precision;
+  for (int a = 0; a < 3; ++a) p->ens[a] = d->ewald_ns[a];
+
+  Tables& t = p->h_tab;
+  memset(&t, 0, sizeof(t));
+  t.n_species = S;
+  t.n_rank = R;
+  t.s6 = d->params[0];
+  t.s8 = d->params[1];
+  t.r_cut = d->r_cut;
+  t.has_cncorr = d->has_cncorr && d->cncorr;
+  for (int s = 0; s < S; ++s) {
+    t.rcov[s] = d->rcov[s];
+    for (int q = 0; q < 7; ++q) t.cnref[7 * s + q] = d->cnref[7 * s + q];
+    if (t.has_cncorr) {
+      t.cncorr[2 * s] = d->cncorr[2 * s];
+      t.cncorr[2 * s + 1] = d->cncorr[2 * s + 1];
+    }
+  }
+  for (int r = 0; r < R; ++r) t.eigs[r] = d->eigs[r];
+  // Green's function constants per species pair (pair_pot.py:55-105) and phi_XX(0) (:84-89)
+  GreenPair* gp = new GreenPair[S * S];
+  const double pi = kPi, pi2 = pi * pi;
+  const double a1 = d->params[2], a2 = d->params[3];
+  for (int X = 0; X < S; ++X)
+    for (int Y = 0; Y < S; ++Y) {
+      GreenPair& g = gp[X * S + Y];
+      g.qq = d->sqrtq[X] * d->sqrtq[Y];
+      g.R = a1 * sqrt(3.0 * g.qq) + a2;
+      const double R2 = g.R * g.R, R3 = R2 * g.R, R4 = g.R * R3, R5 = g.R * R4, R6 = R3 * R3;
+      g.c6s1 = (2.0 * pi2) / (3.0 * R3);
+      g.c6s2 = (2.0 * pi2 * g.R) / 9.0;
+      g.c6pre = (2.0 * pi2) / (3.0 * R4);
+      g.c8s1 = (pi2 * sqrt(2.0) * sin(pi / 8.0)) / R5;
+      g.c8s2 = g.c8s1 * R2 / 6.0;
+      g.c8pre = -pi2 / R6;
+      if (X == Y) {
+        const double R8 = R3 * R5;
+        t.selfcont[X] = t.s6 / R6 + 3.0 * t.s8 * g.qq / R8;
+      }
+    }
+  int rc = FD3_OK;
+  do {
+    if (cudaMalloc(&p->d_tab, sizeof(Tables)) != cudaSuccess ||
+        cudaMalloc(&p->d_eigvecs, sizeof(double) * S * 7 * R) != cudaSuccess ||
+        cudaMalloc(&p->d_green, sizeof(GreenPair) * S * S) != cudaSuccess) {
+      set_error("fd3_plan_create", "cudaMalloc of the species tables failed");
+      rc = FD3_ECUDA;
+      break;
+    }
+    if (cudaMemcpy(p->d_tab, &t, sizeof(Tables), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(p->d_eigvecs, d->eigvecs, sizeof(double) * S * 7 * R, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(p->d_green, gp, sizeof(GreenPair) * S * S, cudaMemcpyHostToDevice) != cudaSuccess) {
+      set_error("fd3_plan_create", "upload of the species tables failed");
+      rc = FD3_ECUDA;
+      break;
+    }
+    if (mesh) {
+      MeshGeom& m = p->mg;
+      for (int a = 0; a < 3; ++a) {
+        m.n[a] = d->mesh[a];
+        m.t[a] = largest_divisor_le(m.n[a], 8);
+        m.nt[a] = m.n[a] / m.t[a];
+        const int need = 1 + (d->order - 1 + m.t[a] - 1) / m.t[a];
+        m.ns[a] = need < m.nt[a] ? need : m.nt[a];
+      }
+      m.nzh = m.n[2] / 2 + 1;
+      m.order = d->order;
+      m.lagrange = d->method == FD3_METHOD_PME;
+      m.S = S;
+      m.R = R;
+      const size_t Mh = (size_t)m.n[0] * m.n[1] * m.nzh;
+      if (d->method == FD3_METHOD_SPME && d->deconv) {
+        if (cudaMalloc(&p->d_deconv, sizeof(float) * Mh) != cudaSuccess ||
+            cudaMemcpy(p->d_deconv, d->deconv, sizeof(float) * Mh, cudaMemcpyHostToDevice) != cudaSuccess) {
+          set_error("fd3_plan_create", "upload of the deconvolution window failed");
+          rc = FD3_ECUDA;
+          break;
+        }
+      }
+      // batched 3D real transforms over the S*R channels (only library call of the pipeline)
+      int n[3] = {m.n[0], m.n[1], m.n[2]};
+      const int C = S * R;
+      const int M = m.n[0] * m.n[1] * m.n[2];
+      const int Mhi = (int)Mh;
+      const bool dp = d->precision == FD3_PREC_FP64;
+      size_t ws1 = 0, ws2 = 0;
+      cufftResult fr;
+      if ((fr = cufftCreate(&p->fwd)) != CUFFT_SUCCESS || (fr = cufftCreate(&p->inv)) != CUFFT_SUCCESS ||
+          (fr = cufftSetAutoAllocation(p->fwd, 0)) != CUFFT_SUCCESS ||
+          (fr = cufftSetAutoAllocation(p->inv, 0)) != CUFFT_SUCCESS ||
+          (fr = cufftMakePlanMany(p->fwd, 3, n, nullptr, 1, M, nullptr, 1, Mhi, dp ? CUFFT_D2Z : CUFFT_R2C, C,
+                                  &ws1)) != CUFFT_SUCCESS ||
+          (fr = cufftMakePlanMany(p->inv, 3, n, nullptr, 1, Mhi, nullptr, 1, M, dp ? CUFFT_Z2D : CUFFT_C2R, C,
+                                  &ws2)) != CUFFT_SUCCESS) {
+        char b[64];
+        snprintf(b, sizeof(b), "cufft status %d", (int)fr);
+        set_error("fd3_plan_create: cufft plan", b);
+        rc = FD3_ECUFFT;
+        break;
+      }
+      p->has_fft = true;
+      p->fft_ws = ws1 > ws2 ? ws1 : ws2;
+    }
+  } while (0);
+  delete[] gp;
+  if (rc) {
+    fd3_plan_destroy(p);
+    return rc;
+  }
+  *out = p;
+  return FD3_OK;
+}
+
+extern "C" int fd3_plan_destroy(fd3_plan* p) {
+  if (!p) return FD3_OK;
+  for (int k = 0; k < fd3_plan::kMaxMarks; ++k)
+    if (p->ev[k]) cudaEventDestroy(p->ev[k]);
+  if (p->fwd) cufftDestroy(p->fwd);
+  if (p->inv) cufftDestroy(p->inv);
+  cudaFree(p->d_tab);
+  cudaFree(p->d_eigvecs);
+  cudaFree(p->d_green);
+  cudaFree(p->d_deconv);
+  delete p;
+  return FD3_OK;
+}
+
+// ------------------------------------------------------------------ workspace layout
+namespace {
+struct Carver {
+  size_t off = 0;
+  char* base = nullptr;
+  template <typename T>
+  T* take(size_t count) {
+    off = (off + 255) & ~(size_t)255;
+    T* r = base ? reinterpret_cast<T*>(base + off) : nullptr;
+    off += sizeof(T) * (count ? count : 1);
+    return r;
+  }
+};
+
+struct Work {
+  CellInfo* ci;
+  double *cn, *c6, *dc6, *gcn;
+  double *self_part, *kspc_part, *cnv_part, *mcell_part;
+  int *mkeys, *mcount, *mstart, *morder;
+  CellList cl;
+  void *rho, *spec, *fftw;
+};
+
+void carve(const fd3_plan* p, int64_t N, int64_t K, Carver& c, Work& w) {
+  const int R = p->R;
+  const int64_t nblk = (N + 7) / 8 + 1;
+  w.ci = c.take<CellInfo>(1);
+  w.cn = c.take<double>(N);
+  w.c6 = c.take<double>(N * R);
+  w.dc6 = c.take<double>(N * R);
+  w.gcn = c.take<double>(N);
+  w.self_part = c.take<double>(nblk);
+  w.cnv_part = c.take<double>(9 * nblk);
+  w.mcell_part = c.take<double>(9 * nblk);
+  const bool mesh = p->method != FD3_METHOD_EWALD;
+  size_t Mh = 0, M = 0;
+  int64_t Kmesh = 1;
+  if (mesh) {
+    Mh = (size_t)p->mg.n[0] * p->mg.n[1] * p->mg.nzh;
+    M = (size_t)p->mg.n[0] * p->mg.n[1] * p->mg.n[2];
+    Kmesh = (int64_t)p->mg.nt[0] * p->mg.nt[1] * p->mg.nt[2] * p->S;
+  }
+  w.kspc_part = c.take<double>(7 * ((Mh + 255) / 256 + 1));
+  w.mkeys = c.take<int>(N);
+  w.mcount = c.take<int>(Kmesh);
+  w.mstart = c.take<int>(Kmesh + 1);
+  w.morder = c.take<int>(N);
+  w.cl.bin_of = c.take<int>(N);
+  w.cl.bin_count = c.take<int>(K);
+  w.cl.bin_start = c.take<int>(K + 1);
+  w.cl.order = c.take<int>(N);
+  w.cl.xs = c.take<double4>(N);
+  w.cl.meta = c.take<int4>(N);
+  w.cl.off = c.take<int4>(N);
+  const size_t es = p->precision == FD3_PREC_FP64 ? sizeof(double) : sizeof(float);
+  const size_t C = (size_t)p->S * p->R;
+  w.rho = c.take<char>(mesh ? C * M * es : 1);
+  w.spec = c.take<char>(mesh ? C * Mh * 2 * es : 1);
+  w.fftw = c.take<char>(p->fft_ws);
+}
+}  // namespace
+
+extern "C" int fd3_workspace_size(const fd3_plan* p, int64_t n_atoms, int64_t n_bins, size_t* bytes) {
+  if (!p || !bytes || n_atoms < 0) return FD3_EINVAL;
+  Carver c;
+  Work w;
+  carve(p, n_atoms, n_bins > 0 ? n_bins : 1, c, w);
+  *bytes = c.off + 256;
+  return FD3_OK;
+}
+
+extern "C" int fd3_cell_grid(const double* h_cell, double r_cut, int32_t* nb3, int32_t* reach3) {
+  CellGrid g;
+  int rc = make_cell_grid(h_cell, r_cut, &g);
+  if (rc) return rc;
+  for (int a = 0; a < 3; ++a) {
+    if (nb3) nb3[a] = g.nb[a];
+    if (reach3) reach3[a] = g.reach[a];
+  }
+  return FD3_OK;
+}
+
+static int check_work(const fd3_plan* p, int64_t N, int64_t K, void* work, size_t bytes, Work& w) {
+  Carver c;
+  carve(p, N, K, c, w);
+  if (!work || bytes < c.off + 256) {
+    set_error("workspace", "smaller than fd3_workspace_size");
+    return FD3_ENOMEM;
+  }
+  Carver c2;
+  c2.base = reinterpret_cast<char*>(((uintptr_t)work + 255) & ~(uintptr_t)255);
+  carve(p, N, K, c2, w);
+  return FD3_OK;
+}
+
+// ------------------------------------------------------------------ shared mesh pipeline
+// spread -> forward FFT -> filter (energy, virial, H = G S) -> [inverse FFT -> gather]
+template <typename T>
+static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const int32_t* species, Work& w,
+                         bool need_grad, double* gpos, double* mcell, int* n_kspc, int* n_mcell, cudaStream_t s) {
+  const MeshGeom& mg = p->mg;
+  const int Kmesh = mg.nt[0] * mg.nt[1] * mg.nt[2] * p->S;
+  FD3_TRY(launch_mesh_keys(mg, N, pos, ps, species, w.ci, w.mkeys, s));
+  FD3_TRY(counting_sort(w.mkeys, N, Kmesh, w.mcount, w.mstart, w.morder, s));
+  prof_mark(p, s, "mesh_sort");
+  FD3_TRY(launch_spread<T>(mg, pos, ps, species, w.c6, w.ci, w.mstart, w.morder, (T*)w.rho, s));
+  prof_mark(p, s, "spread");
+  FD3_CUFFT(cufftSetStream(p->fwd, s));
+  FD3_CUFFT(cufftSetWorkArea(p->fwd, w.fftw));
+  if (sizeof(T) == 8)
+    FD3_CUFFT(cufftExecD2Z(p->fwd, (cufftDoubleReal*)w.rho, (cufftDoubleComplex*)w.spec));
+  else
+    FD3_CUFFT(cufftExecR2C(p->fwd, (cufftReal*)w.rho, (cufftComplex*)w.spec));
+  prof_mark(p, s, "fft_r2c");
+  FD3_TRY(launch_filter<T>(mg, w.ci, p->d_green, p->d_tab, p->d_deconv, p->method == FD3_METHOD_SPME, w.spec,
+                           w.kspc_part, n_kspc, s));
+  prof_mark(p, s, "filter");
+  *n_mcell = 0;
+  if (!need_grad) return FD3_OK;
+  FD3_CUFFT(cufftSetStream(p->inv, s));
+  FD3_CUFFT(cufftSetWorkArea(p->inv, w.fftw));
+  if (sizeof(T) == 8)
+    FD3_CUFFT(cufftExecZ2D(p->inv, (cufftDoubleComplex*)w.spec, (cufftDoubleReal*)w.rho));
+  else
+    FD3_CUFFT(cufftExecC2R(p->inv, (cufftComplex*)w.spec, (cufftReal*)w.rho));
+  prof_mark(p, s, "fft_c2r");
+  FD3_TRY(launch_gather<T>(mg, N, pos, ps, species, w.c6, w.dc6, w.ci, p->d_tab, w.morder, (const T*)w.rho, w.gcn,
+                           gpos, mcell, n_mcell, s));
+  prof_mark(p, s, "gather");
+  return FD3_OK;
+}
+
+static int run_mesh(fd3_plan* p, int N, const double* pos, double ps, const int32_t* species, Work& w,
+                    bool need_grad, double* gpos, double* mcell, int* n_kspc, int* n_mcell, cudaStream_t s) {
+  if (p->precision == FD3_PREC_FP64)
+    return mesh_pipeline<double>(p, N, pos, ps, species, w, need_grad, gpos, mcell, n_kspc, n_mcell, s);
+  return mesh_pipeline<float>(p, N, pos, ps, species, w, need_grad, gpos, mcell, n_kspc, n_mcell, s);
+}
+
+// ------------------------------------------------------------------ edge-list entry
+extern "C" int fd3_energy_edges(fd3_plan* p, int64_t n_atoms, const double* d_pos, const int32_t* d_species,
+                                const double* d_cell, int64_t n_edges, const int64_t* d_src, const int64_t* d_dst,
+                                const double* d_shift, int32_t need_grad, void* d_work, size_t work_bytes,
+                                double* d_energy, double* d_gpos, double* d_gshift, double* d_gcell, void* stream) {
+  if (!p || n_atoms < 1 || n_atoms > (int64_t)1 << 30 || !d_pos || !d_species || !d_cell || !d_energy)
+    return FD3_EINVAL;
+  if (n_edges < 0 || (n_edges > 0 && (!d_src || !d_dst || !d_shift))) return FD3_EINVAL;
+  if (need_grad && (!d_gpos || !d_gcell || (n_edges > 0 && !d_gshift))) return FD3_EINVAL;
+  if (p->method == FD3_METHOD_EWALD) {
+    set_error("fd3_energy_edges", "method ewald is served by fd3_ewald_* entry points");
+    return FD3_EINVAL;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const int N = (int)n_atoms;
+  Work w;
+  FD3_TRY(check_work(p, N, 1, d_work, work_bytes, w));
+  prof_begin(p, s);
+  FD3_TRY(launch_cellinfo(d_cell, 1.0, w.ci, s));
+  FD3_CUDA(cudaMemsetAsync(w.cn, 0, sizeof(double) * N, s));
+  FD3_TRY(launch_cn_edges(n_edges, d_pos, d_species, d_src, d_dst, d_shift, p->d_tab, w.cn, s));
+  int n_self = 0, n_kspc = 0, n_mcell = 0;
+  FD3_TRY(launch_c6_atoms(N, d_species, p->d_tab, p->d_eigvecs, p->R, w.cn, w.c6, w.dc6, w.self_part, &n_self, s));
+  prof_mark(p, s, "cn_c6");
+  FD3_TRY(run_mesh(p, N, d_pos, 1.0, d_species, w, need_grad != 0, d_gpos, w.mcell_part, &n_kspc, &n_mcell, s));
+  if (need_grad)
+    FD3_TRY(launch_cn_adjoint_edges(n_edges, d_pos, d_species, d_src, d_dst, d_shift, p->d_tab, w.gcn, d_gpos,
+                                    d_gshift, s));
+  prof_mark(p, s, "cn_adjoint");
+  Partials pa{w.self_part, n_self, w.kspc_part, n_kspc, w.cnv_part, 0, w.mcell_part, n_mcell};
+  FD3_TRY(launch_finalize(pa, w.ci, 0, 1.0, d_energy, need_grad ? d_gcell : nullptr, s));
+  prof_mark(p, s, "finalize");
+  return FD3_OK;
+}
+
+// ------------------------------------------------------------------ fused entry
+extern "C" int fd3_energy_forces_stress(fd3_plan* p, int64_t n_atoms, const double* d_pos_ang,
+                                        const int32_t* d_species, const double* h_cell_ang,
+                                        const double* d_cell_ang, double r_cut_ang, void* d_work,
+                                        size_t work_bytes, double* d_energy, double* d_forces, double* d_stress,
+                                        void* stream) {
+  if (!p || n_atoms < 1 || n_atoms > (int64_t)1 << 30 || !d_pos_ang || !d_species || !h_cell_ang || !d_cell_ang ||
+      !d_energy || !d_forces || !d_stress)
+    return FD3_EINVAL;
+  if (p->method == FD3_METHOD_EWALD) {
+    set_error("fd3_energy_forces_stress", "method ewald is served by fd3_ewald_* entry points");
+    return FD3_EINVAL;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const int N = (int)n_atoms;
+  CellGrid g;
+  FD3_TRY(make_cell_grid(h_cell_ang, r_cut_ang, &g));
+  const int64_t K = (int64_t)g.nb[0] * g.nb[1] * g.nb[2];
+  Work w;
+  FD3_TRY(check_work(p, N, K, d_work, work_bytes, w));
+  prof_begin(p, s);
+  FD3_TRY(launch_cellinfo(d_cell_ang, kAngToBohr, w.ci, s));
+  FD3_TRY(build_cell_list(g, N, d_pos_ang, d_species, w.cl, s));
+  prof_mark(p, s, "cell_list");
+  int n_self = 0, n_kspc = 0, n_mcell = 0, n_cnv = 0;
+  FD3_TRY(launch_cn_c6_cells(g, N, w.cl, d_pos_ang, d_species, p->d_tab, p->d_eigvecs, p->R, w.cn, w.c6, w.dc6,
+                             w.self_part, &n_self, s));
+  prof_mark(p, s, "cn_c6");
+  // the mesh gradient (Hartree/Bohr) is staged in d_forces, then finished by the CN adjoint
+  FD3_TRY(run_mesh(p, N, d_pos_ang, kAngToBohr, d_species, w, true, d_forces, nullptr, &n_kspc, &n_mcell, s));
+  FD3_TRY(launch_cn_adjoint_cells(g, N, w.cl, d_pos_ang, d_species, p->d_tab, w.gcn, d_forces,
+                                  -kHartreeToEv * kAngToBohr, w.cnv_part, &n_cnv, s));
+  prof_mark(p, s, "cn_adjoint");
+  Partials pa{w.self_part, n_self, w.kspc_part, n_kspc, w.cnv_part, n_cnv, nullptr, 0};
+  FD3_TRY(launch_finalize(pa, w.ci, 1, kHartreeToEv, d_energy, d_stress, s));
+  prof_mark(p, s, "finalize");
+  return FD3_OK;
+}
+
+// ------------------------------------------------------------------ neighbour export
+namespace {
+struct NbrWork {
+  CellList cl;
+  int* counts;
+  int* row_start;
+};
+void carve_nbr(int64_t N, int64_t K, Carver& c, NbrWork& w) {
+  w.cl.bin_of = c.take<int>(N);
+  w.cl.bin_count = c.take<int>(K);
+  w.cl.bin_start = c.take<int>(K + 1);
+  w.cl.order = c.take<int>(N);
+  w.cl.xs = c.take<double4>(N);
+  w.cl.meta = c.take<int4>(N);
+  w.cl.off = c.take<int4>(N);
+  w.counts = c.take<int>(N);
+  w.row_start = c.take<int>(N + 1);
+}
+int nbr_prepare(int64_t n, const double* d_pos, const double* h_cell, double r_cut, void* d_work, size_t bytes,
+                CellGrid& g, NbrWork& w, cudaStream_t s) {
+  if (n < 1 || n > (int64_t)1 << 30 || !d_pos || !h_cell) return FD3_EINVAL;
+  FD3_TRY(make_cell_grid(h_cell, r_cut, &g));
+  const int64_t K = (int64_t)g.nb[0] * g.nb[1] * g.nb[2];
+  Carver c;
+  carve_nbr(n, K, c, w);
+  if (!d_work || bytes < c.off + 256) return FD3_ENOMEM;
+  Carver c2;
+  c2.base = reinterpret_cast<char*>(((uintptr_t)d_work + 255) & ~(uintptr_t)255);
+  carve_nbr(n, K, c2, w);
+  FD3_TRY(build_cell_list(g, (int)n, d_pos, nullptr, w.cl, s));
+  FD3_TRY(launch_nbr_count(g, (int)n, w.cl, d_pos, w.counts, s));
+  FD3_TRY(scan_exclusive(w.counts, (int)n, w.row_start, s));
+  return FD3_OK;
+}
+}  // namespace
+
+extern "C" int fd3_neighbor_workspace_size(int64_t n, const double* h_cell, double r_cut, size_t* bytes) {
+  CellGrid g;
+  if (!bytes) return FD3_EINVAL;
+  FD3_TRY(make_cell_grid(h_cell, r_cut, &g));
+  Carver c;
+  NbrWork w;
+  carve_nbr(n, (int64_t)g.nb[0] * g.nb[1] * g.nb[2], c, w);
+  *bytes = c.off + 256;
+  return FD3_OK;
+}
+
+extern "C" int fd3_neighbor_count(int64_t n, const double* d_pos, const double* h_cell, double r_cut, void* d_work,
+                                  size_t bytes, int64_t* h_count, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  CellGrid g;
+  NbrWork w;
+  if (!h_count) return FD3_EINVAL;
+  FD3_TRY(nbr_prepare(n, d_pos, h_cell, r_cut, d_work, bytes, g, w, s));
+  int total = 0;
+  FD3_CUDA(cudaMemcpyAsync(&total, w.row_start + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FD3_CUDA(cudaStreamSynchronize(s));
+  *h_count = total;
+  return FD3_OK;
+}
+
+extern "C" int fd3_neighbor_fill(int64_t n, const double* d_pos, const double* h_cell, double r_cut, void* d_work,
+                                 size_t bytes, int64_t capacity, int64_t* d_src, int64_t* d_dst, int32_t* d_shift,
+                                 int64_t* h_count, void* stream) {
+  cudaStream_t s = (cudaStream_t)stream;
+  CellGrid g;
+  NbrWork w;
+  if (!h_count || !d_src || !d_dst || !d_shift) return FD3_EINVAL;
+  FD3_TRY(nbr_prepare(n, d_pos, h_cell, r_cut, d_work, bytes, g, w, s));
+  int total = 0;
+  FD3_CUDA(cudaMemcpyAsync(&total, w.row_start + n, sizeof(int), cudaMemcpyDeviceToHost, s));
+  FD3_CUDA(cudaStreamSynchronize(s));
+  *h_count = total;
+  if (total > capacity) return FD3_ECAPACITY;
+  FD3_TRY(launch_nbr_fill(g, (int)n, w.cl, d_pos, w.row_start, d_src, d_dst, d_shift, s));
+  return FD3_OK;
+}
+
+// ------------------------------------------------------------------ profiling
+extern "C" int fd3_profile_enable(fd3_plan* p, int32_t on) {
+  if (!p) return FD3_EINVAL;
+  if (on && !p->ev[0])
+    for (int k = 0; k < fd3_plan::kMaxMarks; ++k) FD3_CUDA(cudaEventCreate(&p->ev[k]));
+  p->prof = on != 0;
+  return FD3_OK;
+}
+
+extern "C" int fd3_profile_read(fd3_plan* p, double* ms, int32_t max_stages, char* names, int32_t names_len,
+                                int32_t* n_stages) {
+  if (!p || !ms || !n_stages) return FD3_EINVAL;
+  *n_stages = 0;
+  if (!p->prof || p->n_marks < 2) return FD3_OK;
+  FD3_CUDA(cudaEventSynchronize(p->ev[p->n_marks - 1]));
+  int n = 0;
+  size_t used = 0;
+  if (names && names_len > 0) names[0] = 0;
+  for (int k = 1; k < p->n_marks && n < max_stages; ++k, ++n) {
+    float t = 0.f;
+    FD3_CUDA(cudaEventElapsedTime(&t, p->ev[k - 1], p->ev[k]));
+    ms[n] = t;
+    if (names && names_len > 0) {
+      const int w = snprintf(names + used, names_len - used, "%s%s", n ? "," : "", p->mark_name[k]);
+      if (w > 0 && used + w < (size_t)names_len) used += w;
+    }
+  }
+  *n_stages = n;
+  return FD3_OK;
+}

@@ -1,0 +1,649 @@
+// Cell-list neighbour search, smooth-cutoff coordination numbers, C6 factors and the
+// CN adjoint (reference: src/fourierd3/core.py:323-386, 449-478, 525-550 and the matscipy
+// neighbour build at src/fourierd3/calculator.py:94-123).
+//
+// Design: atoms are counting-sorted into a bin grid whose bins are at least r_cut wide (in
+// perpendicular height), so a neighbour lies within `reach` bins per axis. Bins are laid out
+// with z fastest, so for a fixed (dx, dy) the bins bz-reach..bz+reach are one contiguous run of
+// the bin-sorted atom array (split only at the periodic wrap). One warp handles one atom and
+// strides its lanes over those runs, so the candidate loads are coalesced.
+#include <math.h>
+#include <stdio.h>
+
+#include "fd3_internal.h"
+
+namespace fd3 {
+
+// ------------------------------------------------------------------ host geometry
+static void inv3_host(const double* m, double* inv, double* det_out) {
+  const double c00 = m[4] * m[8] - m[5] * m[7];
+  const double c01 = m[2] * m[7] - m[1] * m[8];
+  const double c02 = m[1] * m[5] - m[2] * m[4];
+  const double c10 = m[5] * m[6] - m[3] * m[8];
+  const double c11 = m[0] * m[8] - m[2] * m[6];
+  const double c12 = m[2] * m[3] - m[0] * m[5];
+  const double c20 = m[3] * m[7] - m[4] * m[6];
+  const double c21 = m[1] * m[6] - m[0] * m[7];
+  const double c22 = m[0] * m[4] - m[1] * m[3];
+  const double det = m[0] * c00 + m[1] * c10 + m[2] * c20;
+  const double a[9] = {c00, c01, c02, c10, c11, c12, c20, c21, c22};
+  for (int k = 0; k < 9; ++k) inv[k] = a[k] / det;
+  if (det_out) *det_out = det;
+}
+
+int make_cell_grid(const double* h_cell, double r_cut, CellGrid* g) {
+  if (!(r_cut > 0)) return FD3_EINVAL;
+  double det;
+  inv3_host(h_cell, g->inv, &det);
+  if (!(fabs(det) > 0) || !isfinite(det)) return FD3_EINVAL;
+  for (int k = 0; k < 9; ++k) g->cell[k] = h_cell[k];
+  for (int a = 0; a < 3; ++a) {
+    // perpendicular height of the cell along axis a = 1 / |column a of inv(cell)|
+    const double cn = sqrt(g->inv[0 * 3 + a] * g->inv[0 * 3 + a] + g->inv[1 * 3 + a] * g->inv[1 * 3 + a] +
+                           g->inv[2 * 3 + a] * g->inv[2 * 3 + a]);
+    const double h = 1.0 / cn;
+    int nb = (int)floor(h / r_cut);
+    if (nb < 1) nb = 1;
+    if (nb > 512) nb = 512;
+    g->nb[a] = nb;
+    g->reach[a] = (int)ceil(r_cut * nb / h + 1e-9);
+  }
+  g->r_cut = r_cut;
+  g->rc2 = r_cut * r_cut;
+  return FD3_OK;
+}
+
+// ------------------------------------------------------------------ scan / sort
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+
+__global__ void k_scan_exclusive(const int* __restrict__ in, int n, int* __restrict__ out) {
+  __shared__ int warp_tot[32];
+  __shared__ int carry_s;
+  if (threadIdx.x == 0) carry_s = 0;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int base = 0; base < n; base += kScanThreads * kScanItems) {
+    int v[kScanItems];
+    int local = 0;
+    const int i0 = base + threadIdx.x * kScanItems;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      v[k] = (i0 + k < n) ? in[i0 + k] : 0;
+      local += v[k];
+    }
+    int incl = local;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_tot[wid] = incl;
+    __syncthreads();
+    if (wid == 0) {
+      int w = warp_tot[lane];
+      int wi = w;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        int t = __shfl_up_sync(0xffffffffu, wi, o);
+        if (lane >= o) wi += t;
+      }
+      warp_tot[lane] = wi - w;   // exclusive warp offsets
+    }
+    __syncthreads();
+    int run = carry_s + warp_tot[wid] + incl - local;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+      if (i0 + k < n) out[i0 + k] = run;
+      run += v[k];
+    }
+    __syncthreads();
+    if (threadIdx.x == kScanThreads - 1) carry_s = run;
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) out[n] = carry_s;
+}
+
+int scan_exclusive(const int* in, int n, int* out, cudaStream_t s) {
+  k_scan_exclusive<<<1, kScanThreads, 0, s>>>(in, n, out);
+  FD3_LAUNCHED();
+  return FD3_OK;
+}
+
+__global__ void k_hist(const int* __restrict__ keys, int n, int* __restrict__ counts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) atomicAdd(&counts[keys[i]], 1);
+}
+
+__global__ void k_scatter(const int* __restrict__ keys, int n, const int* __restrict__ starts,
+                          int* __restrict__ fill, int* __restrict__ order) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) {
+    const int k = keys[i];
+    order[starts[k] + atomicAdd(&fill[k], 1)] = i;
+  }
+}
+
+// Insertion sort of each key segment by atom id: makes the order (and every sum taken in
+// that order) independent of the atomic slot assignment above.
+__global__ void k_sort_segments(const int* __restrict__ starts, int K, int* __restrict__ order) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= K) return;
+  const int a = starts[k], b = starts[k + 1];
+  for (int u = a + 1; u < b; ++u) {
+    const int v = order[u];
+    int w = u - 1;
+    while (w >= a && order[w] > v) {
+      order[w + 1] = order[w];
+      --w;
+    }
+    order[w + 1] = v;
+  }
+}
+
+int counting_sort(const int* keys, int n, int K, int* counts, int* starts, int* order, cudaStream_t s) {
+  const int tb = 256;
+  FD3_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * K, s));
+  if (n > 0) {
+    k_hist<<<(n + tb - 1) / tb, tb, 0, s>>>(keys, n, counts);
+    FD3_LAUNCHED();
+  }
+  int rc = scan_exclusive(counts, K, starts, s);
+  if (rc) return rc;
+  FD3_CUDA(cudaMemsetAsync(counts, 0, sizeof(int) * K, s));
+  if (n > 0) {
+    k_scatter<<<(n + tb - 1) / tb, tb, 0, s>>>(keys, n, starts, counts, order);
+    FD3_LAUNCHED();
+  }
+  k_sort_segments<<<(K + tb - 1) / tb, tb, 0, s>>>(starts, K, order);
+  FD3_LAUNCHED();
+  return FD3_OK;
+}
+
+// ------------------------------------------------------------------ cell list
+struct GridDev {
+  int nb[3], reach[3];
+  double cell[9], inv[9];
+  double rc2;
+};
+static GridDev to_dev(const CellGrid& g) {
+  GridDev d;
+  for (int a = 0; a < 3; ++a) {
+    d.nb[a] = g.nb[a];
+    d.reach[a] = g.reach[a];
+  }
+  for (int k = 0; k < 9; ++k) {
+    d.cell[k] = g.cell[k];
+    d.inv[k] = g.inv[k];
+  }
+  d.rc2 = g.rc2;
+  return d;
+}
+
+__global__ void k_bin_atoms(GridDev g, int n, const double* __restrict__ x, int* __restrict__ bin_of,
+                            int4* __restrict__ off) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double x0 = x[3 * i], x1 = x[3 * i + 1], x2 = x[3 * i + 2];
+  int o[3], b[3];
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double f = x0 * g.inv[a] + x1 * g.inv[3 + a] + x2 * g.inv[6 + a];
+    const double fl = floor(f);
+    o[a] = (int)fl;
+    int bb = (int)((f - fl) * g.nb[a]);
+    b[a] = bb < 0 ? 0 : (bb >= g.nb[a] ? g.nb[a] - 1 : bb);
+  }
+  const int bin = (b[0] * g.nb[1] + b[1]) * g.nb[2] + b[2];
+  bin_of[i] = bin;
+  off[i] = make_int4(o[0], o[1], o[2], bin);
+}
+
+__global__ void k_gather_sorted(int n, const int* __restrict__ order, const double* __restrict__ x,
+                                const int32_t* __restrict__ species, const int4* __restrict__ off,
+                                double4* __restrict__ xs, int4* __restrict__ meta) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int i = order[t];
+  xs[t] = make_double4(x[3 * i], x[3 * i + 1], x[3 * i + 2], species ? (double)species[i] : 0.0);
+  const int4 o = off[i];
+  meta[t] = make_int4(o.x, o.y, o.z, i);
+}
+
+int build_cell_list(const CellGrid& g, int n, const double* pos_ang, const int32_t* species, CellList& cl,
+                    cudaStream_t s) {
+  const int K = g.nb[0] * g.nb[1] * g.nb[2];
+  const int tb = 256;
+  if (n > 0) {
+    k_bin_atoms<<<(n + tb - 1) / tb, tb, 0, s>>>(to_dev(g), n, pos_ang, cl.bin_of, cl.off);
+    FD3_LAUNCHED();
+  }
+  int rc = counting_sort(cl.bin_of, n, K, cl.bin_count, cl.bin_start, cl.order, s);
+  if (rc) return rc;
+  if (n > 0) {
+    k_gather_sorted<<<(n + tb - 1) / tb, tb, 0, s>>>(n, cl.order, pos_ang, species, cl.off, cl.xs, cl.meta);
+    FD3_LAUNCHED();
+  }
+  return FD3_OK;
+}
+
+// Visit every candidate (j, S) of atom i. All lanes of the warp run the same number of
+// iterations; `fn(hit, u, j, S, d)` gets the exact-predicate result (Angstrom, no FMA).
+template <class Fn>
+__device__ __forceinline__ void visit_neighbors(const GridDev& g, const int* __restrict__ bin_start,
+                                                const double4* __restrict__ xs, const int4* __restrict__ meta,
+                                                int i, double xi0, double xi1, double xi2, int4 offi, Fn&& fn) {
+  const int lane = threadIdx.x & 31;
+  const int bin = offi.w;
+  const int bz = bin % g.nb[2];
+  const int by = (bin / g.nb[2]) % g.nb[1];
+  const int bx = bin / (g.nb[2] * g.nb[1]);
+  for (int dx = -g.reach[0]; dx <= g.reach[0]; ++dx) {
+    const int cx = bx + dx;
+    const int sx = floordiv(cx, g.nb[0]);
+    const int wx = cx - sx * g.nb[0];
+    for (int dy = -g.reach[1]; dy <= g.reach[1]; ++dy) {
+      const int cy = by + dy;
+      const int sy = floordiv(cy, g.nb[1]);
+      const int wy = cy - sy * g.nb[1];
+      int zs = bz - g.reach[2];
+      const int ze = bz + g.reach[2];
+      while (zs <= ze) {
+        const int sz = floordiv(zs, g.nb[2]);
+        const int wz = zs - sz * g.nb[2];
+        int len = g.nb[2] - wz;
+        if (len > ze - zs + 1) len = ze - zs + 1;
+        const int b0 = (wx * g.nb[1] + wy) * g.nb[2] + wz;
+        const int a0 = bin_start[b0], a1 = bin_start[b0 + len];
+        for (int u0 = a0; u0 < a1; u0 += 32) {
+          const int u = u0 + lane;
+          bool hit = false;
+          int j = 0;
+          int S0 = 0, S1 = 0, S2 = 0;
+          double d0 = 0, d1 = 0, d2 = 0;
+          if (u < a1) {
+            const double4 xj = xs[u];
+            const int4 mj = meta[u];
+            j = mj.w;
+            S0 = sx + offi.x - mj.x;
+            S1 = sy + offi.y - mj.y;
+            S2 = sz + offi.z - mj.z;
+            const double sh0 = dadd(dadd(dmul((double)S0, g.cell[0]), dmul((double)S1, g.cell[3])),
+                                    dmul((double)S2, g.cell[6]));
+            const double sh1 = dadd(dadd(dmul((double)S0, g.cell[1]), dmul((double)S1, g.cell[4])),
+                                    dmul((double)S2, g.cell[7]));
+            const double sh2 = dadd(dadd(dmul((double)S0, g.cell[2]), dmul((double)S1, g.cell[5])),
+                                    dmul((double)S2, g.cell[8]));
+            d0 = dadd(dsub(xj.x, xi0), sh0);
+            d1 = dadd(dsub(xj.y, xi1), sh1);
+            d2 = dadd(dsub(xj.z, xi2), sh2);
+            const double r2 = dadd(dadd(dmul(d0, d0), dmul(d1, d1)), dmul(d2, d2));
+            hit = r2 < g.rc2 && !(j == i && S0 == 0 && S1 == 0 && S2 == 0);
+          }
+          fn(hit, u, j, S0, S1, S2, d0, d1, d2);
+        }
+        zs += len;
+      }
+    }
+  }
+}
+
+// ------------------------------------------------------------------ C6 factors
+// Softmax interpolation over the 7 reference CNs and the rank-r factors
+// c_r = sum_p w_p V[s, p, r] (core.py:449-478, 525-532), its CN derivative and the self
+// term sum_r lambda_r c_r^2 phi_ss(0) (core.py:545-550). Whole warp, lane-parallel.
+__device__ __forceinline__ double c6_factors_warp(double cn_raw, int s, const Tables* __restrict__ tab,
+                                                  const double* __restrict__ V, int R, double* __restrict__ c6,
+                                                  double* __restrict__ dc6, double* cn_out) {
+  const int lane = threadIdx.x & 31;
+  double cn = cn_raw, slope = 1.0;
+  if (tab->has_cncorr) {
+    slope = tab->cncorr[2 * s + 1];
+    cn = slope * cn_raw + tab->cncorr[2 * s + 0];
+  }
+  double logit = -INFINITY, dl = 0.0;
+  bool valid = false;
+  if (lane < 7) {
+    const double ref = tab->cnref[7 * s + lane];
+    valid = ref != -1.0;
+    const double diff = cn - ref;
+    if (valid) {
+      logit = -4.0 * (diff * diff);
+      dl = -8.0 * diff;
+    }
+  }
+  const double mx = warp_max(logit);
+  const double e = valid ? exp(logit - mx) : 0.0;
+  const double w = e / warp_sum(e);
+  const double dlbar = warp_sum(w * dl);
+  const double wd = w * (dl - dlbar);
+  double wp[7], wdp[7];
+#pragma unroll
+  for (int p = 0; p < 7; ++p) {
+    wp[p] = __shfl_sync(0xffffffffu, w, p);
+    wdp[p] = __shfl_sync(0xffffffffu, wd, p);
+  }
+  double selfv = 0.0;
+  for (int r = lane; r < R; r += 32) {
+    double c = 0.0, dc = 0.0;
+#pragma unroll
+    for (int p = 0; p < 7; ++p) {
+      const double v = V[(7 * s + p) * R + r];
+      c += wp[p] * v;
+      dc += wdp[p] * v;
+    }
+    c6[r] = c;
+    dc6[r] = slope * dc;
+    selfv += tab->eigs[r] * c * c * tab->selfcont[s];
+  }
+  if (lane == 0 && cn_out) *cn_out = cn;
+  return warp_sum(selfv);
+}
+
+constexpr int kWarpsPerBlock = 8;
+
+__global__ void __launch_bounds__(256) k_cn_c6_cells(GridDev g, int n, const int* __restrict__ bin_start,
+                                                    const double4* __restrict__ xs, const int4* __restrict__ meta,
+                                                    const int4* __restrict__ off, const Tables* __restrict__ tab,
+                                                    const double* __restrict__ V, int R, double* __restrict__ cn,
+                                                    double* __restrict__ c6, double* __restrict__ dc6,
+                                                    double* __restrict__ self_part) {
+  __shared__ double wsum[kWarpsPerBlock];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int t = blockIdx.x * kWarpsPerBlock + wid;
+  double selfv = 0.0;
+  if (t < n) {
+    const double4 xi = xs[t];
+    const int i = meta[t].w;
+    const int4 offi = off[i];
+    const int si = (int)xi.w;
+    const double rci = tab->rcov[si];
+    const double rcut_b = tab->r_cut;
+    double acc = 0.0;
+    visit_neighbors(g, bin_start, xs, meta, i, xi.x, xi.y, xi.z, offi,
+                    [&](bool hit, int u, int j, int S0, int S1, int S2, double, double, double) {
+                      if (!hit) return;
+                      const double4 xj = xs[u];
+                      // Bohr vector exactly as the reference forms it: x*a2b, shift*a2b
+                      const double sh0 = (S0 * g.cell[0] + S1 * g.cell[3] + S2 * g.cell[6]) * kAngToBohr;
+                      const double sh1 = (S0 * g.cell[1] + S1 * g.cell[4] + S2 * g.cell[7]) * kAngToBohr;
+                      const double sh2 = (S0 * g.cell[2] + S1 * g.cell[5] + S2 * g.cell[8]) * kAngToBohr;
+                      const double v0 = xj.x * kAngToBohr - xi.x * kAngToBohr + sh0;
+                      const double v1 = xj.y * kAngToBohr - xi.y * kAngToBohr + sh1;
+                      const double v2 = xj.z * kAngToBohr - xi.z * kAngToBohr + sh2;
+                      const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+                      double f, df;
+                      cn_edge(r, rci + tab->rcov[(int)xj.w], rcut_b, f, df);
+                      acc += f;
+                    });
+    const double cn_raw = warp_sum(acc);
+    selfv = c6_factors_warp(cn_raw, si, tab, V, R, c6 + (size_t)i * R, dc6 + (size_t)i * R, cn + i);
+  }
+  if (lane == 0) wsum[wid] = selfv;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < kWarpsPerBlock; ++w) s += wsum[w];
+    self_part[blockIdx.x] = s;
+  }
+}
+
+int launch_cn_c6_cells(const CellGrid& g, int n, const CellList& cl, const double* pos_ang,
+                       const int32_t* species, const Tables* tab, const double* eigvecs, int R, double* cn,
+                       double* c6, double* dc6, double* self_part, int* n_self_blocks, cudaStream_t s) {
+  (void)pos_ang;
+  (void)species;
+  const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  *n_self_blocks = blocks;
+  if (blocks == 0) return FD3_OK;
+  k_cn_c6_cells<<<blocks, 32 * kWarpsPerBlock, 0, s>>>(to_dev(g), n, cl.bin_start, cl.xs, cl.meta, cl.off, tab,
+                                                        eigvecs, R, cn, c6, dc6, self_part);
+  FD3_LAUNCHED();
+  return FD3_OK;
+}
+
+// CN adjoint: dE/dx_i = -sum_(j,S) (g_i + g_j) f'(r) d / r  (the list is symmetric), and the
+// strain virial W_ab = sum_i g_i sum_(j,S) f'(r) d_a d_b / r  (Bohr, Hartree).
+__global__ void __launch_bounds__(256) k_cn_adjoint_cells(GridDev g, int n, const int* __restrict__ bin_start,
+                                                         const double4* __restrict__ xs,
+                                                         const int4* __restrict__ meta, const int4* __restrict__ off,
+                                                         const Tables* __restrict__ tab,
+                                                         const double* __restrict__ gcn, double* __restrict__ grad,
+                                                         double out_scale, double* __restrict__ vir_part) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int t = blockIdx.x * kWarpsPerBlock + wid;
+  double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (t < n) {
+    const double4 xi = xs[t];
+    const int i = meta[t].w;
+    const int4 offi = off[i];
+    const int si = (int)xi.w;
+    const double rci = tab->rcov[si];
+    const double rcut_b = tab->r_cut;
+    const double gi = gcn[i];
+    double f0 = 0, f1 = 0, f2 = 0;
+    visit_neighbors(g, bin_start, xs, meta, i, xi.x, xi.y, xi.z, offi,
+                    [&](bool hit, int u, int j, int S0, int S1, int S2, double, double, double) {
+                      if (!hit) return;
+                      const double4 xj = xs[u];
+                      const double sh0 = (S0 * g.cell[0] + S1 * g.cell[3] + S2 * g.cell[6]) * kAngToBohr;
+                      const double sh1 = (S0 * g.cell[1] + S1 * g.cell[4] + S2 * g.cell[7]) * kAngToBohr;
+                      const double sh2 = (S0 * g.cell[2] + S1 * g.cell[5] + S2 * g.cell[8]) * kAngToBohr;
+                      const double v0 = xj.x * kAngToBohr - xi.x * kAngToBohr + sh0;
+                      const double v1 = xj.y * kAngToBohr - xi.y * kAngToBohr + sh1;
+                      const double v2 = xj.z * kAngToBohr - xi.z * kAngToBohr + sh2;
+                      const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+                      double f, df;
+                      cn_edge(r, rci + tab->rcov[(int)xj.w], rcut_b, f, df);
+                      if (r > 1e-6) {
+                        const double a = df / r;
+                        const double w = (gi + gcn[j]) * a;
+                        f0 -= w * v0;
+                        f1 -= w * v1;
+                        f2 -= w * v2;
+                        const double b = gi * a;
+                        v[0] += b * v0 * v0; v[1] += b * v0 * v1; v[2] += b * v0 * v2;
+                        v[4] += b * v1 * v1; v[5] += b * v1 * v2; v[8] += b * v2 * v2;
+                      }
+                    });
+    f0 = warp_sum(f0);
+    f1 = warp_sum(f1);
+    f2 = warp_sum(f2);
+    if (lane == 0) {
+      // grad holds the mesh part already; write (mesh + CN) scaled to the caller's unit
+      grad[3 * i] = out_scale * (grad[3 * i] + f0);
+      grad[3 * i + 1] = out_scale * (grad[3 * i + 1] + f1);
+      grad[3 * i + 2] = out_scale * (grad[3 * i + 2] + f2);
+    }
+  }
+  v[3] = v[1];
+  v[6] = v[2];
+  v[7] = v[5];
+  block_sum_store<9>(v, vir_part + 9 * blockIdx.x);
+}
+
+int launch_cn_adjoint_cells(const CellGrid& g, int n, const CellList& cl, const double* pos_ang,
+                            const int32_t* species, const Tables* tab, const double* gcn, double* grad,
+                            double out_scale, double* vir_part, int* n_blocks, cudaStream_t s) {
+  (void)pos_ang;
+  (void)species;
+  const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  *n_blocks = blocks;
+  if (blocks == 0) return FD3_OK;
+  k_cn_adjoint_cells<<<blocks, 32 * kWarpsPerBlock, 0, s>>>(to_dev(g), n, cl.bin_start, cl.xs, cl.meta, cl.off,
+                                                             tab, gcn, grad, out_scale, vir_part);
+  FD3_LAUNCHED();
+  return FD3_OK;
+}
+
+// ------------------------------------------------------------------ edge-list path
+__global__ void k_cn_edges(int64_t ne, const double* __restrict__ x, const int32_t* __restrict__ species,
+                           const int64_t* __restrict__ src, const int64_t* __restrict__ dst,
+                           const double* __restrict__ sh, const Tables* __restrict__ tab, double* __restrict__ cn) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const int64_t i = src[e], j = dst[e];
+  const double v0 = x[3 * j] - x[3 * i] + sh[3 * e];
+  const double v1 = x[3 * j + 1] - x[3 * i + 1] + sh[3 * e + 1];
+  const double v2 = x[3 * j + 2] - x[3 * i + 2] + sh[3 * e + 2];
+  const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+  double f, df;
+  cn_edge(r, tab->rcov[species[i]] + tab->rcov[species[j]], tab->r_cut, f, df);
+  atomicAdd(&cn[i], f);
+}
+
+int launch_cn_edges(int64_t n_edges, const double* pos, const int32_t* species, const int64_t* src,
+                    const int64_t* dst, const double* shift, const Tables* tab, double* cn, cudaStream_t s) {
+  if (n_edges == 0) return FD3_OK;
+  const int tb = 256;
+  k_cn_edges<<<(unsigned)((n_edges + tb - 1) / tb), tb, 0, s>>>(n_edges, pos, species, src, dst, shift, tab, cn);
+  FD3_LAUNCHED();
+  return FD3_OK;
+}
+
+__global__ void __launch_bounds__(256) k_c6_atoms(int n, const int32_t* __restrict__ species,
+                                                 const Tables* __restrict__ tab, const double* __restrict__ V, int R,
+                                                 double* __restrict__ cn, double* __restrict__ c6,
+                                                 double* __restrict__ dc6, double* __restrict__ self_part) {
+  __shared__ double wsum[kWarpsPerBlock];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int i = blockIdx.x * kWarpsPerBlock + wid;
+  double selfv = 0.0;
+  if (i < n) {
+    const double cn_raw = cn[i];
+    __syncwarp();
+    selfv = c6_factors_warp(cn_raw, species[i], tab, V, R, c6 + (size_t)i * R, dc6 + (size_t)i * R, cn + i);
+  }
+  if (lane == 0) wsum[wid] = selfv;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double s = 0.0;
+    for (int w = 0; w < kWarpsPerBlock; ++w) s += wsum[w];
+    self_part[blockIdx.x] = s;
+  }
+}
+
+int launch_c6_atoms(int n, const int32_t* species, const Tables* tab, const double* eigvecs, int R,
+                    const double* cn, double* c6, double* dc6, double* self_part, int* n_self_blocks,
+                    cudaStream_t s) {
+  const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  *n_self_blocks = blocks;
+  if (blocks == 0) return FD3_OK;
+  k_c6_atoms<<<blocks, 32 * kWarpsPerBlock, 0, s>>>(n, species, tab, eigvecs, R, const_cast<double*>(cn), c6, dc6,
+                                                     self_part);
+  FD3_LAUNCHED();
+  return FD3_OK;
+}
+
+__global__ void k_cn_adjoint_edges(int64_t ne, const double* __restrict__ x, const int32_t* __restrict__ species,
+                                   const int64_t* __restrict__ src, const int64_t* __restrict__ dst,
+                                   const double* __restrict__ sh, const Tables* __restrict__ tab,
+                                   const double* __restrict__ gcn, double* __restrict__ gpos,
+                                   double* __restrict__ gshift) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const int64_t i = src[e], j = dst[e];
+  const double v0 = x[3 * j] - x[3 * i] + sh[3 * e];
+  const double v1 = x[3 * j + 1] - x[3 * i + 1] + sh[3 * e + 1];
+  const double v2 = x[3 * j + 2] - x[3 * i + 2] + sh[3 * e + 2];
+  const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+  double f, df;
+  cn_edge(r, tab->rcov[species[i]] + tab->rcov[species[j]], tab->r_cut, f, df);
+  double g0 = 0, g1 = 0, g2 = 0;
+  if (r > 1e-6) {
+    const double a = gcn[i] * df / r;
+    g0 = a * v0;
+    g1 = a * v1;
+    g2 = a * v2;
+  }
+  if (gshift) {
+    gshift[3 * e] = g0;
+    gshift[3 * e + 1] = g1;
+    gshift[3 * e + 2] = g2;
+  }
+  if (gpos && (g0 != 0 || g1 != 0 || g2 != 0)) {
+    atomicAdd(&gpos[3 * j], g0);
+    atomicAdd(&gpos[3 * j + 1], g1);
+    atomicAdd(&gpos[3 * j + 2], g2);
+    atomicAdd(&gpos[3 * i], -g0);
+    atomicAdd(&gpos[3 * i + 1], -g1);
+    atomicAdd(&gpos[3 * i + 2], -g2);
+  }
+}
+
+int launch_cn_adjoint_edges(int64_t n_edges, const double* pos, const int32_t* species, const int64_t* src,
+                            const int64_t* dst, const double* shift, const Tables* tab, const double* gcn,
+                            double* gpos, double* gshift, cudaStream_t s) {
+  if (n_edges == 0) return FD3_OK;
+  const int tb = 256;
+  k_cn_adjoint_edges<<<(unsigned)((n_edges + tb - 1) / tb), tb, 0, s>>>(n_edges, pos, species, src, dst, shift, tab,
+                                                                       gcn, gpos, gshift);
+  FD3_LAUNCHED();
+  return FD3_OK;
+}
+
+// ------------------------------------------------------------------ neighbour export
+__global__ void __launch_bounds__(256) k_nbr_count(GridDev g, int n, const int* __restrict__ bin_start,
+                                                  const double4* __restrict__ xs, const int4* __restrict__ meta,
+                                                  const int4* __restrict__ off, int* __restrict__ counts) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int t = blockIdx.x * kWarpsPerBlock + wid;
+  if (t >= n) return;
+  const double4 xi = xs[t];
+  const int i = meta[t].w;
+  int cnt = 0;
+  visit_neighbors(g, bin_start, xs, meta, i, xi.x, xi.y, xi.z, off[i],
+                  [&](bool hit, int, int, int, int, int, double, double, double) {
+                    cnt += __popc(__ballot_sync(0xffffffffu, hit));
+                  });
+  if (lane == 0) counts[i] = cnt;
+}
+
+__global__ void __launch_bounds__(256) k_nbr_fill(GridDev g, int n, const int* __restrict__ bin_start,
+                                                 const double4* __restrict__ xs, const int4* __restrict__ meta,
+                                                 const int4* __restrict__ off, const int* __restrict__ row_start,
+                                                 int64_t* __restrict__ src, int64_t* __restrict__ dst,
+                                                 int32_t* __restrict__ shift) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int t = blockIdx.x * kWarpsPerBlock + wid;
+  if (t >= n) return;
+  const double4 xi = xs[t];
+  const int i = meta[t].w;
+  int pos = row_start[i];
+  visit_neighbors(g, bin_start, xs, meta, i, xi.x, xi.y, xi.z, off[i],
+                  [&](bool hit, int, int j, int S0, int S1, int S2, double, double, double) {
+                    const unsigned m = __ballot_sync(0xffffffffu, hit);
+                    if (hit) {
+                      const int k = pos + __popc(m & ((1u << lane) - 1u));
+                      src[k] = i;
+                      dst[k] = j;
+                      shift[3 * k] = S0;
+                      shift[3 * k + 1] = S1;
+                      shift[3 * k + 2] = S2;
+                    }
+                    pos += __popc(m);
+                  });
+}
+
+int launch_nbr_count(const CellGrid& g, int n, const CellList& cl, const double* pos_ang, int* counts,
+                     cudaStream_t s) {
+  (void)pos_ang;
+  const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  if (blocks == 0) return FD3_OK;
+  k_nbr_count<<<blocks, 32 * kWarpsPerBlock, 0, s>>>(to_dev(g), n, cl.bin_start, cl.xs, cl.meta, cl.off, counts);
+  FD3_LAUNCHED();
+  return FD3_OK;
+}
+
+int launch_nbr_fill(const CellGrid& g, int n, const CellList& cl, const double* pos_ang, const int* row_start,
+                    int64_t* src, int64_t* dst, int32_t* shift, cudaStream_t s) {
+  (void)pos_ang;
+  const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  if (blocks == 0) return FD3_OK;
+  k_nbr_fill<<<blocks, 32 * kWarpsPerBlock, 0, s>>>(to_dev(g), n, cl.bin_start, cl.xs, cl.meta, cl.off, row_start,
+                                                     src, dst, shift);
+  FD3_LAUNCHED();
+  return FD3_OK;
+}
+
+}  // namespace fd3

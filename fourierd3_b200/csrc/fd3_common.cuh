@@ -1,0 +1,213 @@
+// Shared device helpers for the FourierD3 sm_100a kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/fd3.h"
+
+#define FD3_WARP 32
+#define FD3_MAX_SPECIES 64
+#define FD3_MAX_RANK 32
+#define FD3_MAX_ORDER 8
+
+namespace fd3 {
+
+constexpr double kPi = 3.14159265358979323846;
+constexpr double kAngToBohr = 1.0 / 0.52917726;   // core.py:120
+constexpr double kHartreeToEv = 27.21138505;      // calculator.py:54
+
+// Cell-derived quantities, computed on the device from the (possibly strained) cell.
+struct CellInfo {
+  double cell[9];   // rows = lattice vectors, Bohr
+  double inv[9];    // adjugate / determinant inverse (utils.py:142-167)
+  double recip[9];  // rows b_i = 2 pi inv[:, i]
+  double volume;    // |det| (utils.py:130-139)
+  double pad[5];
+};
+
+// Per species-pair constants of the BJ Green's function (pair_pot.py:63-105).
+struct GreenPair {
+  double R, qq, c6s1, c6s2, c6pre, c8s1, c8s2, c8pre;
+};
+
+// Device-resident per-plan tables (uploaded once by fd3_plan_create).
+struct Tables {
+  double rcov[FD3_MAX_SPECIES];
+  double cnref[FD3_MAX_SPECIES * 7];
+  double selfcont[FD3_MAX_SPECIES];          // phi_XX(0) (pair_pot.py:84-89)
+  double cncorr[FD3_MAX_SPECIES * 2];
+  double eigs[FD3_MAX_RANK];
+  double s6, s8, r_cut;
+  int n_species, n_rank, has_cncorr, pad;
+  // eigvecs (S,7,r) and the (S,S) GreenPair matrix follow in separate device arrays
+};
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+__device__ __forceinline__ double warp_max(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+// Block-wide sum of NV doubles into out[0..NV) (thread 0 writes). blockDim multiple of 32.
+template <int NV>
+__device__ void block_sum_store(double (&v)[NV], double* out) {
+  __shared__ double red[NV][32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    double s = warp_sum(v[k]);
+    if (lane == 0) red[k][wid] = s;
+  }
+  __syncthreads();
+  if (wid == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      double s = lane < nw ? red[k][lane] : 0.0;
+      s = warp_sum(s);
+      if (lane == 0) out[k] = s;
+    }
+  }
+  __syncthreads();
+}
+
+// Exact-order helpers: the neighbour predicate must not be contracted into FMAs.
+__device__ __forceinline__ double dmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double dadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double dsub(double a, double b) { return __dsub_rn(a, b); }
+
+// Smooth-cutoff CN edge function and its r-derivative (core.py:348-378).
+// r: distance (Bohr), rcs: rcov_i + rcov_j, rc: CN cutoff (Bohr).
+__device__ __forceinline__ void cn_edge(double r, double rcs, double rc, double& f, double& df) {
+  const double rs = fmax(r, 1e-6);
+  const double r1 = 0.5 * rcs + 0.5 * rc;
+  const bool outer = rs > r1;
+  const double coeff = outer ? rs : r1;
+  const double t = rc - coeff;
+  const double denom = t * t + 1e-6;
+  const double dd = coeff - r1;
+  const double k = 16.0 + dd * dd / denom;
+  const double ratio = (4.0 / 3.0) * rcs;
+  const double z = k * (ratio * (1.0 / rs) - 1.0);   // sigmoid argument
+  const double e = exp(-z);
+  const double s = 1.0 / (1.0 + e);
+  if (r > 1e-6) {
+    f = s;
+    // dk/dr on the outer branch; zero where the clamp or the inner branch is active
+    const double dk = outer ? (2.0 * dd / denom + dd * dd * 2.0 * t / (denom * denom)) : 0.0;
+    const double dz = dk * (ratio / rs - 1.0) - k * ratio / (rs * rs);
+    df = s * (1.0 - s) * dz;
+  } else {
+    f = 0.0;
+    df = 0.0;
+  }
+}
+
+// Order-p cardinal B-spline weights at the p stencil nodes for local coordinate x in
+// [-1/2, 1/2]: w[k] = M_p(1/2 - x + k); dw = dw/dx (Cox-de Boor recursion).
+template <int P, typename T>
+__device__ __forceinline__ void bspline(T x, T* w, T* dw) {
+  const T a = T(0.5) - x;
+  T m[P];
+  m[0] = T(1);
+#pragma unroll
+  for (int q = 2; q <= P; ++q) {
+    if (q == P) {
+      // derivative from M_{P-1}: d/da M_P(a+k) = M_{P-1}(a+k) - M_{P-1}(a+k-1)
+#pragma unroll
+      for (int k = 0; k < P; ++k) {
+        const T l = k < P - 1 ? m[k] : T(0);
+        const T r = k >= 1 ? m[k - 1] : T(0);
+        dw[k] = -(l - r);
+      }
+    }
+    T nm[P];
+#pragma unroll
+    for (int j = 0; j < q; ++j) {
+      const T u = a + T(j);
+      const T l = j < q - 1 ? m[j] : T(0);
+      const T r = j >= 1 ? m[j - 1] : T(0);
+      nm[j] = (u * l + (T(q) - u) * r) / T(q - 1);
+    }
+#pragma unroll
+    for (int j = 0; j < q; ++j) m[j] = nm[j];
+  }
+  if (P == 1) dw[0] = T(0);
+#pragma unroll
+  for (int k = 0; k < P; ++k) w[k] = m[k];
+}
+
+// p-point Lagrange basis on nodes 0..p-1 with the charge at t = x + (p-1)/2.
+template <int P, typename T>
+__device__ __forceinline__ void lagrange(T x, T* w, T* dw) {
+  const T t = x + T(0.5) * T(P - 1);
+#pragma unroll
+  for (int k = 0; k < P; ++k) {
+    T prod = T(1), der = T(0);
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+      if (m == k) continue;
+      const T f = (t - T(m)) / T(k - m);
+      der = der * f + prod / T(k - m);
+      prod = prod * f;
+    }
+    w[k] = prod;
+    dw[k] = der;
+  }
+}
+
+// Green's function G_XY(k) and dG/dk for one species pair (pair_pot.py:142-178).
+template <typename T>
+__device__ __forceinline__ void green_eval(const GreenPair& g, T k, T s6, T s8, T& G, T& dG) {
+  const T R = T(g.R);
+  const T ksq = k * k;
+  if (k * R < T(1e-15)) {
+    const T f6 = s6 * (T(g.c6s1) - T(g.c6s2) * ksq);
+    const T d6 = s6 * (T(-2) * T(g.c6s2) * k);
+    const T f8 = T(3) * s8 * (T(g.c8s1) - T(g.c8s2) * ksq);
+    const T d8 = T(3) * s8 * (T(-2) * T(g.c8s2) * k);
+    G = f6 + T(g.qq) * f8;
+    dG = d6 + T(g.qq) * d8;
+    return;
+  }
+  const T sq3 = T(1.7320508075688772935);
+  const T sin8 = T(0.38268343236508977173);   // sin(pi/8)
+  const T cos8 = T(0.92387953251128675613);   // cos(pi/8)
+  const T u = k * R;
+  const T e1 = exp(-u);
+  const T e2 = exp(-u / T(2));
+  T sa, ca;
+  sincos(T(kPi / 3) + u * sq3 / T(2), &sa, &ca);
+  const T n6 = e1 - T(2) * e2 * ca;
+  const T dn6 = -e1 + e2 * ca + sq3 * e2 * sa;
+  const T e3 = exp(-u * sin8);
+  const T e4 = exp(-u * cos8);
+  T s1, c1, s2, c2;
+  sincos(T(kPi / 4) + u * cos8, &s1, &c1);
+  sincos(T(3 * kPi / 4) + u * sin8, &s2, &c2);
+  const T n8 = e3 * c1 + e4 * c2;
+  const T dn8 = -sin8 * e3 * c1 - cos8 * e3 * s1 - cos8 * e4 * c2 - sin8 * e4 * s2;
+  const T invk = T(1) / k;
+  const T f6 = s6 * ((T(g.c6pre) * invk) * n6);
+  const T d6 = s6 * T(g.c6pre) * (R * dn6 * invk - n6 * invk * invk);
+  const T f8 = T(3) * s8 * ((T(g.c8pre) * invk) * n8);
+  const T d8 = T(3) * s8 * T(g.c8pre) * (R * dn8 * invk - n8 * invk * invk);
+  G = f6 + T(g.qq) * f8;
+  dG = d6 + T(g.qq) * d8;
+}
+
+// floor division / modulo for possibly negative ints
+__device__ __forceinline__ int floordiv(int a, int b) { return (a >= 0) ? a / b : -((-a + b - 1) / b); }
+__device__ __forceinline__ int posmod(int a, int b) { int m = a % b; return m < 0 ? m + b : m; }
+
+}  // namespace fd3

@@ -1,0 +1,8 @@
+// Explicit instantiation of the gather kernels for float32 (mixed precision) meshes (split for parallel compilation).
+#include "fd3_mesh_impl.cuh"
+
+namespace fd3 {
+template int launch_gather<float>(const MeshGeom&, int, const double*, double, const int32_t*, const double*,
+                                  const double*, const CellInfo*, const Tables*, const int*, const float*, double*,
+                                  double*, double*, int*, cudaStream_t);
+}  // namespace fd3

@@ -1,0 +1,124 @@
+// Internal declarations shared by the .cu files of libfd3 (not part of the ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cufft.h>
+#include <stdint.h>
+
+#include "fd3_common.cuh"
+
+namespace fd3 {
+
+// ---- error plumbing ---------------------------------------------------------
+void set_error(const char* where, const char* what);
+void count_launch();
+#define FD3_CUDA(call)                                            \
+  do {                                                            \
+    cudaError_t e_ = (call);                                      \
+    if (e_ != cudaSuccess) {                                      \
+      ::fd3::set_error(#call, cudaGetErrorString(e_));            \
+      return FD3_ECUDA;                                           \
+    }                                                             \
+  } while (0)
+#define FD3_LAUNCHED()                                            \
+  do {                                                            \
+    ::fd3::count_launch();                                        \
+    cudaError_t e_ = cudaGetLastError();                          \
+    if (e_ != cudaSuccess) {                                      \
+      ::fd3::set_error("kernel launch", cudaGetErrorString(e_));  \
+      return FD3_ECUDA;                                           \
+    }                                                             \
+  } while (0)
+
+// ---- cell list geometry ------------------------------------------------------
+struct CellGrid {
+  int nb[3];        // bins per axis
+  int reach[3];     // bins to visit on each side
+  double cell[9];   // Angstrom rows
+  double inv[9];    // Angstrom inverse (host-computed; only used for binning)
+  double rc2;       // r_cut^2 (Angstrom^2) for the exact predicate
+  double r_cut;
+};
+int make_cell_grid(const double* h_cell, double r_cut, CellGrid* g);
+
+// Device arrays of a built cell list (all sized from the plan workspace).
+struct CellList {
+  int* bin_of;      // [N]   bin id of each atom
+  int* bin_count;   // [K]   histogram (zeroed before use)
+  int* bin_start;   // [K+1] exclusive scan
+  int* order;       // [N]   atom ids sorted by bin, then by id
+  double4* xs;      // [N]   bin-sorted positions (A) + species in .w
+  int4* meta;       // [N]   bin-sorted {off_x, off_y, off_z, atom id}
+  int4* off;        // [N]   per atom {off_x, off_y, off_z, bin}
+};
+
+// counting sort of keys[N] in [0, K): out order sorted by key then by index.
+// counts[K] and starts[K+1] are workspace; counts must be zeroed by the caller.
+int counting_sort(const int* keys, int n, int K, int* counts, int* starts, int* order, cudaStream_t s);
+int scan_exclusive(const int* in, int n, int* out, cudaStream_t s);   // out[n] = total
+
+int build_cell_list(const CellGrid& g, int n, const double* pos_ang, const int32_t* species, CellList& cl,
+                    cudaStream_t s);
+
+// fused CN + C6 factors over the cell list (warp per atom)
+int launch_cn_c6_cells(const CellGrid& g, int n, const CellList& cl, const double* pos_ang,
+                       const int32_t* species, const Tables* tab, const double* eigvecs, int R, double* cn,
+                       double* c6, double* dc6, double* self_part, int* n_self_blocks, cudaStream_t s);
+// CN adjoint over the cell list: grad += dE/dx (Hartree/Bohr); virial partials (9 per block)
+int launch_cn_adjoint_cells(const CellGrid& g, int n, const CellList& cl, const double* pos_ang,
+                            const int32_t* species, const Tables* tab, const double* gcn, double* grad,
+                            double out_scale, double* vir_part, int* n_blocks, cudaStream_t s);
+
+// edge-list CN path
+int launch_cn_edges(int64_t n_edges, const double* pos, const int32_t* species, const int64_t* src,
+                    const int64_t* dst, const double* shift, const Tables* tab, double* cn, cudaStream_t s);
+int launch_c6_atoms(int n, const int32_t* species, const Tables* tab, const double* eigvecs, int R,
+                    const double* cn, double* c6, double* dc6, double* self_part, int* n_self_blocks,
+                    cudaStream_t s);
+int launch_cn_adjoint_edges(int64_t n_edges, const double* pos, const int32_t* species, const int64_t* src,
+                            const int64_t* dst, const double* shift, const Tables* tab, const double* gcn,
+                            double* gpos, double* gshift, cudaStream_t s);
+
+// neighbour export
+int launch_nbr_count(const CellGrid& g, int n, const CellList& cl, const double* pos_ang, int* counts,
+                     cudaStream_t s);
+int launch_nbr_fill(const CellGrid& g, int n, const CellList& cl, const double* pos_ang, const int* row_start,
+                    int64_t* src, int64_t* dst, int32_t* shift, cudaStream_t s);
+
+// ---- mesh ---------------------------------------------------------------------
+struct MeshGeom {
+  int n[3];       // mesh points per axis
+  int nzh;        // nz/2 + 1
+  int t[3];       // tile edge per axis (divides n)
+  int nt[3];      // tiles per axis
+  int ns[3];      // source tiles per axis that can reach a tile
+  int order;      // p
+  int lagrange;   // 0: B-spline (spme), 1: Lagrange (pme)
+  int S, R;
+};
+int launch_cellinfo(const double* cell, double scale, CellInfo* ci, cudaStream_t s);
+int launch_mesh_keys(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
+                     const CellInfo* ci, int* keys, cudaStream_t s);
+template <typename T>
+int launch_spread(const MeshGeom& mg, const double* pos, double pos_scale, const int32_t* species,
+                  const double* c6, const CellInfo* ci, const int* key_start, const int* order, T* rho,
+                  cudaStream_t s);
+template <typename T>
+int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab,
+                  const float* deconv, int spme, void* spec, double* part, int* n_blocks, cudaStream_t s);
+template <typename T>
+int launch_gather(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
+                  const double* c6, const double* dc6, const CellInfo* ci, const Tables* tab, const int* order,
+                  const T* phi, double* gcn, double* gpos, double* mcell_part, int* n_blocks, cudaStream_t s);
+
+// ---- finalisation ---------------------------------------------------------------
+struct Partials {
+  const double* self;  int n_self;     // 1 value per block
+  const double* kspc;  int n_kspc;     // 7 per block: q, V00 V11 V22 V01 V02 V12
+  const double* cnv;   int n_cnv;      // 9 per block (CN virial), may be 0
+  const double* mcell; int n_mcell;    // 9 per block: sum_i s_iA g_ia, may be 0
+};
+int launch_finalize(const Partials& p, const CellInfo* ci, int mode, double e_scale, double* energy,
+                    double* out9, cudaStream_t s);
+
+}  // namespace fd3

@@ -1,0 +1,255 @@
+"""Plan + workspace owner around the C ABI (one per model / structure shape).
+
+``Engine`` holds one ``fd3_plan`` (per-species tables, cuFFT plans) and a cached
+device workspace allocated through PyTorch's caching allocator; it exposes the two
+compute entry points of include/fd3.h:
+
+* ``energy_edges``  -- the reference module surface: energy and its gradients with
+  respect to Bohr positions, Bohr shift vectors and the Bohr cell, from a
+  caller-supplied edge list (src/fourierd3/core.py:480-583);
+* ``energy_forces_stress`` -- the fused calculator path: device cell-list neighbour
+  search + CN + C6 factors + SPME/PME + adjoints, returning eV, eV/A, eV/A^3
+  (src/fourierd3/calculator.py:125-192).
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional, Sequence
+
+import numpy as np
+import torch
+
+from fourierd3_b200 import _native, geometry, tables
+
+PBE_BJ = (1.0, 0.7875, 0.4289, 4.4407)   # src/fourierd3/core.py:168
+
+
+@dataclass
+class SpeciesSetup:
+    """Species remapping and per-species tables (src/fourierd3/core.py:102-161)."""
+
+    types: tuple           # sorted unique atomic numbers
+    species: np.ndarray    # compact ids (N,) int32
+    eigs: np.ndarray       # (r,)
+    eigvecs: np.ndarray    # (S*7, r)
+    rcov: np.ndarray       # (S,) Bohr, float32 values widened (core.py:152)
+    cnref: np.ndarray      # (S, 7)
+    sqrtq: np.ndarray      # (S,)
+    c6_err: float
+
+    @property
+    def n_species(self) -> int:
+        return len(self.types)
+
+    @property
+    def n_rank(self) -> int:
+        return int(self.eigs.shape[0])
+
+
+def species_setup(numbers: Sequence[int], c6tol: float) -> SpeciesSetup:
+    numbers = np.asarray(numbers).astype(np.int64)
+    uniq = np.unique(numbers)
+    remap = {int(z): i for i, z in enumerate(uniq)}
+    species = np.array([remap[int(z)] for z in numbers], dtype=np.int32)
+    eigs, vecs, err = tables.species_setup(tuple(int(z) for z in uniq), float(c6tol))
+    t = tables.load_tables()
+    return SpeciesSetup(
+        types=tuple(int(z) for z in uniq), species=species,
+        eigs=np.ascontiguousarray(eigs, dtype=np.float64),
+        eigvecs=np.ascontiguousarray(vecs, dtype=np.float64),
+        rcov=t["rcov"][uniq].astype(np.float64), cnref=t["cnref"][uniq].astype(np.float64),
+        sqrtq=t["sqrtQz"][uniq].astype(np.float64), c6_err=float(err))
+
+
+def _stream_ptr(device: torch.device) -> int:
+    return torch.cuda.current_stream(device).cuda_stream
+
+
+class Engine:
+    """One fd3 plan for a fixed species set, method, mesh and precision."""
+
+    def __init__(self, setup: SpeciesSetup, *, method: str, order: int, mesh: Sequence[int],
+                 ewald_ns: Sequence[int] = (0, 0, 0), precision: str = "fp64", r_cut_bohr: float,
+                 params: Sequence[float] = PBE_BJ, cncorr: Optional[np.ndarray] = None,
+                 device: torch.device):
+        if device.type != "cuda":
+            raise RuntimeError("fourierd3_b200 computes on CUDA devices only (B200, sm_100a)")
+        if method not in _native.METHODS:
+            raise ValueError(f"unknown method {method!r}; expected 'spme', 'pme' or 'ewald'")
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("precision must be 'fp64' or 'mixed'")
+        self.setup = setup
+        self.method = method
+        self.order = int(order)
+        self.mesh = tuple(int(v) for v in mesh)
+        self.precision = precision
+        self.device = device
+        self._keep = []  # numpy arrays referenced by the descriptor until create returns
+        d = _native.PlanDesc()
+        d.n_species = setup.n_species
+        d.n_rank = setup.n_rank
+        d.method = _native.METHODS[method]
+        d.order = self.order
+        for a in range(3):
+            d.mesh[a] = self.mesh[a]
+            d.ewald_ns[a] = int(ewald_ns[a])
+        d.precision = _native.PREC_FP64 if precision == "fp64" else _native.PREC_MIXED
+        d.r_cut = float(r_cut_bohr)
+        for k in range(4):
+            d.params[k] = float(params[k])
+
+        def keep(a, dt=np.float64):
+            a = np.ascontiguousarray(a, dtype=dt)
+            self._keep.append(a)
+            return a
+
+        d.rcov = _native.dptr(keep(setup.rcov))
+        d.cnref = _native.dptr(keep(setup.cnref))
+        d.eigvecs = _native.dptr(keep(setup.eigvecs))
+        d.eigs = _native.dptr(keep(setup.eigs))
+        d.sqrtq = _native.dptr(keep(setup.sqrtq))
+        if cncorr is not None:
+            d.has_cncorr = 1
+            d.cncorr = _native.dptr(keep(np.asarray(cncorr, dtype=np.float64).reshape(-1, 2)))
+        if method == "spme":
+            win = keep(geometry.spme_window(self.mesh, self.order), np.float32)
+            d.deconv = win.ctypes.data_as(ctypes.POINTER(ctypes.c_float))
+        self._plan = ctypes.c_void_p()
+        lib = _native.lib()
+        with torch.cuda.device(device):
+            _native.check(lib.fd3_plan_create(ctypes.byref(d), ctypes.byref(self._plan)), "fd3_plan_create")
+        self._keep = []
+        self._work = None
+        self._species_dev = None
+
+    def __del__(self):
+        plan = getattr(self, "_plan", None)
+        if plan is not None and plan.value:
+            try:
+                _native.lib().fd3_plan_destroy(plan)
+            except Exception:
+                pass
+
+    # ------------------------------------------------------------------ helpers
+    def species_tensor(self) -> torch.Tensor:
+        if self._species_dev is None:
+            self._species_dev = torch.as_tensor(self.setup.species, dtype=torch.int32, device=self.device)
+        return self._species_dev
+
+    def workspace(self, n_atoms: int, n_bins: int) -> torch.Tensor:
+        nbytes = ctypes.c_size_t()
+        _native.check(_native.lib().fd3_workspace_size(self._plan, n_atoms, n_bins, ctypes.byref(nbytes)),
+                      "fd3_workspace_size")
+        if self._work is None or self._work.numel() < nbytes.value:
+            self._work = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
+        return self._work
+
+    @staticmethod
+    def cell_grid(cell_ang: np.ndarray, r_cut_ang: float):
+        c = np.ascontiguousarray(cell_ang, dtype=np.float64).reshape(9)
+        nb = (ctypes.c_int32 * 3)()
+        rr = (ctypes.c_int32 * 3)()
+        _native.check(_native.lib().fd3_cell_grid(_native.dptr(c), float(r_cut_ang), nb, rr), "fd3_cell_grid")
+        return tuple(nb), tuple(rr)
+
+    def profile(self, on: bool = True) -> None:
+        """Record CUDA events between pipeline stages of the following calls."""
+        _native.check(_native.lib().fd3_profile_enable(self._plan, 1 if on else 0), "fd3_profile_enable")
+
+    def stage_times(self) -> dict:
+        """{stage name: milliseconds} of the last call (waits for its last event)."""
+        ms = (ctypes.c_double * 24)()
+        names = ctypes.create_string_buffer(512)
+        n = ctypes.c_int32()
+        _native.check(_native.lib().fd3_profile_read(self._plan, ms, 24, names, 512, ctypes.byref(n)),
+                      "fd3_profile_read")
+        keys = names.value.decode().split(",") if n.value else []
+        out: dict = {}
+        for k, v in zip(keys, list(ms)[: n.value]):
+            out[k] = out.get(k, 0.0) + v
+        return out
+
+    # ------------------------------------------------------------------ entry points
+    def energy_edges(self, pos_b: torch.Tensor, cell_b: torch.Tensor, edge_index: torch.Tensor,
+                     shifts_b: torch.Tensor, need_grad: bool):
+        """Returns (energy [Ha], dE/dpos, dE/dshift, dE/dcell) -- gradients None if not need_grad."""
+        n = pos_b.shape[0]
+        e = edge_index.shape[1]
+        pos = pos_b.detach().to(torch.float64).contiguous()
+        cell = cell_b.detach().to(torch.float64).contiguous()
+        sh = shifts_b.detach().to(torch.float64).contiguous()
+        ei = edge_index.to(torch.int64).contiguous()
+        src, dst = ei[0], ei[1]
+        energy = torch.empty((), dtype=torch.float64, device=self.device)
+        gpos = torch.empty_like(pos) if need_grad else None
+        gsh = torch.empty_like(sh) if need_grad else None
+        gcell = torch.empty((3, 3), dtype=torch.float64, device=self.device) if need_grad else None
+        work = self.workspace(n, 1)
+
+        def ptr(t):
+            return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else None
+
+        rc = _native.lib().fd3_energy_edges(
+            self._plan, n, ptr(pos), ptr(self.species_tensor()), ptr(cell), e, ptr(src), ptr(dst), ptr(sh),
+            1 if need_grad else 0, ptr(work), work.numel(), ptr(energy), ptr(gpos), ptr(gsh), ptr(gcell),
+            ctypes.c_void_p(_stream_ptr(self.device)))
+        _native.check(rc, "fd3_energy_edges")
+        return energy, gpos, gsh, gcell
+
+    def energy_forces_stress(self, pos_ang: torch.Tensor, cell_ang: np.ndarray, r_cut_ang: float,
+                             cell_dev: Optional[torch.Tensor] = None, out=None):
+        """Fused path. Returns (energy [eV], forces [eV/A], stress [eV/A^3] 3x3)."""
+        n = pos_ang.shape[0]
+        cell_h = np.ascontiguousarray(cell_ang, dtype=np.float64).reshape(9)
+        (nb, _) = self.cell_grid(cell_h, r_cut_ang)
+        work = self.workspace(n, nb[0] * nb[1] * nb[2])
+        if cell_dev is None:
+            cell_dev = torch.as_tensor(cell_h, dtype=torch.float64).to(self.device, non_blocking=False)
+        if out is None:
+            energy = torch.empty((), dtype=torch.float64, device=self.device)
+            forces = torch.empty((n, 3), dtype=torch.float64, device=self.device)
+            stress = torch.empty((3, 3), dtype=torch.float64, device=self.device)
+        else:
+            energy, forces, stress = out
+        rc = _native.lib().fd3_energy_forces_stress(
+            self._plan, n, ctypes.c_void_p(pos_ang.data_ptr()), ctypes.c_void_p(self.species_tensor().data_ptr()),
+            _native.dptr(cell_h), ctypes.c_void_p(cell_dev.data_ptr()), float(r_cut_ang),
+            ctypes.c_void_p(work.data_ptr()), work.numel(), ctypes.c_void_p(energy.data_ptr()),
+            ctypes.c_void_p(forces.data_ptr()), ctypes.c_void_p(stress.data_ptr()),
+            ctypes.c_void_p(_stream_ptr(self.device)))
+        _native.check(rc, "fd3_energy_forces_stress")
+        return energy, forces, stress
+
+
+def neighbour_list(positions: torch.Tensor, cell_ang: np.ndarray, r_cut: float):
+    """GPU replacement of matscipy ``neighbour_list("ijS")`` (calculator.py:94-123).
+
+    Returns (i, j, S) device tensors (int64, int64, int32 (E, 3)), rows sorted by i.
+    """
+    if positions.device.type != "cuda":
+        raise RuntimeError("neighbour_list runs on CUDA devices only")
+    lib = _native.lib()
+    pos = positions.detach().to(torch.float64).contiguous()
+    n = pos.shape[0]
+    cell_h = np.ascontiguousarray(cell_ang, dtype=np.float64).reshape(9)
+    nbytes = ctypes.c_size_t()
+    _native.check(lib.fd3_neighbor_workspace_size(n, _native.dptr(cell_h), float(r_cut), ctypes.byref(nbytes)),
+                  "fd3_neighbor_workspace_size")
+    work = torch.empty(int(nbytes.value), dtype=torch.uint8, device=pos.device)
+    stream = ctypes.c_void_p(_stream_ptr(pos.device))
+    count = ctypes.c_int64()
+    _native.check(lib.fd3_neighbor_count(n, ctypes.c_void_p(pos.data_ptr()), _native.dptr(cell_h), float(r_cut),
+                                         ctypes.c_void_p(work.data_ptr()), work.numel(), ctypes.byref(count), stream),
+                  "fd3_neighbor_count")
+    cap = int(count.value)
+    src = torch.empty(max(cap, 1), dtype=torch.int64, device=pos.device)
+    dst = torch.empty(max(cap, 1), dtype=torch.int64, device=pos.device)
+    sh = torch.empty((max(cap, 1), 3), dtype=torch.int32, device=pos.device)
+    _native.check(lib.fd3_neighbor_fill(n, ctypes.c_void_p(pos.data_ptr()), _native.dptr(cell_h), float(r_cut),
+                                        ctypes.c_void_p(work.data_ptr()), work.numel(), cap,
+                                        ctypes.c_void_p(src.data_ptr()), ctypes.c_void_p(dst.data_ptr()),
+                                        ctypes.c_void_p(sh.data_ptr()), ctypes.byref(count), stream),
+                  "fd3_neighbor_fill")
+    m = int(count.value)
+    return src[:m], dst[:m], sh[:m]

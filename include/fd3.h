@@ -1,0 +1,153 @@
+/*
+ * fd3.h -- C ABI of the B200 FourierD3 dispersion library (libfd3.so).
+ *
+ * The library evaluates the DFT-D3(BJ) dispersion energy of a 3D-periodic box in
+ * reciprocal space from a low-rank C6 decomposition, together with its exact
+ * derivatives (forces, cell gradient / virial), on one NVIDIA B200 (sm_100a).
+ *
+ * Conventions
+ *   - Every pointer argument named d_* is DEVICE memory owned by the caller; h_* is
+ *     host memory. No function allocates device memory except fd3_plan_create (small
+ *     per-species tables and cuFFT plan handles). All large scratch lives in a caller
+ *     supplied workspace whose size fd3_workspace_size returns.
+ *   - Work is stream-ordered on the caller's stream; nothing synchronises the host
+ *     except fd3_neighbor_count (returns the edge count) and fd3_plan_create.
+ *   - Internal length unit Bohr (1 A = 1/0.52917726 Bohr), energy unit Hartree,
+ *     except where an argument says Angstrom.
+ *   - Status codes: FD3_OK on success; no C++ exception crosses this boundary.
+ *   - A plan is not thread-safe; use one plan per stream.
+ */
+#ifndef FD3_H
+#define FD3_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define FD3_API __attribute__((visibility("default")))
+#else
+#define FD3_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  FD3_OK = 0,
+  FD3_EINVAL = 1,     /* bad argument (shape, range, unsupported option)          */
+  FD3_ECAPACITY = 2,  /* output capacity too small; the needed size is written back */
+  FD3_ECUDA = 3,      /* a CUDA runtime call failed                               */
+  FD3_ECUFFT = 4,     /* a cuFFT call failed                                      */
+  FD3_ENOMEM = 5,     /* workspace smaller than fd3_workspace_size                */
+} fd3_status;
+
+enum { FD3_METHOD_SPME = 0, FD3_METHOD_PME = 1, FD3_METHOD_EWALD = 2 };
+enum { FD3_PREC_FP64 = 0, FD3_PREC_MIXED = 1 };
+
+typedef struct fd3_plan fd3_plan;
+
+/* Everything the reference fixes at model construction (src/fourierd3/core.py:50-242).
+ * Table arrays are host pointers, copied by fd3_plan_create. */
+typedef struct {
+  int32_t n_species;      /* S: unique elements present                           */
+  int32_t n_rank;         /* r: rank of the C6 decomposition (utils.py:35-73)      */
+  int32_t method;         /* FD3_METHOD_*  (core.py:184-242)                       */
+  int32_t order;          /* p: interpolation nodes per axis, 1..8 (spme / pme)    */
+  int32_t mesh[3];        /* nx, ny, nz (spme / pme; core.py:186)                  */
+  int32_t ewald_ns[3];    /* Miller-index box (ewald; core.py:228-230)             */
+  int32_t precision;      /* FD3_PREC_*                                            */
+  int32_t has_cncorr;     /* 1: apply cncorr (core.py:383-384)                     */
+  double r_cut;           /* CN cutoff in Bohr (core.py:121)                       */
+  double params[4];       /* s6, s8, a1, a2 (core.py:165-170)                      */
+  const double* rcov;     /* [S]      covalent radii, Bohr (core.py:152)           */
+  const double* cnref;    /* [S*7]    reference CNs, -1 = unused (core.py:155)     */
+  const double* eigvecs;  /* [S*7*r]  V reshaped (S, 7, r) (core.py:148)           */
+  const double* eigs;     /* [r]      lambda (core.py:139-142)                     */
+  const double* sqrtq;    /* [S]      sqrt(Q) (pair_pot.py:53)                     */
+  const double* cncorr;   /* [S*2]    columns [b, a] or NULL                       */
+  const float* deconv;    /* [nx*ny*(nz/2+1)] the float32 SPME window
+                             sinc^(2p) clamped at 1e-10, exactly as the reference
+                             builds it (pair_pot.py:180-207); NULL: evaluate it in
+                             float64 inside the filter kernel instead            */
+} fd3_plan_desc;
+
+/* Replaces: FourierD3.__init__ buffers + KSpaceFilterD3 / MeshInterpolatorD3 /
+ * D3Potential construction (src/fourierd3/core.py:50-242). */
+FD3_API int fd3_plan_create(const fd3_plan_desc* desc, fd3_plan** out);
+FD3_API int fd3_plan_destroy(fd3_plan* plan);
+
+/* Workspace bytes for a call with n_atoms atoms. n_bins: cell-list bins of the
+ * fused path (0 for the edge path; see fd3_cell_grid). */
+FD3_API int fd3_workspace_size(const fd3_plan* plan, int64_t n_atoms, int64_t n_bins, size_t* bytes);
+
+/* Cell-list geometry for a box: bins per axis and the bin reach (A). */
+FD3_API int fd3_cell_grid(const double* h_cell_ang, double r_cut_ang, int32_t* nbins3, int32_t* reach3);
+
+/*
+ * Energy and gradients from a caller-supplied edge list -- the reference's module
+ * surface FourierD3.forward(positions, edge_index, shifts) (core.py:480-583) whose
+ * autograd the reference relies on (calculator.py:177-188).
+ *   d_pos      [N*3]  positions, Bohr
+ *   d_species  [N]    compact species ids 0..S-1 (core.py:104-114)
+ *   d_cell     [9]    cell rows, Bohr
+ *   d_src,d_dst[E]    edge_index rows (int64)
+ *   d_shift    [E*3]  Cartesian shift vectors, Bohr
+ * outputs (any gradient pointer may be NULL when need_grad == 0):
+ *   d_energy   [1]    energy, Hartree
+ *   d_gpos     [N*3]  dE/dpos      (Hartree/Bohr)
+ *   d_gshift   [E*3]  dE/dshift    (Hartree/Bohr)
+ *   d_gcell    [9]    dE/dcell     (Hartree/Bohr), positions and shifts held fixed
+ */
+FD3_API int fd3_energy_edges(fd3_plan* plan, int64_t n_atoms, const double* d_pos, const int32_t* d_species,
+                     const double* d_cell, int64_t n_edges, const int64_t* d_src, const int64_t* d_dst,
+                     const double* d_shift, int32_t need_grad, void* d_work, size_t work_bytes,
+                     double* d_energy, double* d_gpos, double* d_gshift, double* d_gcell, void* stream);
+
+/*
+ * Fused energy + forces + stress with the neighbour search done on the device by a
+ * cell list (no edge list is materialised) -- the ASE calculator path
+ * FourierD3ASECalculator.calculate (calculator.py:125-192) including its matscipy
+ * neighbour build (calculator.py:94-123).
+ *   d_pos_ang [N*3]  positions, Angstrom;  h_cell_ang [9] cell rows, Angstrom (host)
+ *   d_cell_ang [9]   the same cell on the device
+ *   r_cut_ang        neighbour cutoff (the pair predicate uses Angstrom, as matscipy)
+ * outputs: d_energy [1] eV, d_forces [N*3] eV/A, d_stress [9] eV/A^3 (ASE sign)
+ */
+FD3_API int fd3_energy_forces_stress(fd3_plan* plan, int64_t n_atoms, const double* d_pos_ang,
+                             const int32_t* d_species, const double* h_cell_ang, const double* d_cell_ang,
+                             double r_cut_ang, void* d_work, size_t work_bytes, double* d_energy,
+                             double* d_forces, double* d_stress, void* stream);
+
+/*
+ * Neighbour list export (replaces matscipy.neighbours.neighbour_list("ijS"),
+ * calculator.py:94-123): all directed pairs (i, j, S) with
+ * |x_j - x_i + S.cell| < r_cut, both directions, self-images included, (i,i,0) excluded.
+ * fd3_neighbor_count synchronises the stream and returns the pair count; fd3_neighbor_fill
+ * writes rows sorted by i (within a row: cell-list order). h_capacity < count gives
+ * FD3_ECAPACITY with the needed count in *h_count.
+ */
+FD3_API int fd3_neighbor_workspace_size(int64_t n_atoms, const double* h_cell_ang, double r_cut_ang, size_t* bytes);
+FD3_API int fd3_neighbor_count(int64_t n_atoms, const double* d_pos_ang, const double* h_cell_ang, double r_cut_ang,
+                       void* d_work, size_t work_bytes, int64_t* h_count, void* stream);
+FD3_API int fd3_neighbor_fill(int64_t n_atoms, const double* d_pos_ang, const double* h_cell_ang, double r_cut_ang,
+                      void* d_work, size_t work_bytes, int64_t capacity, int64_t* d_src, int64_t* d_dst,
+                      int32_t* d_shift, int64_t* h_count, void* stream);
+
+/* Per-stage timing of the last call on this plan, from CUDA events recorded on the
+ * launching stream between stages (cell_list, cn_c6, mesh_sort, spread, fft_r2c,
+ * filter, fft_c2r, gather, cn_adjoint, finalize). fd3_profile_read waits for the last
+ * event, writes milliseconds per stage and a comma-separated list of stage names. */
+FD3_API int fd3_profile_enable(fd3_plan* plan, int32_t on);
+FD3_API int fd3_profile_read(fd3_plan* plan, double* ms, int32_t max_stages, char* names, int32_t names_len,
+                             int32_t* n_stages);
+
+/* Last CUDA / cuFFT error text of the calling thread (static storage). */
+FD3_API const char* fd3_last_error(void);
+/* Number of kernel launches this library issued since load (for launch accounting). */
+FD3_API int64_t fd3_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FD3_H */

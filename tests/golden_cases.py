@@ -1,0 +1,27 @@
+"""Loader for the golden fixtures in tests/golden/ (made by tests/golden/make_golden.py)."""
+import glob
+import json
+import os
+
+import numpy as np
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def names():
+    return sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(GOLDEN, "*.npz")))
+
+
+def load(name):
+    z = np.load(os.path.join(GOLDEN, name + ".npz"))
+    rec = {k: z[k] for k in z.files}
+    rec["config"] = json.loads(str(rec["config"]))
+    return rec
+
+
+def model_kwargs(cfg):
+    kw = dict(method=cfg["method"], mesh_spacing=cfg["mesh_spacing"], interpolation_nodes=cfg["interpolation_nodes"],
+              c6tol=cfg["c6tol"], k_cutoff=cfg["k_cutoff"], r_cut=cfg["r_cut"])
+    if cfg.get("cncorr") is not None:
+        kw["cncorr"] = np.asarray(cfg["cncorr"], dtype=np.float64)
+    return kw

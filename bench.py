@@ -41,6 +41,9 @@ def parse():
     ap.add_argument("--impl", default="fd3", choices=["fd3", "reference"])
     ap.add_argument("--reps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
+                    help="'both' times plain fp64 and mixed (headline); one value restricts the run")
+    ap.add_argument("--no-e2e", action="store_true")
     return ap.parse_args()
 
 
@@ -245,11 +248,13 @@ def main():
     device = torch.device("cuda", local)
     pos, cell, nums = st.sio2_scaled(args.reps)
     n = len(nums)
+    precs = ("fp64", "mixed") if args.precision == "both" else (args.precision,)
+    head = "mixed" if "mixed" in precs else "fp64"
     models = {prec: D3Model(nums, cell, precision=prec, device=device, method="spme", mesh_spacing=1.2,
-                            interpolation_nodes=5, c6tol=1.0, r_cut=6.0) for prec in ("mixed", "fp64")}
-    mesh = models["mixed"].mesh
-    R = models["mixed"].setup.n_rank
-    S = models["mixed"].setup.n_species
+                            interpolation_nodes=5, c6tol=1.0, r_cut=6.0) for prec in precs}
+    mesh = models[head].mesh
+    R = models[head].setup.n_rank
+    S = models[head].setup.n_species
     C = S * R
     pos_dev = torch.tensor(pos, dtype=torch.float64, device=device)
     cell_dev = torch.tensor(cell, dtype=torch.float64, device=device)
@@ -262,8 +267,8 @@ def main():
 
     res = {}
     clocks = None
-    for prec in ("fp64", "mixed"):
-        if prec == "mixed":
+    for prec in precs:
+        if prec == head:
             with ClockSampler(torch.cuda.current_device()) as cs:
                 l0 = _native.launch_count()
                 ms = time_steps(lambda: step(prec), args.steps, args.warmup, ws, device)
@@ -276,7 +281,7 @@ def main():
 
     # per-stage CUDA-event times on the launching stream (separate, profiled steps)
     stages = {}
-    for prec in ("mixed", "fp64"):
+    for prec in precs:
         eng = models[prec].engine
         eng.profile(True)
         acc: dict = {}
@@ -296,19 +301,21 @@ def main():
 
     def e2e_step():
         pd = pos_h.to(device, non_blocking=True)
-        e, f, s = models["mixed"](pd, cell, out=outs["mixed"])
+        e, f, s = models[head](pd, cell, out=outs[head])
         e_h.copy_(e, non_blocking=True)
         f_h.copy_(f, non_blocking=True)
         s_h.copy_(s, non_blocking=True)
 
-    e2e_ms = max_over_ranks(time_steps(e2e_step, args.steps, args.warmup, ws, device), ws, device)
+    e2e_ms = None
+    if not args.no_e2e:
+        e2e_ms = max_over_ranks(time_steps(e2e_step, args.steps, args.warmup, ws, device), ws, device)
 
-    b = 4
-    st_mixed = stages["mixed"]
+    b = 4 if head == "mixed" else 8
+    st_mixed = stages[head]
     ours = {k: v for k, v in st_mixed.items() if not k.startswith("fft")}
     dom = max(ours, key=ours.get)
     peak, peak_kind = measured_peaks()
-    dom_bytes = stage_bytes(dom, n, mesh, C, R, b if dom in ("spread", "filter", "gather") else 8)
+    dom_bytes = stage_bytes(dom, n, mesh, C, R, b)
     achieved = dom_bytes / (ours[dom] * 1e-3) / 1e9
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": achieved / peak, "traffic": None,
@@ -322,23 +329,24 @@ def main():
                "sample": f"oracle (CPU float64 restatement) one E+F+stress of the {natoms}-atom 2x2x2 replica, "
                          f"{dt:.1f} s"}
 
-    ms = res["mixed"]
+    ms = res[head]
     line = {
         "metric": METRIC, "value": ws * n / (ms * 1e-3), "unit": "atoms/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f32-mesh+f64-accum", "data": "synthetic",
+        "vs_baseline": None, "dtype": "f32-mesh+f64-accum" if head == "mixed" else "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD, "n_atoms": n, "mesh": list(mesh), "method": "spme", "order": 5,
-                   "species": S, "c6_rank": R, "precision": "mixed", "parallelism": f"replicas{ws}",
+                   "species": S, "c6_rank": R, "precision": head, "parallelism": f"replicas{ws}",
                    "l2": "inputs larger than L2 (mesh channels %.2f GB)" % (C * mesh[0] * mesh[1] * mesh[2] * 4 / 1e9),
                    "c6_source": tables.c6_source()},
-        "plain_fp64": {"value": ws * n / (res["fp64"] * 1e-3), "ms_per_step": res["fp64"],
-                       "stages_ms": stages["fp64"]},
-        "mixed_over_fp64": res["fp64"] / ms,
-        "stages_ms": stages["mixed"],
+        "plain_fp64": ({"value": ws * n / (res["fp64"] * 1e-3), "ms_per_step": res["fp64"],
+                        "stages_ms": stages["fp64"]} if "fp64" in res else None),
+        "mixed_over_fp64": res["fp64"] / ms if "fp64" in res and head == "mixed" else None,
+        "stages_ms": stages[head],
         "roofline": roof,
         "cpu_baseline": cpu,
-        "e2e": {"value": ws * n / (e2e_ms * 1e-3), "unit": "atoms/s", "ms_per_step": e2e_ms,
-                "h2d_bytes_per_step": n * 3 * 8, "d2h_bytes_per_step": 8 + n * 3 * 8 + 9 * 8},
+        "e2e": ({"value": ws * n / (e2e_ms * 1e-3), "unit": "atoms/s", "ms_per_step": e2e_ms,
+                 "h2d_bytes_per_step": n * 3 * 8, "d2h_bytes_per_step": 8 + n * 3 * 8 + 9 * 8}
+                if e2e_ms is not None else None),
         "gpu_launches": int(launches) * args.steps,
         "clocks": clocks,
     }

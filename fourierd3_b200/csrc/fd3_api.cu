@@ -96,10 +96,6 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
     }
     for (int a = 0; a < 3; ++a)
       if (d->mesh[a] < 1) return FD3_EINVAL;
-    if (S > 8) {
-      set_error("fd3_plan_create", "mesh filter kernel supports up to 8 species");
-      return FD3_EINVAL;
-    }
   }
   fd3_plan* p = new (std::nothrow) fd3_plan();
   if (!p) return FD3_EINVAL;
@@ -168,7 +164,7 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
       MeshGeom& m = p->mg;
       for (int a = 0; a < 3; ++a) {
         m.n[a] = d->mesh[a];
-        m.t[a] = largest_divisor_le(m.n[a], 8);
+        m.t[a] = largest_divisor_le(m.n[a], a == 2 ? 8 : 16);   // spread tile 16 x 16 x 8
         m.nt[a] = m.n[a] / m.t[a];
         const int need = 1 + (d->order - 1 + m.t[a] - 1) / m.t[a];
         m.ns[a] = need < m.nt[a] ? need : m.nt[a];
@@ -255,12 +251,13 @@ struct Work {
   double *self_part, *kspc_part, *cnv_part, *mcell_part;
   int *mkeys, *mcount, *mstart, *morder;
   CellList cl;
-  void *rho, *spec, *fftw;
+  void *rho, *spec, *spec2, *fftw;
 };
 
 void carve(const fd3_plan* p, int64_t N, int64_t K, Carver& c, Work& w) {
   const int R = p->R;
-  const int64_t nblk = (N + 7) / 8 + 1;
+  // per-block partials: per-atom kernels use ceil(N/8) blocks, the bin kernels one per bin
+  const int64_t nblk = ((N + 7) / 8 > K ? (N + 7) / 8 : K) + 1;
   w.ci = c.take<CellInfo>(1);
   w.cn = c.take<double>(N);
   w.c6 = c.take<double>(N * R);
@@ -277,7 +274,7 @@ void carve(const fd3_plan* p, int64_t N, int64_t K, Carver& c, Work& w) {
     M = (size_t)p->mg.n[0] * p->mg.n[1] * p->mg.n[2];
     Kmesh = (int64_t)p->mg.nt[0] * p->mg.nt[1] * p->mg.nt[2] * p->S;
   }
-  w.kspc_part = c.take<double>(7 * ((Mh + 255) / 256 + 1));
+  w.kspc_part = c.take<double>(7 * (filter_max_blocks() + 1));
   w.mkeys = c.take<int>(N);
   w.mcount = c.take<int>(Kmesh);
   w.mstart = c.take<int>(Kmesh + 1);
@@ -293,6 +290,8 @@ void carve(const fd3_plan* p, int64_t N, int64_t K, Carver& c, Work& w) {
   const size_t C = (size_t)p->S * p->R;
   w.rho = c.take<char>(mesh ? C * M * es : 1);
   w.spec = c.take<char>(mesh ? C * Mh * 2 * es : 1);
+  // more than 8 species: the filter writes H out of place
+  w.spec2 = c.take<char>(mesh && p->S > 8 ? C * Mh * 2 * es : 1);
   w.fftw = c.take<char>(p->fft_ws);
 }
 }  // namespace
@@ -349,17 +348,18 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
   else
     FD3_CUFFT(cufftExecR2C(p->fwd, (cufftReal*)w.rho, (cufftComplex*)w.spec));
   prof_mark(p, s, "fft_r2c");
+  void* hspec = p->S > 8 ? w.spec2 : w.spec;
   FD3_TRY(launch_filter<T>(mg, w.ci, p->d_green, p->d_tab, p->d_deconv, p->method == FD3_METHOD_SPME, w.spec,
-                           w.kspc_part, n_kspc, s));
+                           hspec, w.kspc_part, n_kspc, s));
   prof_mark(p, s, "filter");
   *n_mcell = 0;
   if (!need_grad) return FD3_OK;
   FD3_CUFFT(cufftSetStream(p->inv, s));
   FD3_CUFFT(cufftSetWorkArea(p->inv, w.fftw));
   if (sizeof(T) == 8)
-    FD3_CUFFT(cufftExecZ2D(p->inv, (cufftDoubleComplex*)w.spec, (cufftDoubleReal*)w.rho));
+    FD3_CUFFT(cufftExecZ2D(p->inv, (cufftDoubleComplex*)hspec, (cufftDoubleReal*)w.rho));
   else
-    FD3_CUFFT(cufftExecC2R(p->inv, (cufftComplex*)w.spec, (cufftReal*)w.rho));
+    FD3_CUFFT(cufftExecC2R(p->inv, (cufftComplex*)hspec, (cufftReal*)w.rho));
   prof_mark(p, s, "fft_c2r");
   FD3_TRY(launch_gather<T>(mg, N, pos, ps, species, w.c6, w.dc6, w.ci, p->d_tab, w.morder, (const T*)w.rho, w.gcn,
                            gpos, mcell, n_mcell, s));

@@ -57,7 +57,7 @@ int make_cell_grid(const double* h_cell, double r_cut, CellGrid* g) {
 constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;
 
-__global__ void k_scan_exclusive(const int* __restrict__ in, int n, int* __restrict__ out) {
+__global__ void __launch_bounds__(1024) k_scan_exclusive(const int* __restrict__ in, int n, int* __restrict__ out) {
   __shared__ int warp_tot[32];
   __shared__ int carry_s;
   if (threadIdx.x == 0) carry_s = 0;
@@ -110,12 +110,12 @@ int scan_exclusive(const int* in, int n, int* out, cudaStream_t s) {
   return FD3_OK;
 }
 
-__global__ void k_hist(const int* __restrict__ keys, int n, int* __restrict__ counts) {
+__global__ void __launch_bounds__(256) k_hist(const int* __restrict__ keys, int n, int* __restrict__ counts) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) atomicAdd(&counts[keys[i]], 1);
 }
 
-__global__ void k_scatter(const int* __restrict__ keys, int n, const int* __restrict__ starts,
+__global__ void __launch_bounds__(256) k_scatter(const int* __restrict__ keys, int n, const int* __restrict__ starts,
                           int* __restrict__ fill, int* __restrict__ order) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) {
@@ -126,7 +126,7 @@ __global__ void k_scatter(const int* __restrict__ keys, int n, const int* __rest
 
 // Insertion sort of each key segment by atom id: makes the order (and every sum taken in
 // that order) independent of the atomic slot assignment above.
-__global__ void k_sort_segments(const int* __restrict__ starts, int K, int* __restrict__ order) {
+__global__ void __launch_bounds__(256) k_sort_segments(const int* __restrict__ starts, int K, int* __restrict__ order) {
   const int k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= K) return;
   const int a = starts[k], b = starts[k + 1];
@@ -180,7 +180,7 @@ static GridDev to_dev(const CellGrid& g) {
   return d;
 }
 
-__global__ void k_bin_atoms(GridDev g, int n, const double* __restrict__ x, int* __restrict__ bin_of,
+__global__ void __launch_bounds__(256) k_bin_atoms(GridDev g, int n, const double* __restrict__ x, int* __restrict__ bin_of,
                             int4* __restrict__ off) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
@@ -199,7 +199,7 @@ __global__ void k_bin_atoms(GridDev g, int n, const double* __restrict__ x, int*
   off[i] = make_int4(o[0], o[1], o[2], bin);
 }
 
-__global__ void k_gather_sorted(int n, const int* __restrict__ order, const double* __restrict__ x,
+__global__ void __launch_bounds__(256) k_gather_sorted(int n, const int* __restrict__ order, const double* __restrict__ x,
                                 const int32_t* __restrict__ species, const int4* __restrict__ off,
                                 double4* __restrict__ xs, int4* __restrict__ meta) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -342,49 +342,175 @@ __device__ __forceinline__ double c6_factors_warp(double cn_raw, int s, const Ta
 
 constexpr int kWarpsPerBlock = 8;
 
-__global__ void __launch_bounds__(256) k_cn_c6_cells(GridDev g, int n, const int* __restrict__ bin_start,
-                                                    const double4* __restrict__ xs, const int4* __restrict__ meta,
-                                                    const int4* __restrict__ off, const Tables* __restrict__ tab,
-                                                    const double* __restrict__ V, int R, double* __restrict__ cn,
-                                                    double* __restrict__ c6, double* __restrict__ dc6,
-                                                    double* __restrict__ self_part) {
+// Per-atom traversal straight from global memory: the path for bins whose neighbourhood does not
+// fit the shared-memory stage (dense clusters, cells much narrower than the cutoff).
+__device__ __forceinline__ double cn_atom_global(const GridDev& g, const int* __restrict__ bin_start,
+                                                 const double4* __restrict__ xs, const int4* __restrict__ meta,
+                                                 const int4* __restrict__ off, const Tables* __restrict__ tab,
+                                                 int t) {
+  const double4 xi = xs[t];
+  const int i = meta[t].w;
+  const int4 offi = off[i];
+  const double rci = tab->rcov[(int)xi.w];
+  double acc = 0.0;
+  visit_neighbors(g, bin_start, xs, meta, i, xi.x, xi.y, xi.z, offi,
+                  [&](bool hit, int u, int, int, int, int, double d0, double d1, double d2) {
+                    if (!hit) return;
+                    const double v0 = d0 * kAngToBohr, v1 = d1 * kAngToBohr, v2 = d2 * kAngToBohr;
+                    double f, df;
+                    cn_edge(sqrt(v0 * v0 + v1 * v1 + v2 * v2), rci + tab->rcov[(int)xs[u].w], tab->r_cut, f, df);
+                    acc += f;
+                  });
+  return warp_sum(acc);
+}
+
+__device__ __forceinline__ void cn_adjoint_atom_global(const GridDev& g, const int* __restrict__ bin_start,
+                                                       const double4* __restrict__ xs,
+                                                       const int4* __restrict__ meta, const int4* __restrict__ off,
+                                                       const Tables* __restrict__ tab, const double* __restrict__ gcn,
+                                                       int t, double* f, double* v) {
+  const double4 xi = xs[t];
+  const int i = meta[t].w;
+  const int4 offi = off[i];
+  const double rci = tab->rcov[(int)xi.w];
+  const double gi = gcn[i];
+  visit_neighbors(g, bin_start, xs, meta, i, xi.x, xi.y, xi.z, offi,
+                  [&](bool hit, int u, int j, int, int, int, double d0, double d1, double d2) {
+                    if (!hit) return;
+                    const double v0 = d0 * kAngToBohr, v1 = d1 * kAngToBohr, v2 = d2 * kAngToBohr;
+                    const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+                    double fe, df;
+                    cn_edge(r, rci + tab->rcov[(int)xs[u].w], tab->r_cut, fe, df);
+                    if (r > 1e-6) {
+                      const double a = df / r;
+                      const double w = (gi + gcn[j]) * a;
+                      f[0] -= w * v0;
+                      f[1] -= w * v1;
+                      f[2] -= w * v2;
+                      const double b = gi * a;
+                      v[0] += b * v0 * v0; v[1] += b * v0 * v1; v[2] += b * v0 * v2;
+                      v[4] += b * v1 * v1; v[5] += b * v1 * v2; v[8] += b * v2 * v2;
+                    }
+                  });
+}
+
+// ------------------------------------------------------------------ bin-staged CN
+// One CTA per bin: the atoms of the (2 reach + 1)^3 neighbour bins are staged once in shared
+// memory as image positions p_j = x_j + (S' - off_j) . cell, and the warps of the CTA run the
+// bin's own atoms against that stage (d = p_j - (x_i - off_i . cell)). The same stage and the
+// same arithmetic serve the CN and its adjoint, so both see the same pairs.
+constexpr int kBinCap = 768;
+constexpr int kMaxNbrBins = 343;
+
+struct BinStage {
+  double4 p[kBinCap];   // image position (A), species in .w
+  int j[kBinCap];
+  int a0[kMaxNbrBins];
+  int pref[kMaxNbrBins + 1];
+  int img[kMaxNbrBins][3];
+};
+
+// Returns the number of staged candidates, or -1 when the neighbourhood does not fit.
+__device__ int stage_bin(const GridDev& g, int b, const int* __restrict__ bin_start,
+                         const double4* __restrict__ xs, const int4* __restrict__ meta, BinStage& st,
+                         double* __restrict__ s_g, const double* __restrict__ gcn) {
+  const int nx = 2 * g.reach[0] + 1, ny = 2 * g.reach[1] + 1, nz = 2 * g.reach[2] + 1;
+  const int nnb = nx * ny * nz;
+  if (nnb > kMaxNbrBins) return -1;
+  const int bz = b % g.nb[2], by = (b / g.nb[2]) % g.nb[1], bx = b / (g.nb[2] * g.nb[1]);
+  for (int e = threadIdx.x; e < nnb; e += blockDim.x) {
+    const int dz = e % nz - g.reach[2], dy = (e / nz) % ny - g.reach[1], dx = e / (nz * ny) - g.reach[0];
+    const int cx = bx + dx, cy = by + dy, cz = bz + dz;
+    const int sx = floordiv(cx, g.nb[0]), sy = floordiv(cy, g.nb[1]), sz = floordiv(cz, g.nb[2]);
+    const int id = ((cx - sx * g.nb[0]) * g.nb[1] + (cy - sy * g.nb[1])) * g.nb[2] + (cz - sz * g.nb[2]);
+    const int a0 = bin_start[id];
+    st.a0[e] = a0;
+    st.pref[e + 1] = bin_start[id + 1] - a0;
+    st.img[e][0] = sx;
+    st.img[e][1] = sy;
+    st.img[e][2] = sz;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    st.pref[0] = 0;
+    for (int e = 0; e < nnb; ++e) st.pref[e + 1] += st.pref[e];
+  }
+  __syncthreads();
+  const int total = st.pref[nnb];
+  if (total > kBinCap) return -1;
+  for (int c = threadIdx.x; c < total; c += blockDim.x) {
+    int lo = 0, hi = nnb - 1;          // last entry with pref[e] <= c
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (st.pref[mid] <= c) lo = mid; else hi = mid - 1;
+    }
+    const int u = st.a0[lo] + (c - st.pref[lo]);
+    const double4 xj = xs[u];
+    const int4 mj = meta[u];
+    const double S0 = st.img[lo][0] - mj.x, S1 = st.img[lo][1] - mj.y, S2 = st.img[lo][2] - mj.z;
+    st.p[c] = make_double4(xj.x + S0 * g.cell[0] + S1 * g.cell[3] + S2 * g.cell[6],
+                           xj.y + S0 * g.cell[1] + S1 * g.cell[4] + S2 * g.cell[7],
+                           xj.z + S0 * g.cell[2] + S1 * g.cell[5] + S2 * g.cell[8], xj.w);
+    st.j[c] = mj.w;
+    if (s_g) s_g[c] = gcn[mj.w];
+  }
+  __syncthreads();
+  return total;
+}
+
+__device__ __forceinline__ void wrapped_pos(const GridDev& g, double4 x, int4 m, double& w0, double& w1,
+                                            double& w2) {
+  w0 = x.x - (m.x * g.cell[0] + m.y * g.cell[3] + m.z * g.cell[6]);
+  w1 = x.y - (m.x * g.cell[1] + m.y * g.cell[4] + m.z * g.cell[7]);
+  w2 = x.z - (m.x * g.cell[2] + m.y * g.cell[5] + m.z * g.cell[8]);
+}
+
+__global__ void __launch_bounds__(256) k_cn_c6_bins(GridDev g, const int* __restrict__ bin_start,
+                                                   const double4* __restrict__ xs, const int4* __restrict__ meta,
+                                                   const int4* __restrict__ off, const Tables* __restrict__ tab,
+                                                   const double* __restrict__ V, int R, double* __restrict__ cn,
+                                                   double* __restrict__ c6, double* __restrict__ dc6,
+                                                   double* __restrict__ self_part) {
+  __shared__ BinStage st;
   __shared__ double wsum[kWarpsPerBlock];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int t = blockIdx.x * kWarpsPerBlock + wid;
+  const int b = blockIdx.x;
+  const int total = stage_bin(g, b, bin_start, xs, meta, st, nullptr, nullptr);
+  const int s0 = bin_start[b], s1 = bin_start[b + 1];
   double selfv = 0.0;
-  if (t < n) {
+  for (int t = s0 + wid; t < s1; t += kWarpsPerBlock) {
     const double4 xi = xs[t];
-    const int i = meta[t].w;
-    const int4 offi = off[i];
+    const int4 mi = meta[t];
     const int si = (int)xi.w;
-    const double rci = tab->rcov[si];
-    const double rcut_b = tab->r_cut;
-    double acc = 0.0;
-    visit_neighbors(g, bin_start, xs, meta, i, xi.x, xi.y, xi.z, offi,
-                    [&](bool hit, int u, int j, int S0, int S1, int S2, double, double, double) {
-                      if (!hit) return;
-                      const double4 xj = xs[u];
-                      // Bohr vector exactly as the reference forms it: x*a2b, shift*a2b
-                      const double sh0 = (S0 * g.cell[0] + S1 * g.cell[3] + S2 * g.cell[6]) * kAngToBohr;
-                      const double sh1 = (S0 * g.cell[1] + S1 * g.cell[4] + S2 * g.cell[7]) * kAngToBohr;
-                      const double sh2 = (S0 * g.cell[2] + S1 * g.cell[5] + S2 * g.cell[8]) * kAngToBohr;
-                      const double v0 = xj.x * kAngToBohr - xi.x * kAngToBohr + sh0;
-                      const double v1 = xj.y * kAngToBohr - xi.y * kAngToBohr + sh1;
-                      const double v2 = xj.z * kAngToBohr - xi.z * kAngToBohr + sh2;
-                      const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-                      double f, df;
-                      cn_edge(r, rci + tab->rcov[(int)xj.w], rcut_b, f, df);
-                      acc += f;
-                    });
-    const double cn_raw = warp_sum(acc);
-    selfv = c6_factors_warp(cn_raw, si, tab, V, R, c6 + (size_t)i * R, dc6 + (size_t)i * R, cn + i);
+    double cn_raw;
+    if (total >= 0) {
+      double w0, w1, w2;
+      wrapped_pos(g, xi, mi, w0, w1, w2);
+      const double rci = tab->rcov[si];
+      double acc = 0.0;
+      for (int c = lane; c < total; c += 32) {
+        const double4 pj = st.p[c];
+        const double d0 = pj.x - w0, d1 = pj.y - w1, d2 = pj.z - w2;
+        if (d0 * d0 + d1 * d1 + d2 * d2 < g.rc2) {
+          const double v0 = d0 * kAngToBohr, v1 = d1 * kAngToBohr, v2 = d2 * kAngToBohr;
+          double f, df;
+          cn_edge(sqrt(v0 * v0 + v1 * v1 + v2 * v2), rci + tab->rcov[(int)pj.w], tab->r_cut, f, df);
+          acc += f;
+        }
+      }
+      cn_raw = warp_sum(acc);
+    } else {
+      cn_raw = cn_atom_global(g, bin_start, xs, meta, off, tab, t);
+    }
+    const int i = mi.w;
+    selfv += c6_factors_warp(cn_raw, si, tab, V, R, c6 + (size_t)i * R, dc6 + (size_t)i * R, cn + i);
   }
   if (lane == 0) wsum[wid] = selfv;
   __syncthreads();
   if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < kWarpsPerBlock; ++w) s += wsum[w];
-    self_part[blockIdx.x] = s;
+    double sum = 0.0;
+    for (int w = 0; w < kWarpsPerBlock; ++w) sum += wsum[w];
+    self_part[blockIdx.x] = sum;
   }
 }
 
@@ -393,67 +519,71 @@ int launch_cn_c6_cells(const CellGrid& g, int n, const CellList& cl, const doubl
                        double* c6, double* dc6, double* self_part, int* n_self_blocks, cudaStream_t s) {
   (void)pos_ang;
   (void)species;
-  const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
-  *n_self_blocks = blocks;
-  if (blocks == 0) return FD3_OK;
-  k_cn_c6_cells<<<blocks, 32 * kWarpsPerBlock, 0, s>>>(to_dev(g), n, cl.bin_start, cl.xs, cl.meta, cl.off, tab,
-                                                        eigvecs, R, cn, c6, dc6, self_part);
+  (void)n;
+  const int K = g.nb[0] * g.nb[1] * g.nb[2];
+  *n_self_blocks = K;
+  k_cn_c6_bins<<<K, 32 * kWarpsPerBlock, 0, s>>>(to_dev(g), cl.bin_start, cl.xs, cl.meta, cl.off, tab, eigvecs, R,
+                                                  cn, c6, dc6, self_part);
   FD3_LAUNCHED();
   return FD3_OK;
 }
 
 // CN adjoint: dE/dx_i = -sum_(j,S) (g_i + g_j) f'(r) d / r  (the list is symmetric), and the
-// strain virial W_ab = sum_i g_i sum_(j,S) f'(r) d_a d_b / r  (Bohr, Hartree).
-__global__ void __launch_bounds__(256) k_cn_adjoint_cells(GridDev g, int n, const int* __restrict__ bin_start,
-                                                         const double4* __restrict__ xs,
-                                                         const int4* __restrict__ meta, const int4* __restrict__ off,
-                                                         const Tables* __restrict__ tab,
-                                                         const double* __restrict__ gcn, double* __restrict__ grad,
-                                                         double out_scale, double* __restrict__ vir_part) {
+// strain virial W_ab = sum_i g_i sum_(j,S) f'(r) d_a d_b / r  (Bohr, Hartree). The force written
+// is out_scale * (mesh gradient already in grad + CN gradient).
+__global__ void __launch_bounds__(256) k_cn_adjoint_bins(GridDev g, const int* __restrict__ bin_start,
+                                                        const double4* __restrict__ xs,
+                                                        const int4* __restrict__ meta, const int4* __restrict__ off,
+                                                        const Tables* __restrict__ tab,
+                                                        const double* __restrict__ gcn, double* __restrict__ grad,
+                                                        double out_scale, double* __restrict__ vir_part) {
+  __shared__ BinStage st;
+  __shared__ double s_g[kBinCap];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int t = blockIdx.x * kWarpsPerBlock + wid;
+  const int b = blockIdx.x;
+  const int total = stage_bin(g, b, bin_start, xs, meta, st, s_g, gcn);
+  const int s0 = bin_start[b], s1 = bin_start[b + 1];
   double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  if (t < n) {
+  for (int t = s0 + wid; t < s1; t += kWarpsPerBlock) {
     const double4 xi = xs[t];
-    const int i = meta[t].w;
-    const int4 offi = off[i];
-    const int si = (int)xi.w;
-    const double rci = tab->rcov[si];
-    const double rcut_b = tab->r_cut;
-    const double gi = gcn[i];
-    double f0 = 0, f1 = 0, f2 = 0;
-    visit_neighbors(g, bin_start, xs, meta, i, xi.x, xi.y, xi.z, offi,
-                    [&](bool hit, int u, int j, int S0, int S1, int S2, double, double, double) {
-                      if (!hit) return;
-                      const double4 xj = xs[u];
-                      const double sh0 = (S0 * g.cell[0] + S1 * g.cell[3] + S2 * g.cell[6]) * kAngToBohr;
-                      const double sh1 = (S0 * g.cell[1] + S1 * g.cell[4] + S2 * g.cell[7]) * kAngToBohr;
-                      const double sh2 = (S0 * g.cell[2] + S1 * g.cell[5] + S2 * g.cell[8]) * kAngToBohr;
-                      const double v0 = xj.x * kAngToBohr - xi.x * kAngToBohr + sh0;
-                      const double v1 = xj.y * kAngToBohr - xi.y * kAngToBohr + sh1;
-                      const double v2 = xj.z * kAngToBohr - xi.z * kAngToBohr + sh2;
-                      const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-                      double f, df;
-                      cn_edge(r, rci + tab->rcov[(int)xj.w], rcut_b, f, df);
-                      if (r > 1e-6) {
-                        const double a = df / r;
-                        const double w = (gi + gcn[j]) * a;
-                        f0 -= w * v0;
-                        f1 -= w * v1;
-                        f2 -= w * v2;
-                        const double b = gi * a;
-                        v[0] += b * v0 * v0; v[1] += b * v0 * v1; v[2] += b * v0 * v2;
-                        v[4] += b * v1 * v1; v[5] += b * v1 * v2; v[8] += b * v2 * v2;
-                      }
-                    });
-    f0 = warp_sum(f0);
-    f1 = warp_sum(f1);
-    f2 = warp_sum(f2);
+    const int4 mi = meta[t];
+    const int i = mi.w;
+    double f[3] = {0, 0, 0};
+    if (total >= 0) {
+      double w0, w1, w2;
+      wrapped_pos(g, xi, mi, w0, w1, w2);
+      const double rci = tab->rcov[(int)xi.w];
+      const double gi = gcn[i];
+      for (int c = lane; c < total; c += 32) {
+        const double4 pj = st.p[c];
+        const double d0 = pj.x - w0, d1 = pj.y - w1, d2 = pj.z - w2;
+        if (d0 * d0 + d1 * d1 + d2 * d2 < g.rc2) {
+          const double v0 = d0 * kAngToBohr, v1 = d1 * kAngToBohr, v2 = d2 * kAngToBohr;
+          const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+          double fe, df;
+          cn_edge(r, rci + tab->rcov[(int)pj.w], tab->r_cut, fe, df);
+          if (r > 1e-6) {
+            const double a = df / r;
+            const double w = (gi + s_g[c]) * a;
+            f[0] -= w * v0;
+            f[1] -= w * v1;
+            f[2] -= w * v2;
+            const double bb = gi * a;
+            v[0] += bb * v0 * v0; v[1] += bb * v0 * v1; v[2] += bb * v0 * v2;
+            v[4] += bb * v1 * v1; v[5] += bb * v1 * v2; v[8] += bb * v2 * v2;
+          }
+        }
+      }
+    } else {
+      cn_adjoint_atom_global(g, bin_start, xs, meta, off, tab, gcn, t, f, v);
+    }
+    f[0] = warp_sum(f[0]);
+    f[1] = warp_sum(f[1]);
+    f[2] = warp_sum(f[2]);
     if (lane == 0) {
-      // grad holds the mesh part already; write (mesh + CN) scaled to the caller's unit
-      grad[3 * i] = out_scale * (grad[3 * i] + f0);
-      grad[3 * i + 1] = out_scale * (grad[3 * i + 1] + f1);
-      grad[3 * i + 2] = out_scale * (grad[3 * i + 2] + f2);
+      grad[3 * i] = out_scale * (grad[3 * i] + f[0]);
+      grad[3 * i + 1] = out_scale * (grad[3 * i + 1] + f[1]);
+      grad[3 * i + 2] = out_scale * (grad[3 * i + 2] + f[2]);
     }
   }
   v[3] = v[1];
@@ -467,17 +597,17 @@ int launch_cn_adjoint_cells(const CellGrid& g, int n, const CellList& cl, const 
                             double out_scale, double* vir_part, int* n_blocks, cudaStream_t s) {
   (void)pos_ang;
   (void)species;
-  const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
-  *n_blocks = blocks;
-  if (blocks == 0) return FD3_OK;
-  k_cn_adjoint_cells<<<blocks, 32 * kWarpsPerBlock, 0, s>>>(to_dev(g), n, cl.bin_start, cl.xs, cl.meta, cl.off,
-                                                             tab, gcn, grad, out_scale, vir_part);
+  (void)n;
+  const int K = g.nb[0] * g.nb[1] * g.nb[2];
+  *n_blocks = K;
+  k_cn_adjoint_bins<<<K, 32 * kWarpsPerBlock, 0, s>>>(to_dev(g), cl.bin_start, cl.xs, cl.meta, cl.off, tab, gcn,
+                                                       grad, out_scale, vir_part);
   FD3_LAUNCHED();
   return FD3_OK;
 }
 
 // ------------------------------------------------------------------ edge-list path
-__global__ void k_cn_edges(int64_t ne, const double* __restrict__ x, const int32_t* __restrict__ species,
+__global__ void __launch_bounds__(256) k_cn_edges(int64_t ne, const double* __restrict__ x, const int32_t* __restrict__ species,
                            const int64_t* __restrict__ src, const int64_t* __restrict__ dst,
                            const double* __restrict__ sh, const Tables* __restrict__ tab, double* __restrict__ cn) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -535,7 +665,7 @@ int launch_c6_atoms(int n, const int32_t* species, const Tables* tab, const doub
   return FD3_OK;
 }
 
-__global__ void k_cn_adjoint_edges(int64_t ne, const double* __restrict__ x, const int32_t* __restrict__ species,
+__global__ void __launch_bounds__(256) k_cn_adjoint_edges(int64_t ne, const double* __restrict__ x, const int32_t* __restrict__ species,
                                    const int64_t* __restrict__ src, const int64_t* __restrict__ dst,
                                    const double* __restrict__ sh, const Tables* __restrict__ tab,
                                    const double* __restrict__ gcn, double* __restrict__ gpos,

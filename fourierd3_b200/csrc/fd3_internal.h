@@ -105,7 +105,9 @@ int launch_spread(const MeshGeom& mg, const double* pos, double pos_scale, const
                   cudaStream_t s);
 template <typename T>
 int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab,
-                  const float* deconv, int spme, void* spec, double* part, int* n_blocks, cudaStream_t s);
+                  const float* deconv, int spme, void* spec, void* spec_out, double* part, int* n_blocks,
+                  cudaStream_t s);
+int filter_max_blocks();
 template <typename T>
 int launch_gather(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
                   const double* c6, const double* dc6, const CellInfo* ci, const Tables* tab, const int* order,

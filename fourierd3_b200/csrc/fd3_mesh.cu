@@ -17,7 +17,7 @@
 namespace fd3 {
 
 // ------------------------------------------------------------------ cell info
-__global__ void k_cellinfo(const double* __restrict__ cell, double scale, CellInfo* __restrict__ ci) {
+__global__ void __launch_bounds__(32) k_cellinfo(const double* __restrict__ cell, double scale, CellInfo* __restrict__ ci) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double m[9];
   for (int k = 0; k < 9; ++k) m[k] = cell[k] * scale;
@@ -49,14 +49,14 @@ int launch_cellinfo(const double* cell, double scale, CellInfo* ci, cudaStream_t
   return FD3_OK;
 }
 
-__global__ void k_mesh_keys(MeshDev g, int n, int P, const double* __restrict__ pos, double ps,
+__global__ void __launch_bounds__(256) k_mesh_keys(MeshDev g, int n, int P, const double* __restrict__ pos, double ps,
                             const int32_t* __restrict__ species, const CellInfo* __restrict__ ci,
                             int* __restrict__ keys) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   int base[3];
   double xl[3];
-  mesh_locate<double>(pos, i, ps, ci, g.n, P, base, xl);
+  mesh_locate<double>(pos, i, ps, ci, g.n[0], g.n[1], g.n[2], P, base, xl);
   const int tx = base[0] / g.t[0], ty = base[1] / g.t[1], tz = base[2] / g.t[2];
   keys[i] = ((tx * g.nt[1] + ty) * g.nt[2] + tz) * g.S + species[i];
 }
@@ -80,6 +80,74 @@ constexpr int kFilterThreads = 256;
 // exact float64 SPME window sinc(m/n)^(2p), clamped at 1e-10 (used when no table is given)
 __device__ __forceinline__ double sinc_pi(double x) { return x == 0.0 ? 1.0 : sin(kPi * x) / (kPi * x); }
 
+// Geometry of rfft k-point k: k-vector (torch fftfreq order on x, y; rfftfreq on z), |k|, the
+// SPME window, the Hermitian weight (1 on the first and last z-plane, pair_pot.py:213-218) and,
+// on the self-conjugate planes, the |k| of the stored conjugate partner when it differs.
+struct KPoint {
+  double kv[3], knorm, sc, wk, kpart;
+  bool partner;
+};
+
+__device__ __forceinline__ KPoint kpoint(const MeshDev& g, size_t k, const CellInfo* __restrict__ ci,
+                                         const float* __restrict__ deconv, int spme, int P) {
+  KPoint q;
+  const int iz = (int)(k % g.nzh);
+  const int iy = (int)((k / g.nzh) % g.n[1]);
+  const int ix = (int)(k / ((size_t)g.nzh * g.n[1]));
+  const int mx = ix <= (g.n[0] - 1) / 2 ? ix : ix - g.n[0];
+  const int my = iy <= (g.n[1] - 1) / 2 ? iy : iy - g.n[1];
+  const int mz = iz;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) q.kv[c] = mx * ci->recip[c] + my * ci->recip[3 + c] + mz * ci->recip[6 + c];
+  q.knorm = sqrt(q.kv[0] * q.kv[0] + q.kv[1] * q.kv[1] + q.kv[2] * q.kv[2]);
+  q.sc = 1.0;
+  if (spme) {
+    if (deconv) {
+      q.sc = (double)deconv[k];
+    } else {
+      const double nzf = (double)(2 * (g.nzh - 1));
+      double v = sinc_pi(mx / (double)g.n[0]) * sinc_pi(my / (double)g.n[1]) * sinc_pi(mz / nzf);
+      v = pow(v, 2.0 * P);
+      q.sc = v < 1e-10 ? 1e-10 : v;
+    }
+  }
+  q.wk = (iz == 0 || iz == g.nzh - 1) ? 1.0 : 2.0;
+  // Self-conjugate planes (kz = 0 and the z-Nyquist plane): the entry at (ix, iy) and its conjugate
+  // partner (-ix, -iy) are both stored, but at the Nyquist rows their k-vectors differ in a
+  // triclinic cell, so G(k) != G(k'). The inverse FFT needs a Hermitian input; using
+  // (G(k) + G(k')) / 2 for H keeps the gradient the exact derivative of the energy sum.
+  q.partner = false;
+  q.kpart = q.knorm;
+  const bool plane = (iz == 0) || (iz == g.nzh - 1 && iz > 0);
+  if (plane) {
+    const int px = (g.n[0] - ix) % g.n[0], py = (g.n[1] - iy) % g.n[1];
+    const int qx = px <= (g.n[0] - 1) / 2 ? px : px - g.n[0];
+    const int qy = py <= (g.n[1] - 1) / 2 ? py : py - g.n[1];
+    if (qx != -mx || qy != -my || mz != 0) {
+      double kp[3];
+#pragma unroll
+      for (int c = 0; c < 3; ++c) kp[c] = qx * ci->recip[c] + qy * ci->recip[3 + c] + mz * ci->recip[6 + c];
+      q.kpart = sqrt(kp[0] * kp[0] + kp[1] * kp[1] + kp[2] * kp[2]);
+      q.partner = q.kpart != q.knorm;
+    }
+  }
+  return q;
+}
+
+__device__ __forceinline__ void virial_acc(const KPoint& q, double dq, double* acc) {
+  if (q.knorm > 0.0) {
+    const double f = q.wk * dq / q.knorm;
+    acc[1] += f * q.kv[0] * q.kv[0];
+    acc[2] += f * q.kv[1] * q.kv[1];
+    acc[3] += f * q.kv[2] * q.kv[2];
+    acc[4] += f * q.kv[0] * q.kv[1];
+    acc[5] += f * q.kv[0] * q.kv[2];
+    acc[6] += f * q.kv[1] * q.kv[2];
+  }
+}
+
+// Up to 8 species: G, dG and the inverse-FFT matrix in registers; spectrum updated in place.
+// Grid-stride over k-points; one partial (energy + 6 virial components) per block.
 template <typename T, int MAXS>
 __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int spme,
                                                            const CellInfo* __restrict__ ci,
@@ -91,82 +159,39 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int
   using C2 = typename Cplx<T>::type;
   const int S = g.S, R = g.R;
   const size_t Mh = (size_t)g.n[0] * g.n[1] * g.nzh;
-  const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
-  if (k < Mh) {
-    const int iz = (int)(k % g.nzh);
-    const int iy = (int)((k / g.nzh) % g.n[1]);
-    const int ix = (int)(k / ((size_t)g.nzh * g.n[1]));
-    // torch.fft.fftfreq order on x and y, rfftfreq on z
-    const int mx = ix <= (g.n[0] - 1) / 2 ? ix : ix - g.n[0];
-    const int my = iy <= (g.n[1] - 1) / 2 ? iy : iy - g.n[1];
-    const int mz = iz;
-    double kv[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) kv[c] = mx * ci->recip[c] + my * ci->recip[3 + c] + mz * ci->recip[6 + c];
-    const double knorm = sqrt(kv[0] * kv[0] + kv[1] * kv[1] + kv[2] * kv[2]);
-    double sc = 1.0;
-    if (spme) {
-      if (deconv) {
-        sc = (double)deconv[k];
-      } else {
-        const double nzf = (double)(2 * (g.nzh - 1));
-        double v = sinc_pi(mx / (double)g.n[0]) * sinc_pi(my / (double)g.n[1]) * sinc_pi(mz / nzf);
-        v = pow(v, 2.0 * P);
-        sc = v < 1e-10 ? 1e-10 : v;
-      }
-    }
-    const double wk = (iz == 0 || iz == g.nzh - 1) ? 1.0 : 2.0;
-    const T kt = (T)knorm;
-    const T s6 = (T)tab->s6, s8 = (T)tab->s8;
+  const T s6 = (T)tab->s6, s8 = (T)tab->s8;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < Mh; k += (size_t)gridDim.x * blockDim.x) {
+    const KPoint q = kpoint(g, k, ci, deconv, spme, P);
+    const T kt = (T)q.knorm;
     T G[MAXS][MAXS], dG[MAXS][MAXS], Gh[MAXS][MAXS];
 #pragma unroll
     for (int X = 0; X < MAXS; ++X)
 #pragma unroll
       for (int Y = X; Y < MAXS; ++Y) {
+        T gv = T(0), dv = T(0);
         if (X < S && Y < S) {
-          T gv, dv;
           green_eval<T>(gp[X * S + Y], kt, s6, s8, gv, dv);
-          G[X][Y] = (T)((double)gv / sc);
-          dG[X][Y] = (T)((double)dv / sc);
-        } else {
-          G[X][Y] = T(0);
-          dG[X][Y] = T(0);
+          gv = (T)((double)gv / q.sc);
+          dv = (T)((double)dv / q.sc);
         }
-        G[Y][X] = G[X][Y];
-        dG[Y][X] = dG[X][Y];
-        Gh[X][Y] = G[X][Y];
-        Gh[Y][X] = G[X][Y];
+        G[X][Y] = G[Y][X] = gv;
+        dG[X][Y] = dG[Y][X] = dv;
+        Gh[X][Y] = Gh[Y][X] = gv;
       }
-    // Self-conjugate planes (kz = 0 and the z-Nyquist plane): the entry at index (ix, iy) and its
-    // conjugate partner (-ix, -iy) are both stored, but at the Nyquist rows their k-vectors differ
-    // in a triclinic cell, so G(k) != G(k'). The inverse FFT needs a Hermitian input; using
-    // (G(k) + G(k')) / 2 for H keeps the gradient the exact derivative of the energy sum.
-    const bool plane = (iz == 0) || (2 * iz == 2 * (g.nzh - 1) && iz > 0 && g.nzh > 1);
-    if (plane) {
-      const int px = (g.n[0] - ix) % g.n[0], py = (g.n[1] - iy) % g.n[1];
-      const int qx = px <= (g.n[0] - 1) / 2 ? px : px - g.n[0];
-      const int qy = py <= (g.n[1] - 1) / 2 ? py : py - g.n[1];
-      if (qx != -mx || qy != -my || mz != 0) {
-        double kp[3];
+    if (q.partner) {
+      const T kpt = (T)q.kpart;
 #pragma unroll
-        for (int c = 0; c < 3; ++c) kp[c] = qx * ci->recip[c] + qy * ci->recip[3 + c] + mz * ci->recip[6 + c];
-        const T kpt = (T)sqrt(kp[0] * kp[0] + kp[1] * kp[1] + kp[2] * kp[2]);
+      for (int X = 0; X < MAXS; ++X)
 #pragma unroll
-        for (int X = 0; X < MAXS; ++X)
-#pragma unroll
-          for (int Y = X; Y < MAXS; ++Y) {
-            if (X < S && Y < S) {
-              T gv, dv;
-              green_eval<T>(gp[X * S + Y], kpt, s6, s8, gv, dv);
-              const T gpv = (T)((double)gv / sc);
-              Gh[X][Y] = T(0.5) * (G[X][Y] + gpv);
-              Gh[Y][X] = Gh[X][Y];
-            }
+        for (int Y = X; Y < MAXS; ++Y)
+          if (X < S && Y < S) {
+            T gv, dv;
+            green_eval<T>(gp[X * S + Y], kpt, s6, s8, gv, dv);
+            Gh[X][Y] = Gh[Y][X] = T(0.5) * (G[X][Y] + (T)((double)gv / q.sc));
           }
-      }
     }
-    double q = 0.0, dq = 0.0;
+    double qq = 0.0, dq = 0.0;
     for (int r = 0; r < R; ++r) {
       C2 sv[MAXS];
 #pragma unroll
@@ -185,29 +210,102 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int
         }
         if (X < S) spec[((size_t)X * R + r) * Mh + k] = C2{hre, him};
       }
-      q += tab->eigs[r] * qr;
+      qq += tab->eigs[r] * qr;
       dq += tab->eigs[r] * dqr;
     }
-    acc[0] = wk * q;
-    if (knorm > 0.0) {
-      const double f = wk * dq / knorm;
-      acc[1] = f * kv[0] * kv[0];
-      acc[2] = f * kv[1] * kv[1];
-      acc[3] = f * kv[2] * kv[2];
-      acc[4] = f * kv[0] * kv[1];
-      acc[5] = f * kv[0] * kv[2];
-      acc[6] = f * kv[1] * kv[2];
-    }
+    acc[0] += q.wk * qq;
+    virial_acc(q, dq, acc);
   }
   block_sum_store<7>(acc, part + 7 * blockIdx.x);
 }
 
+// Any number of species (<= 64): G_XY evaluated per pair on the fly, H written out of place
+// (spec_out), ranks in chunks of 8 held in registers.
+constexpr int kAnyRC = 8;
+template <typename T>
+__global__ void __launch_bounds__(kFilterThreads) k_filter_any(MeshDev g, int P, int spme,
+                                                               const CellInfo* __restrict__ ci,
+                                                               const GreenPair* __restrict__ gp,
+                                                               const Tables* __restrict__ tab,
+                                                               const float* __restrict__ deconv,
+                                                               const typename Cplx<T>::type* __restrict__ spec,
+                                                               typename Cplx<T>::type* __restrict__ spec_out,
+                                                               double* __restrict__ part) {
+  using C2 = typename Cplx<T>::type;
+  const int S = g.S, R = g.R;
+  const size_t Mh = (size_t)g.n[0] * g.n[1] * g.nzh;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  const T s6 = (T)tab->s6, s8 = (T)tab->s8;
+  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < Mh; k += (size_t)gridDim.x * blockDim.x) {
+    const KPoint q = kpoint(g, k, ci, deconv, spme, P);
+    const T kt = (T)q.knorm, kpt = (T)q.kpart;
+    double qq = 0.0, dq = 0.0;
+    for (int r0 = 0; r0 < R; r0 += kAnyRC) {
+      for (int X = 0; X < S; ++X) {
+        C2 hq[kAnyRC], hd[kAnyRC], hh[kAnyRC];
+#pragma unroll
+        for (int r = 0; r < kAnyRC; ++r) hq[r] = hd[r] = hh[r] = C2{T(0), T(0)};
+        for (int Y = 0; Y < S; ++Y) {
+          T gv, dv;
+          green_eval<T>(gp[X * S + Y], kt, s6, s8, gv, dv);
+          gv = (T)((double)gv / q.sc);
+          dv = (T)((double)dv / q.sc);
+          T gh = gv;
+          if (q.partner) {
+            T gpv, dpv;
+            green_eval<T>(gp[X * S + Y], kpt, s6, s8, gpv, dpv);
+            gh = T(0.5) * (gv + (T)((double)gpv / q.sc));
+          }
+#pragma unroll
+          for (int r = 0; r < kAnyRC; ++r) {
+            if (r0 + r < R) {
+              const C2 sy = spec[((size_t)Y * R + r0 + r) * Mh + k];
+              hq[r].x += gv * sy.x; hq[r].y += gv * sy.y;
+              hd[r].x += dv * sy.x; hd[r].y += dv * sy.y;
+              hh[r].x += gh * sy.x; hh[r].y += gh * sy.y;
+            }
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < kAnyRC; ++r) {
+          if (r0 + r < R) {
+            const size_t idx = ((size_t)X * R + r0 + r) * Mh + k;
+            const C2 sx = spec[idx];
+            const double lam = tab->eigs[r0 + r];
+            qq += lam * ((double)sx.x * (double)hq[r].x + (double)sx.y * (double)hq[r].y);
+            dq += lam * ((double)sx.x * (double)hd[r].x + (double)sx.y * (double)hd[r].y);
+            spec_out[idx] = hh[r];
+          }
+        }
+      }
+    }
+    acc[0] += q.wk * qq;
+    virial_acc(q, dq, acc);
+  }
+  block_sum_store<7>(acc, part + 7 * blockIdx.x);
+}
+
+static int filter_grid(size_t Mh) {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  const size_t need = (Mh + kFilterThreads - 1) / kFilterThreads;
+  const size_t cap = (size_t)sms * 8;
+  return (int)(need < cap ? need : cap);
+}
+
+int filter_max_blocks() { return 148 * 8 * 4; }
+
 template <typename T>
 int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab,
-                  const float* deconv, int spme, void* spec, double* part, int* n_blocks, cudaStream_t s) {
+                  const float* deconv, int spme, void* spec, void* spec_out, double* part, int* n_blocks,
+                  cudaStream_t s) {
   using C2 = typename Cplx<T>::type;
   const size_t Mh = (size_t)mg.n[0] * mg.n[1] * mg.nzh;
-  const int blocks = (int)((Mh + kFilterThreads - 1) / kFilterThreads);
+  const int blocks = filter_grid(Mh);
   *n_blocks = blocks;
   const MeshDev g = to_dev(mg);
   C2* sp = reinterpret_cast<C2*>(spec);
@@ -220,19 +318,20 @@ int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, c
   else if (mg.S <= 8)
     k_filter<T, 8><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gp, tab, deconv, sp, part);
   else
-    return FD3_EINVAL;
+    k_filter_any<T><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gp, tab, deconv, sp,
+                                                      reinterpret_cast<C2*>(spec_out), part);
   FD3_LAUNCHED();
   return FD3_OK;
 }
 template int launch_filter<double>(const MeshGeom&, const CellInfo*, const GreenPair*, const Tables*, const float*,
-                                   int, void*, double*, int*, cudaStream_t);
+                                   int, void*, void*, double*, int*, cudaStream_t);
 template int launch_filter<float>(const MeshGeom&, const CellInfo*, const GreenPair*, const Tables*, const float*,
-                                  int, void*, double*, int*, cudaStream_t);
+                                  int, void*, void*, double*, int*, cudaStream_t);
 
 // ------------------------------------------------------------------ finalize
 // mode 0: energy [Hartree] and dE/dcell [Hartree/Bohr] with positions/shifts fixed (edge path)
 // mode 1: energy [eV] and ASE stress [eV/A^3] = (dE/dstrain) / Omega (fused path)
-__global__ void k_finalize(Partials p, const CellInfo* __restrict__ ci, int mode, double e_scale,
+__global__ void __launch_bounds__(1024) k_finalize(Partials p, const CellInfo* __restrict__ ci, int mode, double e_scale,
                            double* __restrict__ energy, double* __restrict__ out9) {
   double v[1 + 7 + 9 + 9];
   for (int k = 0; k < 26; ++k) v[k] = 0.0;
@@ -275,7 +374,7 @@ __global__ void k_finalize(Partials p, const CellInfo* __restrict__ ci, int mode
 
 int launch_finalize(const Partials& p, const CellInfo* ci, int mode, double e_scale, double* energy, double* out9,
                     cudaStream_t s) {
-  k_finalize<<<1, 256, 0, s>>>(p, ci, mode, e_scale, energy, out9);
+  k_finalize<<<1, 1024, 0, s>>>(p, ci, mode, e_scale, energy, out9);
   FD3_LAUNCHED();
   return FD3_OK;
 }

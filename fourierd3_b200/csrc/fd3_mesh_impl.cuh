@@ -39,8 +39,9 @@ static inline MeshDev to_dev(const MeshGeom& g) {
 // (odd p) or floor(u) (even p); local x = u - ref (odd) or u - ref - 1/2 (even).
 template <typename T>
 __device__ __forceinline__ void mesh_locate(const double* __restrict__ pos, int i, double ps, const CellInfo* ci,
-                                            const int* n, int P, int* base, T* xl) {
+                                            int n0, int n1, int n2, int P, int* base, T* xl) {
   const double x0 = pos[3 * i] * ps, x1 = pos[3 * i + 1] * ps, x2 = pos[3 * i + 2] * ps;
+  const int n[3] = {n0, n1, n2};
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const double u = n[a] * (x0 * ci->inv[a] + x1 * ci->inv[3 + a] + x2 * ci->inv[6 + a]);
@@ -69,164 +70,179 @@ __device__ __forceinline__ void stencil_weights(T x, T* w, T* dw) {
 }
 
 // ------------------------------------------------------------------ spread
-constexpr int kSpreadThreads = 256;
-constexpr int kSpreadPts = 2;          // points per thread (512-point tile)
+// Tile-owned spread. A CTA owns one (16 x 16 x 8)-point tile of one species; thread (lx, ly)
+// owns the z-row of 8 points at (lx, ly). The atoms whose stencil can reach the tile come from
+// the counting-sorted (tile, species) segments of the source tiles; they are examined 256 at a
+// time, the overlapping ones are compacted (warp ballots, sorted order kept) into shared memory
+// as three tile-local 1D weight rows (zero outside the stencil; stencil nodes that wrap onto
+// the same point are summed), and every thread accumulates w_x(lx) w_y(ly) w_z(z) c_r for its
+// row. Each mesh value is written exactly once: no atomics, no zero fill, fixed summation order.
+constexpr int kSpTX = 16, kSpTY = 16, kSpTZ = 8;
+constexpr int kSpThreads = kSpTX * kSpTY;
+constexpr int kSpRC = 4;                 // ranks accumulated per pass
 
-// candidate atoms staged in shared memory per pass (fits the 48 KB static limit)
-template <typename T, int P, int MAXR>
-struct SpreadChunk {
-  static constexpr int bytes_per = 12 + (3 * P + MAXR) * (int)sizeof(T);
-  static constexpr int value = bytes_per * 128 <= 40000 ? 128 : (bytes_per * 64 <= 40000 ? 64 : 32);
+template <typename T>
+struct SpChunk {
+  static constexpr int value = sizeof(T) == 8 ? 64 : 128;
 };
 
-template <typename T, int P, bool LAG, int MAXR>
-__global__ void __launch_bounds__(kSpreadThreads) k_spread(MeshDev g, const double* __restrict__ pos, double ps,
-                                                            const double* __restrict__ c6,
-                                                            const CellInfo* __restrict__ ci,
-                                                            const int* __restrict__ key_start,
-                                                            const int* __restrict__ order, T* __restrict__ rho) {
-  constexpr int kChunk = SpreadChunk<T, P, MAXR>::value;
-  __shared__ int s_base[kChunk][3];
-  __shared__ T s_w[kChunk][3][P];
-  __shared__ T s_c[kChunk][MAXR];
-  __shared__ int s_warp_cnt[kSpreadThreads / 32];
-  __shared__ int s_nc;
+template <typename T, int P, bool LAG>
+__global__ void __launch_bounds__(kSpThreads, 2) k_spread(MeshDev g, const double* __restrict__ pos, double ps,
+                                                       const double* __restrict__ c6,
+                                                       const CellInfo* __restrict__ ci,
+                                                       const int* __restrict__ key_start,
+                                                       const int* __restrict__ order, T* __restrict__ rho) {
+  constexpr int CH = SpChunk<T>::value;
+  __shared__ T s_wx[CH][kSpTX];
+  __shared__ T s_wy[CH][kSpTY];
+  __shared__ T s_wz[CH][kSpTZ];
+  __shared__ T s_c[CH][kSpRC];
+  __shared__ int s_a0[125], s_pref[126];
+  __shared__ int s_wcnt[kSpThreads / 32];
 
+  const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
   const int X = blockIdx.y;
   const int tile = blockIdx.x;
   const int tz = tile % g.nt[2];
   const int ty = (tile / g.nt[2]) % g.nt[1];
   const int tx = tile / (g.nt[2] * g.nt[1]);
   const int t0[3] = {tx * g.t[0], ty * g.t[1], tz * g.t[2]};
-  const int npts = g.t[0] * g.t[1] * g.t[2];
-  const int pf[3] = {P < g.n[0] ? P : g.n[0], P < g.n[1] ? P : g.n[1], P < g.n[2] ? P : g.n[2]};
+  const int lx = tid / kSpTY, ly = tid % kSpTY;
+  const bool row_ok = lx < g.t[0] && ly < g.t[1];
   const int R = g.R;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int nsrc = g.ns[0] * g.ns[1] * g.ns[2];
 
-  int pm[kSpreadPts][3];
-  bool pv[kSpreadPts];
-#pragma unroll
-  for (int q = 0; q < kSpreadPts; ++q) {
-    const int id = threadIdx.x + q * kSpreadThreads;
-    pv[q] = id < npts;
-    const int lz = id % g.t[2], ly = (id / g.t[2]) % g.t[1], lx = id / (g.t[2] * g.t[1]);
-    pm[q][0] = t0[0] + lx;
-    pm[q][1] = t0[1] + ly;
-    pm[q][2] = t0[2] + lz;
+  if (tid < nsrc) {
+    const int sxo = tid / (g.ns[1] * g.ns[2]), syo = (tid / g.ns[2]) % g.ns[1], szo = tid % g.ns[2];
+    const int sx = posmod(tx - sxo, g.nt[0]), sy = posmod(ty - syo, g.nt[1]), sz = posmod(tz - szo, g.nt[2]);
+    const int key = ((sx * g.nt[1] + sy) * g.nt[2] + sz) * g.S + X;
+    const int a0 = key_start[key];
+    s_a0[tid] = a0;
+    s_pref[tid + 1] = key_start[key + 1] - a0;
   }
-  T acc[kSpreadPts][MAXR];
-#pragma unroll
-  for (int q = 0; q < kSpreadPts; ++q)
-#pragma unroll
-    for (int r = 0; r < MAXR; ++r) acc[q][r] = T(0);
+  __syncthreads();
+  if (tid == 0) {
+    s_pref[0] = 0;
+    for (int k = 0; k < nsrc; ++k) s_pref[k + 1] += s_pref[k];
+  }
+  __syncthreads();
+  const int total = s_pref[nsrc];
+  const size_t M = (size_t)g.n[0] * g.n[1] * g.n[2];
 
-  for (int sxo = 0; sxo < g.ns[0]; ++sxo)
-    for (int syo = 0; syo < g.ns[1]; ++syo)
-      for (int szo = 0; szo < g.ns[2]; ++szo) {
-        const int sx = posmod(tx - sxo, g.nt[0]);
-        const int sy = posmod(ty - syo, g.nt[1]);
-        const int sz = posmod(tz - szo, g.nt[2]);
-        const int key = ((sx * g.nt[1] + sy) * g.nt[2] + sz) * g.S + X;
-        const int a0 = key_start[key], a1 = key_start[key + 1];
-        for (int c0 = a0; c0 < a1; c0 += kSpreadThreads) {
-          // each thread examines one candidate; keepers are compacted in candidate order
-          const int ca = c0 + threadIdx.x;
-          bool keep = false;
-          int base[3] = {0, 0, 0};
-          T xl[3] = {T(0), T(0), T(0)};
-          int atom = 0;
-          if (ca < a1) {
-            atom = order[ca];
-            mesh_locate<T>(pos, atom, ps, ci, g.n, P, base, xl);
-            keep = true;
+  for (int r0 = 0; r0 < R; r0 += kSpRC) {
+    T acc[kSpTZ][kSpRC];
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-              int d = t0[a] - base[a];
-              if (d < 0) d += g.n[a];
-              // the stencil covers offsets [0, pf) from base; the tile covers [d, d + t)
-              if (!(d < pf[a] || d + g.t[a] > g.n[a])) keep = false;
-            }
-          }
-          const unsigned bal = __ballot_sync(0xffffffffu, keep);
-          if (lane == 0) s_warp_cnt[wid] = __popc(bal);
-          __syncthreads();
-          int off = 0, tot = 0;
-          for (int w = 0; w < kSpreadThreads / 32; ++w) {
-            if (w < wid) off += s_warp_cnt[w];
-            tot += s_warp_cnt[w];
-          }
-          __syncthreads();   // s_warp_cnt is rewritten by the next candidate pass
-          // tot <= kSpreadThreads; stage in two halves if it exceeds the chunk
-          for (int h0 = 0; h0 < tot; h0 += kChunk) {
-            const int slot = off + __popc(bal & ((1u << lane) - 1u)) - h0;
-            if (keep && slot >= 0 && slot < kChunk) {
-              T w[3][P], dw[P];
-              stencil_weights<P, LAG, T>(xl[0], w[0], dw);
-              stencil_weights<P, LAG, T>(xl[1], w[1], dw);
-              stencil_weights<P, LAG, T>(xl[2], w[2], dw);
+    for (int z = 0; z < kSpTZ; ++z)
 #pragma unroll
-              for (int a = 0; a < 3; ++a) {
-                s_base[slot][a] = base[a];
-                if (pf[a] == P) {
+      for (int r = 0; r < kSpRC; ++r) acc[z][r] = T(0);
+
+    for (int c0 = 0; c0 < total; c0 += kSpThreads) {
+      // examine one candidate per thread
+      const int ca = c0 + tid;
+      bool keep = false;
+      int atom = 0, base[3] = {0, 0, 0};
+      T xl[3] = {T(0), T(0), T(0)};
+      if (ca < total) {
+        int seg = 0;
+        while (s_pref[seg + 1] <= ca) ++seg;
+        atom = order[s_a0[seg] + (ca - s_pref[seg])];
+        mesh_locate<T>(pos, atom, ps, ci, g.n[0], g.n[1], g.n[2], P, base, xl);
+        keep = true;
 #pragma unroll
-                  for (int k = 0; k < P; ++k) s_w[slot][a][k] = w[a][k];
-                } else {
-                  // fold stencil nodes that wrap onto the same mesh point (n < p)
-                  for (int k = 0; k < P; ++k) s_w[slot][a][k] = T(0);
-                  for (int k = 0; k < P; ++k) s_w[slot][a][k % pf[a]] += w[a][k];
-                }
-              }
-#pragma unroll
-              for (int r = 0; r < MAXR; ++r) s_c[slot][r] = r < R ? (T)c6[(size_t)atom * R + r] : T(0);
-            }
-            if (threadIdx.x == 0) s_nc = min(kChunk, tot - h0);
-            __syncthreads();
-            const int nc = s_nc;
-#pragma unroll
-            for (int q = 0; q < kSpreadPts; ++q) {
-              if (!pv[q]) continue;
-              for (int c = 0; c < nc; ++c) {
-                int kx = pm[q][0] - s_base[c][0];
-                if (kx < 0) kx += g.n[0];
-                if (kx >= pf[0]) continue;
-                int ky = pm[q][1] - s_base[c][1];
-                if (ky < 0) ky += g.n[1];
-                if (ky >= pf[1]) continue;
-                int kz = pm[q][2] - s_base[c][2];
-                if (kz < 0) kz += g.n[2];
-                if (kz >= pf[2]) continue;
-                const T w = s_w[c][0][kx] * s_w[c][1][ky] * s_w[c][2][kz];
-#pragma unroll
-                for (int r = 0; r < MAXR; ++r) acc[q][r] += w * s_c[c][r];
-              }
-            }
-            __syncthreads();
-          }
+        for (int a = 0; a < 3; ++a) {
+          int d = t0[a] - base[a];
+          if (d < 0) d += g.n[a];
+          // stencil offsets [0, min(P, n)) from base; the tile covers offsets [d, d + t)
+          const int pf = P < g.n[a] ? P : g.n[a];
+          if (!(d < pf || d + g.t[a] > g.n[a])) keep = false;
         }
       }
-  const size_t M = (size_t)g.n[0] * g.n[1] * g.n[2];
+      const unsigned bal = __ballot_sync(0xffffffffu, keep);
+      if (lane == 0) s_wcnt[wid] = __popc(bal);
+      __syncthreads();
+      int off = 0, tot = 0;
 #pragma unroll
-  for (int q = 0; q < kSpreadPts; ++q) {
-    if (!pv[q]) continue;
-    const size_t m = ((size_t)pm[q][0] * g.n[1] + pm[q][1]) * g.n[2] + pm[q][2];
+      for (int w = 0; w < kSpThreads / 32; ++w) {
+        off += w < wid ? s_wcnt[w] : 0;
+        tot += s_wcnt[w];
+      }
+      __syncthreads();   // s_wcnt is rewritten by the next examination pass
+      for (int h0 = 0; h0 < tot; h0 += CH) {
+        const int slot = off + __popc(bal & ((1u << lane) - 1u)) - h0;
+        if (keep && slot >= 0 && slot < CH) {
+          T w[3][P], dw[P];
 #pragma unroll
-    for (int r = 0; r < MAXR; ++r)
-      if (r < R) rho[((size_t)X * R + r) * M + m] = acc[q][r];
+          for (int a = 0; a < 3; ++a) stencil_weights<P, LAG, T>(xl[a], w[a], dw);
+#pragma unroll
+          for (int z = 0; z < kSpTX; ++z) s_wx[slot][z] = T(0);
+#pragma unroll
+          for (int z = 0; z < kSpTY; ++z) s_wy[slot][z] = T(0);
+#pragma unroll
+          for (int z = 0; z < kSpTZ; ++z) s_wz[slot][z] = T(0);
+#pragma unroll
+          for (int k = 0; k < P; ++k) {
+            int ix = (base[0] + k - t0[0]) % g.n[0]; if (ix < 0) ix += g.n[0];
+            int iy = (base[1] + k - t0[1]) % g.n[1]; if (iy < 0) iy += g.n[1];
+            int iz = (base[2] + k - t0[2]) % g.n[2]; if (iz < 0) iz += g.n[2];
+            if (ix < g.t[0]) s_wx[slot][ix] += w[0][k];
+            if (iy < g.t[1]) s_wy[slot][iy] += w[1][k];
+            if (iz < g.t[2]) s_wz[slot][iz] += w[2][k];
+          }
+#pragma unroll
+          for (int r = 0; r < kSpRC; ++r) s_c[slot][r] = r0 + r < R ? (T)c6[(size_t)atom * R + r0 + r] : T(0);
+        }
+        __syncthreads();
+        const int nc = min(CH, tot - h0);
+        if (row_ok) {
+          for (int c = 0; c < nc; ++c) {
+            const T wxy = s_wx[c][lx] * s_wy[c][ly];
+            if (wxy != T(0)) {
+              T cr[kSpRC];
+#pragma unroll
+              for (int r = 0; r < kSpRC; ++r) cr[r] = wxy * s_c[c][r];
+#pragma unroll
+              for (int z = 0; z < kSpTZ; ++z) {
+                const T wz = s_wz[c][z];
+#pragma unroll
+                for (int r = 0; r < kSpRC; ++r) acc[z][r] += wz * cr[r];
+              }
+            }
+          }
+        }
+        __syncthreads();
+      }
+    }
+    if (row_ok) {
+      const size_t m0 = ((size_t)(t0[0] + lx) * g.n[1] + (t0[1] + ly)) * g.n[2] + t0[2];
+#pragma unroll
+      for (int r = 0; r < kSpRC; ++r) {
+        if (r0 + r >= R) break;
+        T* dst = rho + ((size_t)X * R + r0 + r) * M + m0;
+        if (g.t[2] == kSpTZ) {
+          // the row starts on an 8-element boundary: two 16-byte stores (float) or four (double)
+          if (sizeof(T) == 4) {
+            float4* v = reinterpret_cast<float4*>(dst);
+            v[0] = make_float4((float)acc[0][r], (float)acc[1][r], (float)acc[2][r], (float)acc[3][r]);
+            v[1] = make_float4((float)acc[4][r], (float)acc[5][r], (float)acc[6][r], (float)acc[7][r]);
+          } else {
+            double2* v = reinterpret_cast<double2*>(dst);
+#pragma unroll
+            for (int z = 0; z < kSpTZ; z += 2) v[z / 2] = make_double2((double)acc[z][r], (double)acc[z + 1][r]);
+          }
+        } else {
+#pragma unroll
+          for (int z = 0; z < kSpTZ; ++z)
+            if (z < g.t[2]) dst[z] = acc[z][r];
+        }
+      }
+    }
   }
 }
 
 template <typename T, int P, bool LAG>
 static int spread_r(const MeshGeom& mg, dim3 grid, const double* pos, double ps, const double* c6,
                     const CellInfo* ci, const int* ks, const int* order, T* rho, cudaStream_t s) {
-  const MeshDev g = to_dev(mg);
-  if (mg.R <= 4)
-    k_spread<T, P, LAG, 4><<<grid, kSpreadThreads, 0, s>>>(g, pos, ps, c6, ci, ks, order, rho);
-  else if (mg.R <= 8)
-    k_spread<T, P, LAG, 8><<<grid, kSpreadThreads, 0, s>>>(g, pos, ps, c6, ci, ks, order, rho);
-  else if (mg.R <= 16)
-    k_spread<T, P, LAG, 16><<<grid, kSpreadThreads, 0, s>>>(g, pos, ps, c6, ci, ks, order, rho);
-  else
-    k_spread<T, P, LAG, 32><<<grid, kSpreadThreads, 0, s>>>(g, pos, ps, c6, ci, ks, order, rho);
+  k_spread<T, P, LAG><<<grid, kSpThreads, 0, s>>>(to_dev(mg), pos, ps, c6, ci, ks, order, rho);
   FD3_LAUNCHED();
   return FD3_OK;
 }
@@ -236,7 +252,9 @@ int launch_spread(const MeshGeom& mg, const double* pos, double pos_scale, const
                   const double* c6, const CellInfo* ci, const int* key_start, const int* order, T* rho,
                   cudaStream_t s) {
   (void)species;
-  if (mg.R > 32 || mg.order < 1 || mg.order > FD3_MAX_ORDER) return FD3_EINVAL;
+  if (mg.R > FD3_MAX_RANK || mg.order < 1 || mg.order > FD3_MAX_ORDER) return FD3_EINVAL;
+  if (mg.t[0] > kSpTX || mg.t[1] > kSpTY || mg.t[2] > kSpTZ || mg.ns[0] * mg.ns[1] * mg.ns[2] > 125)
+    return FD3_EINVAL;
   const dim3 grid(mg.nt[0] * mg.nt[1] * mg.nt[2], mg.S);
 #define FD3_SPREAD_CASE(PP)                                                                          \
   case PP:                                                                                           \
@@ -255,6 +273,7 @@ int launch_spread(const MeshGeom& mg, const double* pos, double pos_scale, const
 #undef FD3_SPREAD_CASE
   return FD3_EINVAL;
 }
+
 // ------------------------------------------------------------------ gather
 constexpr int kGatherWarps = 8;
 
@@ -278,7 +297,7 @@ __global__ void __launch_bounds__(32 * kGatherWarps) k_gather(MeshDev g, int n, 
     const int s = species[i];
     int base[3];
     T xl[3];
-    mesh_locate<T>(pos, i, ps, ci, g.n, P, base, xl);
+    mesh_locate<T>(pos, i, ps, ci, g.n[0], g.n[1], g.n[2], P, base, xl);
     T w[3][P], dw[3][P];
 #pragma unroll
     for (int a = 0; a < 3; ++a) stencil_weights<P, LAG, T>(xl[a], w[a], dw[a]);
@@ -290,29 +309,47 @@ __global__ void __launch_bounds__(32 * kGatherWarps) k_gather(MeshDev g, int n, 
 #pragma unroll
     for (int r = 0; r < MAXR; ++r) pr[r] = 0.0;
     double gu0 = 0, gu1 = 0, gu2 = 0;
-    constexpr int P3 = P * P * P;
-    for (int qn = lane; qn < P3; qn += 32) {
-      const int kx = qn / (P * P), ky = (qn / P) % P, kz = qn % P;
-      int ix = base[0] + kx; if (ix >= g.n[0]) ix -= g.n[0] * (ix / g.n[0]);
-      int iy = base[1] + ky; if (iy >= g.n[1]) iy -= g.n[1] * (iy / g.n[1]);
-      int iz = base[2] + kz; if (iz >= g.n[2]) iz -= g.n[2] * (iz / g.n[2]);
-      const size_t m = ((size_t)ix * g.n[1] + iy) * g.n[2] + iz;
-      const T W = w[0][kx] * w[1][ky] * w[2][kz];
-      const T Wx = dw[0][kx] * w[1][ky] * w[2][kz];
-      const T Wy = w[0][kx] * dw[1][ky] * w[2][kz];
-      const T Wz = w[0][kx] * w[1][ky] * dw[2][kz];
-      double cp = 0.0;
+    // lanes over the (y, z) stencil nodes, x nodes unrolled: every weight index is static
+    int ixs[P];
 #pragma unroll
-      for (int r = 0; r < MAXR; ++r) {
-        if (r < R) {
-          const double ph = (double)phi[((size_t)s * R + r) * M + m];
-          pr[r] += (double)W * ph;
-          cp += cl[r] * ph;
-        }
+    for (int kx = 0; kx < P; ++kx) {
+      int ix = base[0] + kx;
+      while (ix >= g.n[0]) ix -= g.n[0];
+      ixs[kx] = ix;
+    }
+    for (int q = lane; q < P * P; q += 32) {
+      const int ky = q / P, kz = q - ky * P;
+      T wy = T(0), dwy = T(0), wz = T(0), dwz = T(0);
+#pragma unroll
+      for (int k = 0; k < P; ++k) {
+        if (k == ky) { wy = w[1][k]; dwy = dw[1][k]; }
+        if (k == kz) { wz = w[2][k]; dwz = dw[2][k]; }
       }
-      gu0 += (double)Wx * cp;
-      gu1 += (double)Wy * cp;
-      gu2 += (double)Wz * cp;
+      int iy = base[1] + ky;
+      while (iy >= g.n[1]) iy -= g.n[1];
+      int iz = base[2] + kz;
+      while (iz >= g.n[2]) iz -= g.n[2];
+      const T wyz = wy * wz, dyz = dwy * wz, ydz = wy * dwz;
+#pragma unroll
+      for (int kx = 0; kx < P; ++kx) {
+        const size_t m = ((size_t)ixs[kx] * g.n[1] + iy) * g.n[2] + iz;
+        const T W = w[0][kx] * wyz;
+        const T Wx = dw[0][kx] * wyz;
+        const T Wy = w[0][kx] * dyz;
+        const T Wz = w[0][kx] * ydz;
+        double cp = 0.0;
+#pragma unroll
+        for (int r = 0; r < MAXR; ++r) {
+          if (r < R) {
+            const double ph = (double)phi[((size_t)s * R + r) * M + m];
+            pr[r] += (double)W * ph;
+            cp += cl[r] * ph;
+          }
+        }
+        gu0 += (double)Wx * cp;
+        gu1 += (double)Wy * cp;
+        gu2 += (double)Wz * cp;
+      }
     }
 #pragma unroll
     for (int r = 0; r < MAXR; ++r) pr[r] = warp_sum(pr[r]);

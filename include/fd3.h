@@ -134,6 +134,23 @@ FD3_API int fd3_neighbor_fill(int64_t n_atoms, const double* d_pos_ang, const do
                       void* d_work, size_t work_bytes, int64_t capacity, int64_t* d_src, int64_t* d_dst,
                       int32_t* d_shift, int64_t* h_count, void* stream);
 
+/*
+ * Neighbour list with no allocation and no workspace argument. No counterpart in the
+ * reference: it exists for callers that cannot allocate device memory themselves (an MD
+ * engine or host runtime that owns all device memory and forbids raw allocations in its
+ * timestep, or code with a fixed, pre-checked memory budget). Same inputs, outputs and
+ * errors as fd3_neighbor_fill, but the cell-list scratch is a fixed 6 MiB device array
+ * inside libfd3 (held on every GPU that loads the library until exit), enough for about
+ * 65,000 atoms; larger inputs return FD3_EINVAL with the bytes needed. All calls share the
+ * array and leave their data in it (the parts that must start at zero are cleared on each
+ * call), so calls that overlap on the GPU race and must be serialised by the caller. The
+ * first call on a device looks up the array's address with that device current; make it
+ * before any stream capture.
+ */
+FD3_API int fd3_neighbor_fill_static(int64_t n_atoms, const double* d_pos_ang, const double* h_cell_ang,
+                                     double r_cut_ang, int64_t capacity, int64_t* d_src, int64_t* d_dst,
+                                     int32_t* d_shift, int64_t* h_count, void* stream);
+
 /* Per-stage timing of the last call on this plan, from CUDA events recorded on the
  * launching stream between stages (cell_list, cn_c6, mesh_sort, spread, fft_r2c,
  * filter, fft_c2r, gather, cn_adjoint, finalize). fd3_profile_read waits for the last

@@ -250,14 +250,20 @@ struct Work {
   double *cn, *c6, *dc6, *gcn;
   double *self_part, *kspc_part, *cnv_part, *mcell_part;
   int *mkeys, *mcount, *mstart, *morder;
+  MeshRecords rec;
   CellList cl;
+  HitStore hits;
   void *rho, *spec, *spec2, *fftw;
 };
 
-void carve(const fd3_plan* p, int64_t N, int64_t K, Carver& c, Work& w) {
+// K = number of cell-list bins of the fused path, 0 for the edge-list path (no cell list).
+void carve(const fd3_plan* p, int64_t N, int64_t K_in, Carver& c, Work& w) {
+  const bool fused = K_in > 0;
+  const int64_t K = fused ? K_in : 1;
+  const size_t es = p->precision == FD3_PREC_FP64 ? sizeof(double) : sizeof(float);
   const int R = p->R;
   // per-block partials: per-atom kernels use ceil(N/8) blocks, the bin kernels one per bin
-  const int64_t nblk = ((N + 7) / 8 > K ? (N + 7) / 8 : K) + 1;
+  const int64_t nblk = (2 * ((N + 7) / 8) > K ? 2 * ((N + 7) / 8) : K) + 1;
   w.ci = c.take<CellInfo>(1);
   w.cn = c.take<double>(N);
   w.c6 = c.take<double>(N * R);
@@ -276,6 +282,11 @@ void carve(const fd3_plan* p, int64_t N, int64_t K, Carver& c, Work& w) {
   }
   w.kspc_part = c.take<double>(7 * (filter_max_blocks() + 1));
   w.mkeys = c.take<int>(N);
+  const size_t P3 = mesh ? (size_t)3 * p->P : 1;
+  w.rec.b = c.take<int4>(N);
+  w.rec.w = c.take<char>(N * P3 * es);
+  w.rec.dw = c.take<char>(N * P3 * es);
+  w.rec.c = c.take<char>(N * p->R * es);
   w.mcount = c.take<int>(Kmesh);
   w.mstart = c.take<int>(Kmesh + 1);
   w.morder = c.take<int>(N);
@@ -286,7 +297,15 @@ void carve(const fd3_plan* p, int64_t N, int64_t K, Carver& c, Work& w) {
   w.cl.xs = c.take<double4>(N);
   w.cl.meta = c.take<int4>(N);
   w.cl.off = c.take<int4>(N);
-  const size_t es = p->precision == FD3_PREC_FP64 ? sizeof(double) : sizeof(float);
+  // CN pair records of the fused path
+  const int64_t hn = fused ? N : 0;
+  w.hits.cap = kHitCap;
+  w.hits.is_double = p->precision == FD3_PREC_FP64;
+  w.hits.j = c.take<int>(hn * kHitCap);
+  w.hits.a = c.take<char>(hn * kHitCap * es);
+  w.hits.d = c.take<char>(hn * kHitCap * 3 * es);
+  w.hits.n = c.take<int>(N);
+  w.hits.ovf = c.take<int>(1);
   const size_t C = (size_t)p->S * p->R;
   w.rho = c.take<char>(mesh ? C * M * es : 1);
   w.spec = c.take<char>(mesh ? C * Mh * 2 * es : 1);
@@ -300,7 +319,7 @@ extern "C" int fd3_workspace_size(const fd3_plan* p, int64_t n_atoms, int64_t n_
   if (!p || !bytes || n_atoms < 0) return FD3_EINVAL;
   Carver c;
   Work w;
-  carve(p, n_atoms, n_bins > 0 ? n_bins : 1, c, w);
+  carve(p, n_atoms, n_bins > 0 ? n_bins : 0, c, w);
   *bytes = c.off + 256;
   return FD3_OK;
 }
@@ -339,7 +358,7 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
   FD3_TRY(launch_mesh_keys(mg, N, pos, ps, species, w.ci, w.mkeys, s));
   FD3_TRY(counting_sort(w.mkeys, N, Kmesh, w.mcount, w.mstart, w.morder, s));
   prof_mark(p, s, "mesh_sort");
-  FD3_TRY(launch_spread<T>(mg, pos, ps, species, w.c6, w.ci, w.mstart, w.morder, (T*)w.rho, s));
+  FD3_TRY(launch_spread<T>(mg, N, pos, ps, species, w.c6, w.ci, w.mstart, w.morder, w.rec, (T*)w.rho, s));
   prof_mark(p, s, "spread");
   FD3_CUFFT(cufftSetStream(p->fwd, s));
   FD3_CUFFT(cufftSetWorkArea(p->fwd, w.fftw));
@@ -361,8 +380,8 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
   else
     FD3_CUFFT(cufftExecC2R(p->inv, (cufftComplex*)hspec, (cufftReal*)w.rho));
   prof_mark(p, s, "fft_c2r");
-  FD3_TRY(launch_gather<T>(mg, N, pos, ps, species, w.c6, w.dc6, w.ci, p->d_tab, w.morder, (const T*)w.rho, w.gcn,
-                           gpos, mcell, n_mcell, s));
+  FD3_TRY(launch_gather<T>(mg, N, pos, ps, species, w.c6, w.dc6, w.ci, p->d_tab, w.morder, w.rec, (const T*)w.rho,
+                           w.gcn, gpos, mcell, n_mcell, s));
   prof_mark(p, s, "gather");
   return FD3_OK;
 }
@@ -390,7 +409,7 @@ extern "C" int fd3_energy_edges(fd3_plan* p, int64_t n_atoms, const double* d_po
   cudaStream_t s = (cudaStream_t)stream;
   const int N = (int)n_atoms;
   Work w;
-  FD3_TRY(check_work(p, N, 1, d_work, work_bytes, w));
+  FD3_TRY(check_work(p, N, 0, d_work, work_bytes, w));
   prof_begin(p, s);
   FD3_TRY(launch_cellinfo(d_cell, 1.0, w.ci, s));
   FD3_CUDA(cudaMemsetAsync(w.cn, 0, sizeof(double) * N, s));
@@ -435,12 +454,12 @@ extern "C" int fd3_energy_forces_stress(fd3_plan* p, int64_t n_atoms, const doub
   prof_mark(p, s, "cell_list");
   int n_self = 0, n_kspc = 0, n_mcell = 0, n_cnv = 0;
   FD3_TRY(launch_cn_c6_cells(g, N, w.cl, d_pos_ang, d_species, p->d_tab, p->d_eigvecs, p->R, w.cn, w.c6, w.dc6,
-                             w.self_part, &n_self, s));
+                             w.self_part, &n_self, w.hits, s));
   prof_mark(p, s, "cn_c6");
   // the mesh gradient (Hartree/Bohr) is staged in d_forces, then finished by the CN adjoint
   FD3_TRY(run_mesh(p, N, d_pos_ang, kAngToBohr, d_species, w, true, d_forces, nullptr, &n_kspc, &n_mcell, s));
   FD3_TRY(launch_cn_adjoint_cells(g, N, w.cl, d_pos_ang, d_species, p->d_tab, w.gcn, d_forces,
-                                  -kHartreeToEv * kAngToBohr, w.cnv_part, &n_cnv, s));
+                                  -kHartreeToEv * kAngToBohr, w.cnv_part, &n_cnv, w.hits, s));
   prof_mark(p, s, "cn_adjoint");
   Partials pa{w.self_part, n_self, w.kspc_part, n_kspc, w.cnv_part, n_cnv, nullptr, 0};
   FD3_TRY(launch_finalize(pa, w.ci, 1, kHartreeToEv, d_energy, d_stress, s));

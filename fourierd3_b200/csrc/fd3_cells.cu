@@ -288,58 +288,6 @@ __device__ __forceinline__ void visit_neighbors(const GridDev& g, const int* __r
   }
 }
 
-// ------------------------------------------------------------------ C6 factors
-// Softmax interpolation over the 7 reference CNs and the rank-r factors
-// c_r = sum_p w_p V[s, p, r] (core.py:449-478, 525-532), its CN derivative and the self
-// term sum_r lambda_r c_r^2 phi_ss(0) (core.py:545-550). Whole warp, lane-parallel.
-__device__ __forceinline__ double c6_factors_warp(double cn_raw, int s, const Tables* __restrict__ tab,
-                                                  const double* __restrict__ V, int R, double* __restrict__ c6,
-                                                  double* __restrict__ dc6, double* cn_out) {
-  const int lane = threadIdx.x & 31;
-  double cn = cn_raw, slope = 1.0;
-  if (tab->has_cncorr) {
-    slope = tab->cncorr[2 * s + 1];
-    cn = slope * cn_raw + tab->cncorr[2 * s + 0];
-  }
-  double logit = -INFINITY, dl = 0.0;
-  bool valid = false;
-  if (lane < 7) {
-    const double ref = tab->cnref[7 * s + lane];
-    valid = ref != -1.0;
-    const double diff = cn - ref;
-    if (valid) {
-      logit = -4.0 * (diff * diff);
-      dl = -8.0 * diff;
-    }
-  }
-  const double mx = warp_max(logit);
-  const double e = valid ? exp(logit - mx) : 0.0;
-  const double w = e / warp_sum(e);
-  const double dlbar = warp_sum(w * dl);
-  const double wd = w * (dl - dlbar);
-  double wp[7], wdp[7];
-#pragma unroll
-  for (int p = 0; p < 7; ++p) {
-    wp[p] = __shfl_sync(0xffffffffu, w, p);
-    wdp[p] = __shfl_sync(0xffffffffu, wd, p);
-  }
-  double selfv = 0.0;
-  for (int r = lane; r < R; r += 32) {
-    double c = 0.0, dc = 0.0;
-#pragma unroll
-    for (int p = 0; p < 7; ++p) {
-      const double v = V[(7 * s + p) * R + r];
-      c += wp[p] * v;
-      dc += wdp[p] * v;
-    }
-    c6[r] = c;
-    dc6[r] = slope * dc;
-    selfv += tab->eigs[r] * c * c * tab->selfcont[s];
-  }
-  if (lane == 0 && cn_out) *cn_out = cn;
-  return warp_sum(selfv);
-}
-
 constexpr int kWarpsPerBlock = 8;
 
 // Per-atom traversal straight from global memory: the path for bins whose neighbourhood does not
@@ -465,118 +413,196 @@ __device__ __forceinline__ void wrapped_pos(const GridDev& g, double4 x, int4 m,
   w2 = x.z - (m.x * g.cell[2] + m.y * g.cell[5] + m.z * g.cell[8]);
 }
 
-__global__ void __launch_bounds__(256) k_cn_c6_bins(GridDev g, const int* __restrict__ bin_start,
-                                                   const double4* __restrict__ xs, const int4* __restrict__ meta,
-                                                   const int4* __restrict__ off, const Tables* __restrict__ tab,
-                                                   const double* __restrict__ V, int R, double* __restrict__ cn,
-                                                   double* __restrict__ c6, double* __restrict__ dc6,
-                                                   double* __restrict__ self_part) {
+// The forward CN kernel also records, per atom, every pair with a non-zero CN derivative:
+// neighbour id, f'(r)/r and the Bohr vector d (HitList, TE = double for the plain form, float for
+// the mixed form). The adjoint then streams those records instead of searching the cell list a
+// second time. An atom with more than `cap` such pairs (or one handled by the global-memory path)
+// is marked n = -1 and the adjoint recomputes it.
+template <typename TE>
+struct HitList {
+  int* j;
+  TE* a;
+  TE* d;
+  int* n;
+  int cap;
+};
+
+// CN of the atoms of one bin from the shared-memory stage (raw CN, before cncorr), plus the
+// pair records. Bins whose neighbourhood does not fit the stage mark their atoms n = -2 and
+// leave them to k_cn_global.
+template <typename TE, typename TC>
+__global__ void __launch_bounds__(256) k_cn_bins(GridDev g, const int* __restrict__ bin_start,
+                                                const double4* __restrict__ xs, const int4* __restrict__ meta,
+                                                const Tables* __restrict__ tab, double* __restrict__ cn,
+                                                HitList<TE> hl, int* __restrict__ ovf) {
   __shared__ BinStage st;
-  __shared__ double wsum[kWarpsPerBlock];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int b = blockIdx.x;
   const int total = stage_bin(g, b, bin_start, xs, meta, st, nullptr, nullptr);
   const int s0 = bin_start[b], s1 = bin_start[b + 1];
-  double selfv = 0.0;
+  if (total < 0) {
+    for (int t = s0 + threadIdx.x; t < s1; t += blockDim.x) hl.n[t] = -2;
+    if (threadIdx.x == 0 && s1 > s0) atomicAdd(ovf, 1);
+    return;
+  }
+  const unsigned lt = (1u << lane) - 1u;
+  const TC rc = (TC)tab->r_cut;
   for (int t = s0 + wid; t < s1; t += kWarpsPerBlock) {
     const double4 xi = xs[t];
     const int4 mi = meta[t];
-    const int si = (int)xi.w;
-    double cn_raw;
-    if (total >= 0) {
-      double w0, w1, w2;
-      wrapped_pos(g, xi, mi, w0, w1, w2);
-      const double rci = tab->rcov[si];
-      double acc = 0.0;
-      for (int c = lane; c < total; c += 32) {
+    double w0, w1, w2;
+    wrapped_pos(g, xi, mi, w0, w1, w2);
+    const TC rci = (TC)tab->rcov[(int)xi.w];
+    TC acc = TC(0);
+    int cnt = 0;
+    const size_t hb = (size_t)t * hl.cap;
+    for (int c0 = 0; c0 < total; c0 += 32) {
+      const int c = c0 + lane;
+      bool hit = false;
+      TC v0 = 0, v1 = 0, v2 = 0, a = 0;
+      if (c < total) {
         const double4 pj = st.p[c];
         const double d0 = pj.x - w0, d1 = pj.y - w1, d2 = pj.z - w2;
         if (d0 * d0 + d1 * d1 + d2 * d2 < g.rc2) {
-          const double v0 = d0 * kAngToBohr, v1 = d1 * kAngToBohr, v2 = d2 * kAngToBohr;
-          double f, df;
-          cn_edge(sqrt(v0 * v0 + v1 * v1 + v2 * v2), rci + tab->rcov[(int)pj.w], tab->r_cut, f, df);
-          acc += f;
+          v0 = (TC)(d0 * kAngToBohr);
+          v1 = (TC)(d1 * kAngToBohr);
+          v2 = (TC)(d2 * kAngToBohr);
+          const TC r2 = v0 * v0 + v1 * v1 + v2 * v2;
+          if (r2 > TC(1e-12)) {
+            TC f;
+            cn_pair<TC>(r2, rci + (TC)tab->rcov[(int)pj.w], rc, f, a);
+            acc += f;
+            hit = a != TC(0);
+          }
         }
       }
-      cn_raw = warp_sum(acc);
-    } else {
-      cn_raw = cn_atom_global(g, bin_start, xs, meta, off, tab, t);
+      const unsigned m = __ballot_sync(0xffffffffu, hit);
+      const int pos = cnt + __popc(m & lt);
+      if (hit && pos < hl.cap) {
+        hl.j[hb + pos] = st.j[c];
+        hl.a[hb + pos] = (TE)a;
+        hl.d[3 * (hb + pos)] = (TE)v0;
+        hl.d[3 * (hb + pos) + 1] = (TE)v1;
+        hl.d[3 * (hb + pos) + 2] = (TE)v2;
+      }
+      cnt += __popc(m);
     }
-    const int i = mi.w;
-    selfv += c6_factors_warp(cn_raw, si, tab, V, R, c6 + (size_t)i * R, dc6 + (size_t)i * R, cn + i);
+    const double cnv = warp_sum((double)acc);
+    if (lane == 0) {
+      hl.n[t] = cnt <= hl.cap ? cnt : -1;
+      if (cnt > hl.cap) atomicAdd(ovf, 1);
+      cn[mi.w] = cnv;
+    }
   }
-  if (lane == 0) wsum[wid] = selfv;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double sum = 0.0;
-    for (int w = 0; w < kWarpsPerBlock; ++w) sum += wsum[w];
-    self_part[blockIdx.x] = sum;
+}
+
+constexpr int kFallbackBlocks = 148 * 4;
+
+// Raw CN of atoms whose bin overflowed the stage, straight from the cell list in global memory.
+// Returns at once when no bin overflowed (the counter is zero).
+__global__ void __launch_bounds__(256) k_cn_global(GridDev g, int n, const int* __restrict__ bin_start,
+                                                  const double4* __restrict__ xs, const int4* __restrict__ meta,
+                                                  const int4* __restrict__ off, const Tables* __restrict__ tab,
+                                                  double* __restrict__ cn, int* __restrict__ hit_n,
+                                                  const int* __restrict__ ovf) {
+  if (*ovf == 0) return;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int t = blockIdx.x * kWarpsPerBlock + wid; t < n; t += gridDim.x * kWarpsPerBlock) {
+    if (hit_n[t] != -2) continue;
+    const double v = cn_atom_global(g, bin_start, xs, meta, off, tab, t);
+    if (lane == 0) {
+      cn[meta[t].w] = v;
+      hit_n[t] = -1;
+    }
   }
 }
 
 int launch_cn_c6_cells(const CellGrid& g, int n, const CellList& cl, const double* pos_ang,
                        const int32_t* species, const Tables* tab, const double* eigvecs, int R, double* cn,
-                       double* c6, double* dc6, double* self_part, int* n_self_blocks, cudaStream_t s) {
+                       double* c6, double* dc6, double* self_part, int* n_self_blocks, const HitStore& hs,
+                       cudaStream_t s) {
   (void)pos_ang;
-  (void)species;
-  (void)n;
   const int K = g.nb[0] * g.nb[1] * g.nb[2];
-  *n_self_blocks = K;
-  k_cn_c6_bins<<<K, 32 * kWarpsPerBlock, 0, s>>>(to_dev(g), cl.bin_start, cl.xs, cl.meta, cl.off, tab, eigvecs, R,
-                                                  cn, c6, dc6, self_part);
+  FD3_CUDA(cudaMemsetAsync(hs.ovf, 0, sizeof(int), s));
+  if (hs.is_double)
+    k_cn_bins<double, double><<<K, 32 * kWarpsPerBlock, 0, s>>>(
+        to_dev(g), cl.bin_start, cl.xs, cl.meta, tab, cn,
+        HitList<double>{hs.j, (double*)hs.a, (double*)hs.d, hs.n, hs.cap}, hs.ovf);
+  else
+    k_cn_bins<float, float><<<K, 32 * kWarpsPerBlock, 0, s>>>(
+        to_dev(g), cl.bin_start, cl.xs, cl.meta, tab, cn,
+        HitList<float>{hs.j, (float*)hs.a, (float*)hs.d, hs.n, hs.cap}, hs.ovf);
   FD3_LAUNCHED();
-  return FD3_OK;
+  const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  if (blocks > 0) {
+    const int fb = blocks < kFallbackBlocks ? blocks : kFallbackBlocks;
+    k_cn_global<<<fb, 32 * kWarpsPerBlock, 0, s>>>(to_dev(g), n, cl.bin_start, cl.xs, cl.meta, cl.off, tab, cn,
+                                                    hs.n, hs.ovf);
+    FD3_LAUNCHED();
+  }
+  return launch_c6_atoms(n, species, tab, eigvecs, R, cn, c6, dc6, self_part, n_self_blocks, s);
 }
 
 // CN adjoint: dE/dx_i = -sum_(j,S) (g_i + g_j) f'(r) d / r  (the list is symmetric), and the
 // strain virial W_ab = sum_i g_i sum_(j,S) f'(r) d_a d_b / r  (Bohr, Hartree). The force written
-// is out_scale * (mesh gradient already in grad + CN gradient).
-__global__ void __launch_bounds__(256) k_cn_adjoint_bins(GridDev g, const int* __restrict__ bin_start,
-                                                        const double4* __restrict__ xs,
-                                                        const int4* __restrict__ meta, const int4* __restrict__ off,
-                                                        const Tables* __restrict__ tab,
+// is out_scale * (mesh gradient already in grad + CN gradient). One warp per atom streams the
+// atom's recorded pairs; atoms without a record (n < 0) are left to k_cn_adjoint_global.
+template <typename TE>
+__global__ void __launch_bounds__(256) k_cn_adjoint_hits(int n, const int4* __restrict__ meta,
                                                         const double* __restrict__ gcn, double* __restrict__ grad,
-                                                        double out_scale, double* __restrict__ vir_part) {
-  __shared__ BinStage st;
-  __shared__ double s_g[kBinCap];
+                                                        double out_scale, double* __restrict__ vir_part,
+                                                        HitList<TE> hl) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int b = blockIdx.x;
-  const int total = stage_bin(g, b, bin_start, xs, meta, st, s_g, gcn);
-  const int s0 = bin_start[b], s1 = bin_start[b + 1];
+  const int t = blockIdx.x * kWarpsPerBlock + wid;
   double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  for (int t = s0 + wid; t < s1; t += kWarpsPerBlock) {
-    const double4 xi = xs[t];
-    const int4 mi = meta[t];
-    const int i = mi.w;
-    double f[3] = {0, 0, 0};
-    if (total >= 0) {
-      double w0, w1, w2;
-      wrapped_pos(g, xi, mi, w0, w1, w2);
-      const double rci = tab->rcov[(int)xi.w];
-      const double gi = gcn[i];
-      for (int c = lane; c < total; c += 32) {
-        const double4 pj = st.p[c];
-        const double d0 = pj.x - w0, d1 = pj.y - w1, d2 = pj.z - w2;
-        if (d0 * d0 + d1 * d1 + d2 * d2 < g.rc2) {
-          const double v0 = d0 * kAngToBohr, v1 = d1 * kAngToBohr, v2 = d2 * kAngToBohr;
-          const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-          double fe, df;
-          cn_edge(r, rci + tab->rcov[(int)pj.w], tab->r_cut, fe, df);
-          if (r > 1e-6) {
-            const double a = df / r;
-            const double w = (gi + s_g[c]) * a;
-            f[0] -= w * v0;
-            f[1] -= w * v1;
-            f[2] -= w * v2;
-            const double bb = gi * a;
-            v[0] += bb * v0 * v0; v[1] += bb * v0 * v1; v[2] += bb * v0 * v2;
-            v[4] += bb * v1 * v1; v[5] += bb * v1 * v2; v[8] += bb * v2 * v2;
-          }
-        }
-      }
-    } else {
-      cn_adjoint_atom_global(g, bin_start, xs, meta, off, tab, gcn, t, f, v);
+  const int nh = t < n ? hl.n[t] : -1;
+  if (nh >= 0) {
+    const int i = meta[t].w;
+    double f0 = 0, f1 = 0, f2 = 0;
+    const double gi = gcn[i];
+    const size_t hb = (size_t)t * hl.cap;
+    for (int e = lane; e < nh; e += 32) {
+      const double a = (double)hl.a[hb + e];
+      const double v0 = (double)hl.d[3 * (hb + e)], v1 = (double)hl.d[3 * (hb + e) + 1],
+                   v2 = (double)hl.d[3 * (hb + e) + 2];
+      const double w = (gi + gcn[hl.j[hb + e]]) * a;
+      f0 -= w * v0;
+      f1 -= w * v1;
+      f2 -= w * v2;
+      const double bb = gi * a;
+      v[0] += bb * v0 * v0; v[1] += bb * v0 * v1; v[2] += bb * v0 * v2;
+      v[4] += bb * v1 * v1; v[5] += bb * v1 * v2; v[8] += bb * v2 * v2;
     }
+    f0 = warp_sum(f0);
+    f1 = warp_sum(f1);
+    f2 = warp_sum(f2);
+    if (lane == 0) {
+      grad[3 * i] = out_scale * (grad[3 * i] + f0);
+      grad[3 * i + 1] = out_scale * (grad[3 * i + 1] + f1);
+      grad[3 * i + 2] = out_scale * (grad[3 * i + 2] + f2);
+    }
+  }
+  v[3] = v[1];
+  v[6] = v[2];
+  v[7] = v[5];
+  block_sum_store<9>(v, vir_part + 9 * blockIdx.x);
+}
+
+__global__ void __launch_bounds__(256) k_cn_adjoint_global(GridDev g, int n, const int* __restrict__ bin_start,
+                                                          const double4* __restrict__ xs,
+                                                          const int4* __restrict__ meta,
+                                                          const int4* __restrict__ off, const Tables* __restrict__ tab,
+                                                          const double* __restrict__ gcn, double* __restrict__ grad,
+                                                          double out_scale, double* __restrict__ vir_part,
+                                                          const int* __restrict__ hit_n, const int* __restrict__ ovf) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  const bool any = *ovf != 0;
+  for (int t = blockIdx.x * kWarpsPerBlock + wid; any && t < n; t += gridDim.x * kWarpsPerBlock) {
+    if (hit_n[t] >= 0) continue;
+    const int i = meta[t].w;
+    double f[3] = {0, 0, 0};
+    cn_adjoint_atom_global(g, bin_start, xs, meta, off, tab, gcn, t, f, v);
     f[0] = warp_sum(f[0]);
     f[1] = warp_sum(f[1]);
     f[2] = warp_sum(f[2]);
@@ -594,14 +620,25 @@ __global__ void __launch_bounds__(256) k_cn_adjoint_bins(GridDev g, const int* _
 
 int launch_cn_adjoint_cells(const CellGrid& g, int n, const CellList& cl, const double* pos_ang,
                             const int32_t* species, const Tables* tab, const double* gcn, double* grad,
-                            double out_scale, double* vir_part, int* n_blocks, cudaStream_t s) {
+                            double out_scale, double* vir_part, int* n_blocks, const HitStore& hs,
+                            cudaStream_t s) {
   (void)pos_ang;
   (void)species;
-  (void)n;
-  const int K = g.nb[0] * g.nb[1] * g.nb[2];
-  *n_blocks = K;
-  k_cn_adjoint_bins<<<K, 32 * kWarpsPerBlock, 0, s>>>(to_dev(g), cl.bin_start, cl.xs, cl.meta, cl.off, tab, gcn,
-                                                       grad, out_scale, vir_part);
+  const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  const int fb = blocks < kFallbackBlocks ? blocks : kFallbackBlocks;
+  *n_blocks = blocks + fb;
+  if (blocks == 0) return FD3_OK;
+  if (hs.is_double)
+    k_cn_adjoint_hits<double><<<blocks, 32 * kWarpsPerBlock, 0, s>>>(
+        n, cl.meta, gcn, grad, out_scale, vir_part,
+        HitList<double>{hs.j, (double*)hs.a, (double*)hs.d, hs.n, hs.cap});
+  else
+    k_cn_adjoint_hits<float><<<blocks, 32 * kWarpsPerBlock, 0, s>>>(
+        n, cl.meta, gcn, grad, out_scale, vir_part, HitList<float>{hs.j, (float*)hs.a, (float*)hs.d, hs.n, hs.cap});
+  FD3_LAUNCHED();
+  k_cn_adjoint_global<<<fb, 32 * kWarpsPerBlock, 0, s>>>(to_dev(g), n, cl.bin_start, cl.xs, cl.meta, cl.off, tab,
+                                                          gcn, grad, out_scale, vir_part + 9 * (size_t)blocks, hs.n,
+                                                          hs.ovf);
   FD3_LAUNCHED();
   return FD3_OK;
 }
@@ -631,36 +668,72 @@ int launch_cn_edges(int64_t n_edges, const double* pos, const int32_t* species, 
   return FD3_OK;
 }
 
+// Softmax interpolation over the 7 reference CNs and the rank-r factors
+// c_r = sum_p w_p V[s, p, r] (core.py:449-478, 525-532), their CN derivative (times the
+// cncorr slope) and the self term sum_r lambda_r c_r^2 phi_ss(0) (core.py:545-550). One thread
+// per atom; cn holds the raw CN on entry and the corrected CN on exit.
 __global__ void __launch_bounds__(256) k_c6_atoms(int n, const int32_t* __restrict__ species,
                                                  const Tables* __restrict__ tab, const double* __restrict__ V, int R,
                                                  double* __restrict__ cn, double* __restrict__ c6,
                                                  double* __restrict__ dc6, double* __restrict__ self_part) {
-  __shared__ double wsum[kWarpsPerBlock];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int i = blockIdx.x * kWarpsPerBlock + wid;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
   double selfv = 0.0;
   if (i < n) {
-    const double cn_raw = cn[i];
-    __syncwarp();
-    selfv = c6_factors_warp(cn_raw, species[i], tab, V, R, c6 + (size_t)i * R, dc6 + (size_t)i * R, cn + i);
+    const int s = species[i];
+    double cnv = cn[i], slope = 1.0;
+    if (tab->has_cncorr) {
+      slope = tab->cncorr[2 * s + 1];
+      cnv = slope * cnv + tab->cncorr[2 * s + 0];
+    }
+    double lg[7], dl[7];
+    double mx = -INFINITY;
+#pragma unroll
+    for (int p = 0; p < 7; ++p) {
+      const double ref = tab->cnref[7 * s + p];
+      const double diff = cnv - ref;
+      const bool ok = ref != -1.0;
+      lg[p] = ok ? -4.0 * (diff * diff) : -INFINITY;
+      dl[p] = ok ? -8.0 * diff : 0.0;
+      mx = fmax(mx, lg[p]);
+    }
+    double sum = 0.0;
+#pragma unroll
+    for (int p = 0; p < 7; ++p) {
+      lg[p] = lg[p] == -INFINITY ? 0.0 : exp(lg[p] - mx);
+      sum += lg[p];
+    }
+    const double inv = 1.0 / sum;
+    double dlbar = 0.0;
+#pragma unroll
+    for (int p = 0; p < 7; ++p) {
+      lg[p] *= inv;                   // softmax weight w_p
+      dlbar += lg[p] * dl[p];
+    }
+    for (int r = 0; r < R; ++r) {
+      double c = 0.0, d = 0.0;
+#pragma unroll
+      for (int p = 0; p < 7; ++p) {
+        const double v = V[(7 * s + p) * R + r];
+        c += lg[p] * v;
+        d += lg[p] * (dl[p] - dlbar) * v;
+      }
+      c6[(size_t)i * R + r] = c;
+      dc6[(size_t)i * R + r] = slope * d;
+      selfv += tab->eigs[r] * c * c * tab->selfcont[s];
+    }
+    cn[i] = cnv;
   }
-  if (lane == 0) wsum[wid] = selfv;
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    double s = 0.0;
-    for (int w = 0; w < kWarpsPerBlock; ++w) s += wsum[w];
-    self_part[blockIdx.x] = s;
-  }
+  double v1[1] = {selfv};
+  block_sum_store<1>(v1, self_part + blockIdx.x);
 }
 
 int launch_c6_atoms(int n, const int32_t* species, const Tables* tab, const double* eigvecs, int R,
                     const double* cn, double* c6, double* dc6, double* self_part, int* n_self_blocks,
                     cudaStream_t s) {
-  const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  const int blocks = (n + 255) / 256;
   *n_self_blocks = blocks;
   if (blocks == 0) return FD3_OK;
-  k_c6_atoms<<<blocks, 32 * kWarpsPerBlock, 0, s>>>(n, species, tab, eigvecs, R, const_cast<double*>(cn), c6, dc6,
-                                                     self_part);
+  k_c6_atoms<<<blocks, 256, 0, s>>>(n, species, tab, eigvecs, R, const_cast<double*>(cn), c6, dc6, self_part);
   FD3_LAUNCHED();
   return FD3_OK;
 }

@@ -113,6 +113,38 @@ __device__ __forceinline__ void cn_edge(double r, double rcs, double rc, double&
   }
 }
 
+__device__ __forceinline__ double rsqrt_t(double x) { return rsqrt(x); }
+__device__ __forceinline__ float rsqrt_t(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double exp_t(double x) { return exp(x); }
+__device__ __forceinline__ float exp_t(float x) { return __expf(x); }
+__device__ __forceinline__ double rcp_t(double x) { return 1.0 / x; }
+__device__ __forceinline__ void sincospi_t(double x, double* s, double* c) { sincospi(x, s, c); }
+__device__ __forceinline__ void sincospi_t(float x, float* s, float* c) { sincospif(x, s, c); }
+__device__ __forceinline__ float rcp_t(float x) { return __frcp_rn(x); }
+
+// The same CN edge function from the squared distance r2 > 1e-12 Bohr^2 (the reference zeroes
+// r <= 1e-6): f and a = f'(r) / r with one reciprocal square root and two reciprocals.
+// TC = double for the plain form, float (fast exp) for the mixed form.
+template <typename TC>
+__device__ __forceinline__ void cn_pair(TC r2, TC rcs, TC rc, TC& f, TC& a) {
+  const TC inv_r = rsqrt_t(r2);
+  const TC r = r2 * inv_r;
+  const TC r1 = TC(0.5) * rcs + TC(0.5) * rc;
+  const bool outer = r > r1;
+  const TC coeff = outer ? r : r1;
+  const TC t = rc - coeff;
+  const TC inv_den = rcp_t(t * t + TC(1e-6));
+  const TC dd = coeff - r1;
+  const TC k = TC(16) + dd * dd * inv_den;
+  const TC ratio = TC(4.0 / 3.0) * rcs;
+  const TC q = ratio * inv_r - TC(1);
+  const TC s = rcp_t(TC(1) + exp_t(-(k * q)));
+  f = s;
+  // dk/dr = 2 dd/den + 2 dd^2 t/den^2 on the outer branch, 0 inside
+  const TC dk = outer ? TC(2) * dd * inv_den * (TC(1) + dd * t * inv_den) : TC(0);
+  a = s * (TC(1) - s) * (dk * q - k * ratio * inv_r * inv_r) * inv_r;
+}
+
 // Order-p cardinal B-spline weights at the p stencil nodes for local coordinate x in
 // [-1/2, 1/2]: w[k] = M_p(1/2 - x + k); dw = dw/dx (Cox-de Boor recursion).
 template <int P, typename T>
@@ -184,17 +216,19 @@ __device__ __forceinline__ void green_eval(const GreenPair& g, T k, T s6, T s8, 
   const T sin8 = T(0.38268343236508977173);   // sin(pi/8)
   const T cos8 = T(0.92387953251128675613);   // cos(pi/8)
   const T u = k * R;
-  const T e1 = exp(-u);
-  const T e2 = exp(-u / T(2));
+  // exp(-u) = exp(-u/2)^2; the phases pi/3 + u sqrt3/2, pi/4 + u cos(pi/8), 3pi/4 + u sin(pi/8)
+  // are evaluated in half-turns with sincospi (exact argument reduction).
+  const T e2 = exp_t(-u * T(0.5));
+  const T e1 = e2 * e2;
   T sa, ca;
-  sincos(T(kPi / 3) + u * sq3 / T(2), &sa, &ca);
+  sincospi_t(T(1.0 / 3.0) + u * T(0.27566444771089604), &sa, &ca);   // sqrt(3) / (2 pi)
   const T n6 = e1 - T(2) * e2 * ca;
   const T dn6 = -e1 + e2 * ca + sq3 * e2 * sa;
-  const T e3 = exp(-u * sin8);
-  const T e4 = exp(-u * cos8);
+  const T e3 = exp_t(-u * sin8);
+  const T e4 = exp_t(-u * cos8);
   T s1, c1, s2, c2;
-  sincos(T(kPi / 4) + u * cos8, &s1, &c1);
-  sincos(T(3 * kPi / 4) + u * sin8, &s2, &c2);
+  sincospi_t(T(0.25) + u * T(0.29407998884120140), &s1, &c1);      // cos(pi/8) / pi
+  sincospi_t(T(0.75) + u * T(0.12181191980055409), &s2, &c2);      // sin(pi/8) / pi
   const T n8 = e3 * c1 + e4 * c2;
   const T dn8 = -sin8 * e3 * c1 - cos8 * e3 * s1 - cos8 * e4 * c2 - sin8 * e4 * s2;
   const T invk = T(1) / k;
@@ -204,6 +238,27 @@ __device__ __forceinline__ void green_eval(const GreenPair& g, T k, T s6, T s8, 
   const T d8 = T(3) * s8 * T(g.c8pre) * (R * dn8 * invk - n8 * invk * invk);
   G = f6 + T(g.qq) * f8;
   dG = d6 + T(g.qq) * d8;
+}
+
+// Division of 32-bit unsigned values by a runtime-invariant divisor (round-up multiplier method):
+// q = (t + ((n - t) >> 1)) >> (s - 1), t = umulhi(n, m), for every n < 2^32.
+struct FastDiv {
+  uint32_t d, m, s;
+};
+inline FastDiv make_fastdiv(uint32_t d) {
+  FastDiv f{d, 0u, 0u};
+  if (d > 1) {
+    uint32_t l = 0;
+    while ((1ull << l) < d) ++l;
+    f.m = (uint32_t)((((1ull << 32) * ((1ull << l) - d)) / d) + 1);
+    f.s = l;
+  }
+  return f;
+}
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv& f) {
+  if (f.d == 1) return n;
+  const uint32_t t = __umulhi(n, f.m);
+  return (t + ((n - t) >> 1)) >> (f.s - 1);
 }
 
 // floor division / modulo for possibly negative ints

@@ -60,14 +60,29 @@ int scan_exclusive(const int* in, int n, int* out, cudaStream_t s);   // out[n] 
 int build_cell_list(const CellGrid& g, int n, const double* pos_ang, const int32_t* species, CellList& cl,
                     cudaStream_t s);
 
-// fused CN + C6 factors over the cell list (warp per atom)
+// Per-atom records of the CN pairs (neighbour, f'(r)/r, Bohr vector), written by the CN kernel
+// and streamed by its adjoint; a/d are double (plain form) or float (mixed form).
+struct HitStore {
+  int* j;
+  void* a;
+  void* d;
+  int* n;
+  int* ovf;     // count of bins / atoms that need the global-memory fallback (zeroed per call)
+  int cap;
+  bool is_double;
+};
+constexpr int kHitCap = 160;
+
+// fused CN + C6 factors over the cell list (one CTA per bin)
 int launch_cn_c6_cells(const CellGrid& g, int n, const CellList& cl, const double* pos_ang,
                        const int32_t* species, const Tables* tab, const double* eigvecs, int R, double* cn,
-                       double* c6, double* dc6, double* self_part, int* n_self_blocks, cudaStream_t s);
-// CN adjoint over the cell list: grad += dE/dx (Hartree/Bohr); virial partials (9 per block)
+                       double* c6, double* dc6, double* self_part, int* n_self_blocks, const HitStore& hs,
+                       cudaStream_t s);
+// CN adjoint: grad = out_scale * (grad + dE/dx_CN) (Hartree/Bohr in); virial partials (9 per block)
 int launch_cn_adjoint_cells(const CellGrid& g, int n, const CellList& cl, const double* pos_ang,
                             const int32_t* species, const Tables* tab, const double* gcn, double* grad,
-                            double out_scale, double* vir_part, int* n_blocks, cudaStream_t s);
+                            double out_scale, double* vir_part, int* n_blocks, const HitStore& hs,
+                            cudaStream_t s);
 
 // edge-list CN path
 int launch_cn_edges(int64_t n_edges, const double* pos, const int32_t* species, const int64_t* src,
@@ -99,10 +114,18 @@ struct MeshGeom {
 int launch_cellinfo(const double* cell, double scale, CellInfo* ci, cudaStream_t s);
 int launch_mesh_keys(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
                      const CellInfo* ci, int* keys, cudaStream_t s);
+// Per-atom stencil records in (tile, species)-sorted order, written by the spread launcher and
+// read again by the gather (T = mesh precision).
+struct MeshRecords {
+  int4* b;      // [N] {base_x, base_y, base_z, species}
+  void* w;      // [N][3][P] weights
+  void* dw;     // [N][3][P] d weight / d local coordinate
+  void* c;      // [N][R] rank factors
+};
 template <typename T>
-int launch_spread(const MeshGeom& mg, const double* pos, double pos_scale, const int32_t* species,
-                  const double* c6, const CellInfo* ci, const int* key_start, const int* order, T* rho,
-                  cudaStream_t s);
+int launch_spread(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
+                  const double* c6, const CellInfo* ci, const int* key_start, const int* order,
+                  const MeshRecords& rec, T* rho, cudaStream_t s);
 template <typename T>
 int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab,
                   const float* deconv, int spme, void* spec, void* spec_out, double* part, int* n_blocks,
@@ -111,7 +134,8 @@ int filter_max_blocks();
 template <typename T>
 int launch_gather(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
                   const double* c6, const double* dc6, const CellInfo* ci, const Tables* tab, const int* order,
-                  const T* phi, double* gcn, double* gpos, double* mcell_part, int* n_blocks, cudaStream_t s);
+                  const MeshRecords& rec, const T* phi, double* gcn, double* gpos, double* mcell_part,
+                  int* n_blocks, cudaStream_t s);
 
 // ---- finalisation ---------------------------------------------------------------
 struct Partials {

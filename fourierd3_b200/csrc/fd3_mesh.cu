@@ -91,9 +91,11 @@ struct KPoint {
 __device__ __forceinline__ KPoint kpoint(const MeshDev& g, size_t k, const CellInfo* __restrict__ ci,
                                          const float* __restrict__ deconv, int spme, int P) {
   KPoint q;
-  const int iz = (int)(k % g.nzh);
-  const int iy = (int)((k / g.nzh) % g.n[1]);
-  const int ix = (int)(k / ((size_t)g.nzh * g.n[1]));
+  const uint32_t kq = fdiv((uint32_t)k, g.div_nzh);
+  const int iz = (int)((uint32_t)k - kq * (uint32_t)g.nzh);
+  const uint32_t kqq = fdiv(kq, g.div_ny);
+  const int iy = (int)(kq - kqq * (uint32_t)g.n[1]);
+  const int ix = (int)kqq;
   const int mx = ix <= (g.n[0] - 1) / 2 ? ix : ix - g.n[0];
   const int my = iy <= (g.n[1] - 1) / 2 ? iy : iy - g.n[1];
   const int mz = iz;
@@ -147,8 +149,10 @@ __device__ __forceinline__ void virial_acc(const KPoint& q, double dq, double* a
 }
 
 // Up to 8 species: G, dG and the inverse-FFT matrix in registers; spectrum updated in place.
-// Grid-stride over k-points; one partial (energy + 6 virial components) per block.
-template <typename T, int MAXS>
+// Ranks are processed in chunks of MAXR whose S x MAXR spectrum values are all loaded before any
+// arithmetic. Per-k terms are formed in T and accumulated in float64. Grid-stride over k-points;
+// one partial (energy + 6 virial components) per block.
+template <typename T, int MAXS, int MAXR>
 __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int spme,
                                                            const CellInfo* __restrict__ ci,
                                                            const GreenPair* __restrict__ gp,
@@ -164,6 +168,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < Mh; k += (size_t)gridDim.x * blockDim.x) {
     const KPoint q = kpoint(g, k, ci, deconv, spme, P);
     const T kt = (T)q.knorm;
+    const double inv_sc = 1.0 / q.sc;
     T G[MAXS][MAXS], dG[MAXS][MAXS], Gh[MAXS][MAXS];
 #pragma unroll
     for (int X = 0; X < MAXS; ++X)
@@ -172,8 +177,8 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int
         T gv = T(0), dv = T(0);
         if (X < S && Y < S) {
           green_eval<T>(gp[X * S + Y], kt, s6, s8, gv, dv);
-          gv = (T)((double)gv / q.sc);
-          dv = (T)((double)dv / q.sc);
+          gv = (T)((double)gv * inv_sc);
+          dv = (T)((double)dv * inv_sc);
         }
         G[X][Y] = G[Y][X] = gv;
         dG[X][Y] = dG[Y][X] = dv;
@@ -188,30 +193,38 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int
           if (X < S && Y < S) {
             T gv, dv;
             green_eval<T>(gp[X * S + Y], kpt, s6, s8, gv, dv);
-            Gh[X][Y] = Gh[Y][X] = T(0.5) * (G[X][Y] + (T)((double)gv / q.sc));
+            Gh[X][Y] = Gh[Y][X] = T(0.5) * (G[X][Y] + (T)((double)gv * inv_sc));
           }
     }
     double qq = 0.0, dq = 0.0;
-    for (int r = 0; r < R; ++r) {
-      C2 sv[MAXS];
+    for (int r0 = 0; r0 < R; r0 += MAXR) {
+      C2 sv[MAXR][MAXS];
 #pragma unroll
-      for (int X = 0; X < MAXS; ++X) sv[X] = X < S ? spec[((size_t)X * R + r) * Mh + k] : C2{T(0), T(0)};
-      double qr = 0.0, dqr = 0.0;
+      for (int r = 0; r < MAXR; ++r)
 #pragma unroll
-      for (int X = 0; X < MAXS; ++X) {
-        T hre = T(0), him = T(0);
+        for (int X = 0; X < MAXS; ++X)
+          sv[r][X] = (X < S && r0 + r < R) ? spec[((size_t)X * R + r0 + r) * Mh + k] : C2{T(0), T(0)};
 #pragma unroll
-        for (int Y = 0; Y < MAXS; ++Y) {
-          hre += Gh[X][Y] * sv[Y].x;
-          him += Gh[X][Y] * sv[Y].y;
-          const double re = (double)sv[X].x * (double)sv[Y].x + (double)sv[X].y * (double)sv[Y].y;
-          qr += (double)G[X][Y] * re;
-          dqr += (double)dG[X][Y] * re;
+      for (int r = 0; r < MAXR; ++r) {
+        T qr = T(0), dqr = T(0);
+#pragma unroll
+        for (int X = 0; X < MAXS; ++X) {
+          T hre = T(0), him = T(0);
+#pragma unroll
+          for (int Y = 0; Y < MAXS; ++Y) {
+            hre += Gh[X][Y] * sv[r][Y].x;
+            him += Gh[X][Y] * sv[r][Y].y;
+            const T re = sv[r][X].x * sv[r][Y].x + sv[r][X].y * sv[r][Y].y;
+            qr += G[X][Y] * re;
+            dqr += dG[X][Y] * re;
+          }
+          if (X < S && r0 + r < R) spec[((size_t)X * R + r0 + r) * Mh + k] = C2{hre, him};
         }
-        if (X < S) spec[((size_t)X * R + r) * Mh + k] = C2{hre, him};
+        if (r0 + r < R) {
+          qq += tab->eigs[r0 + r] * (double)qr;
+          dq += tab->eigs[r0 + r] * (double)dqr;
+        }
       }
-      qq += tab->eigs[r] * qr;
-      dq += tab->eigs[r] * dqr;
     }
     acc[0] += q.wk * qq;
     virial_acc(q, dq, acc);
@@ -309,17 +322,24 @@ int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, c
   *n_blocks = blocks;
   const MeshDev g = to_dev(mg);
   C2* sp = reinterpret_cast<C2*>(spec);
+#define FD3_FILTER(SS, RR) \
+  k_filter<T, SS, RR><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gp, tab, deconv, sp, part)
   if (mg.S <= 1)
-    k_filter<T, 1><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gp, tab, deconv, sp, part);
+    FD3_FILTER(1, 4);
+  else if (mg.S <= 2 && mg.R <= 4)
+    FD3_FILTER(2, 4);
   else if (mg.S <= 2)
-    k_filter<T, 2><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gp, tab, deconv, sp, part);
+    FD3_FILTER(2, 2);
+  else if (mg.S <= 4 && mg.R <= 4)
+    FD3_FILTER(4, 4);
   else if (mg.S <= 4)
-    k_filter<T, 4><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gp, tab, deconv, sp, part);
+    FD3_FILTER(4, 2);
   else if (mg.S <= 8)
-    k_filter<T, 8><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gp, tab, deconv, sp, part);
+    FD3_FILTER(8, 1);
   else
     k_filter_any<T><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gp, tab, deconv, sp,
                                                       reinterpret_cast<C2*>(spec_out), part);
+#undef FD3_FILTER
   FD3_LAUNCHED();
   return FD3_OK;
 }

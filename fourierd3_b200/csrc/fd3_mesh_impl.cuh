@@ -19,6 +19,7 @@ namespace fd3 {
 
 struct MeshDev {
   int n[3], nzh, t[3], nt[3], ns[3], S, R;
+  FastDiv div_nzh, div_ny;
 };
 static inline MeshDev to_dev(const MeshGeom& g) {
   MeshDev d;
@@ -31,6 +32,8 @@ static inline MeshDev to_dev(const MeshGeom& g) {
   d.nzh = g.nzh;
   d.S = g.S;
   d.R = g.R;
+  d.div_nzh = make_fastdiv((uint32_t)g.nzh);
+  d.div_ny = make_fastdiv((uint32_t)g.n[1]);
   return d;
 }
 
@@ -69,6 +72,36 @@ __device__ __forceinline__ void stencil_weights(T x, T* w, T* dw) {
     bspline<P, T>(x, w, dw);
 }
 
+// ------------------------------------------------------------------ stencil records
+// One record per atom in (tile, species)-sorted order: first stencil node + species, the p
+// weights and their x-derivatives per axis, and the rank factors in the mesh precision. The
+// spread and the gather read these instead of recomputing the float64 mesh location per use.
+template <typename T, int P, bool LAG>
+__global__ void __launch_bounds__(256) k_mesh_records(MeshDev g, int n, const double* __restrict__ pos, double ps,
+                                                      const int32_t* __restrict__ species,
+                                                      const double* __restrict__ c6, const CellInfo* __restrict__ ci,
+                                                      const int* __restrict__ order, int4* __restrict__ rb,
+                                                      T* __restrict__ rw, T* __restrict__ rdw, T* __restrict__ rc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int atom = order[t];
+  int base[3];
+  T xl[3];
+  mesh_locate<T>(pos, atom, ps, ci, g.n[0], g.n[1], g.n[2], P, base, xl);
+  rb[t] = make_int4(base[0], base[1], base[2], species[atom]);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    T w[P], dw[P];
+    stencil_weights<P, LAG, T>(xl[a], w, dw);
+#pragma unroll
+    for (int k = 0; k < P; ++k) {
+      rw[((size_t)t * 3 + a) * P + k] = w[k];
+      rdw[((size_t)t * 3 + a) * P + k] = dw[k];
+    }
+  }
+  for (int r = 0; r < g.R; ++r) rc[(size_t)t * g.R + r] = (T)c6[(size_t)atom * g.R + r];
+}
+
 // ------------------------------------------------------------------ spread
 // Tile-owned spread. A CTA owns one (16 x 16 x 8)-point tile of one species; thread (lx, ly)
 // owns the z-row of 8 points at (lx, ly). The atoms whose stencil can reach the tile come from
@@ -86,12 +119,10 @@ struct SpChunk {
   static constexpr int value = sizeof(T) == 8 ? 64 : 128;
 };
 
-template <typename T, int P, bool LAG>
-__global__ void __launch_bounds__(kSpThreads, 2) k_spread(MeshDev g, const double* __restrict__ pos, double ps,
-                                                       const double* __restrict__ c6,
-                                                       const CellInfo* __restrict__ ci,
-                                                       const int* __restrict__ key_start,
-                                                       const int* __restrict__ order, T* __restrict__ rho) {
+template <typename T, int P>
+__global__ void __launch_bounds__(kSpThreads, sizeof(T) == 8 ? 2 : 4) k_spread(MeshDev g, const int4* __restrict__ rb,
+                                                       const T* __restrict__ rw, const T* __restrict__ rc,
+                                                       const int* __restrict__ key_start, T* __restrict__ rho) {
   constexpr int CH = SpChunk<T>::value;
   __shared__ T s_wx[CH][kSpTX];
   __shared__ T s_wy[CH][kSpTY];
@@ -140,13 +171,15 @@ __global__ void __launch_bounds__(kSpThreads, 2) k_spread(MeshDev g, const doubl
       // examine one candidate per thread
       const int ca = c0 + tid;
       bool keep = false;
-      int atom = 0, base[3] = {0, 0, 0};
-      T xl[3] = {T(0), T(0), T(0)};
+      int u = 0, base[3] = {0, 0, 0};
       if (ca < total) {
         int seg = 0;
         while (s_pref[seg + 1] <= ca) ++seg;
-        atom = order[s_a0[seg] + (ca - s_pref[seg])];
-        mesh_locate<T>(pos, atom, ps, ci, g.n[0], g.n[1], g.n[2], P, base, xl);
+        u = s_a0[seg] + (ca - s_pref[seg]);      // record slot (sorted order)
+        const int4 b4 = rb[u];
+        base[0] = b4.x;
+        base[1] = b4.y;
+        base[2] = b4.z;
         keep = true;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
@@ -170,9 +203,11 @@ __global__ void __launch_bounds__(kSpThreads, 2) k_spread(MeshDev g, const doubl
       for (int h0 = 0; h0 < tot; h0 += CH) {
         const int slot = off + __popc(bal & ((1u << lane) - 1u)) - h0;
         if (keep && slot >= 0 && slot < CH) {
-          T w[3][P], dw[P];
+          T w[3][P];
 #pragma unroll
-          for (int a = 0; a < 3; ++a) stencil_weights<P, LAG, T>(xl[a], w[a], dw);
+          for (int a = 0; a < 3; ++a)
+#pragma unroll
+            for (int k = 0; k < P; ++k) w[a][k] = rw[((size_t)u * 3 + a) * P + k];
 #pragma unroll
           for (int z = 0; z < kSpTX; ++z) s_wx[slot][z] = T(0);
 #pragma unroll
@@ -189,7 +224,7 @@ __global__ void __launch_bounds__(kSpThreads, 2) k_spread(MeshDev g, const doubl
             if (iz < g.t[2]) s_wz[slot][iz] += w[2][k];
           }
 #pragma unroll
-          for (int r = 0; r < kSpRC; ++r) s_c[slot][r] = r0 + r < R ? (T)c6[(size_t)atom * R + r0 + r] : T(0);
+          for (int r = 0; r < kSpRC; ++r) s_c[slot][r] = r0 + r < R ? rc[(size_t)u * R + r0 + r] : T(0);
         }
         __syncthreads();
         const int nc = min(CH, tot - h0);
@@ -240,26 +275,34 @@ __global__ void __launch_bounds__(kSpThreads, 2) k_spread(MeshDev g, const doubl
 }
 
 template <typename T, int P, bool LAG>
-static int spread_r(const MeshGeom& mg, dim3 grid, const double* pos, double ps, const double* c6,
-                    const CellInfo* ci, const int* ks, const int* order, T* rho, cudaStream_t s) {
-  k_spread<T, P, LAG><<<grid, kSpThreads, 0, s>>>(to_dev(mg), pos, ps, c6, ci, ks, order, rho);
+static int spread_r(const MeshGeom& mg, dim3 grid, int n, const double* pos, double ps, const int32_t* species,
+                    const double* c6, const CellInfo* ci, const int* ks, const int* order, const MeshRecords& rec,
+                    T* rho, cudaStream_t s) {
+  const MeshDev g = to_dev(mg);
+  if (n > 0) {
+    k_mesh_records<T, P, LAG><<<(n + 255) / 256, 256, 0, s>>>(g, n, pos, ps, species, c6, ci, order, rec.b, (T*)rec.w,
+                                                              (T*)rec.dw, (T*)rec.c);
+    FD3_LAUNCHED();
+  }
+  k_spread<T, P><<<grid, kSpThreads, 0, s>>>(g, rec.b, (const T*)rec.w, (const T*)rec.c, ks, rho);
   FD3_LAUNCHED();
   return FD3_OK;
 }
 
 template <typename T>
-int launch_spread(const MeshGeom& mg, const double* pos, double pos_scale, const int32_t* species,
-                  const double* c6, const CellInfo* ci, const int* key_start, const int* order, T* rho,
-                  cudaStream_t s) {
-  (void)species;
+int launch_spread(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
+                  const double* c6, const CellInfo* ci, const int* key_start, const int* order,
+                  const MeshRecords& rec, T* rho, cudaStream_t s) {
   if (mg.R > FD3_MAX_RANK || mg.order < 1 || mg.order > FD3_MAX_ORDER) return FD3_EINVAL;
   if (mg.t[0] > kSpTX || mg.t[1] > kSpTY || mg.t[2] > kSpTZ || mg.ns[0] * mg.ns[1] * mg.ns[2] > 125)
     return FD3_EINVAL;
   const dim3 grid(mg.nt[0] * mg.nt[1] * mg.nt[2], mg.S);
-#define FD3_SPREAD_CASE(PP)                                                                          \
-  case PP:                                                                                           \
-    return mg.lagrange ? spread_r<T, PP, true>(mg, grid, pos, pos_scale, c6, ci, key_start, order, rho, s) \
-                       : spread_r<T, PP, false>(mg, grid, pos, pos_scale, c6, ci, key_start, order, rho, s);
+#define FD3_SPREAD_CASE(PP)                                                                                  \
+  case PP:                                                                                                   \
+    return mg.lagrange ? spread_r<T, PP, true>(mg, grid, n, pos, pos_scale, species, c6, ci, key_start, order, rec, \
+                                               rho, s)                                                       \
+                       : spread_r<T, PP, false>(mg, grid, n, pos, pos_scale, species, c6, ci, key_start, order, rec, \
+                                                rho, s);
   switch (mg.order) {
     FD3_SPREAD_CASE(1)
     FD3_SPREAD_CASE(2)
@@ -285,6 +328,8 @@ __global__ void __launch_bounds__(32 * kGatherWarps) k_gather(MeshDev g, int n, 
                                                               const CellInfo* __restrict__ ci,
                                                               const Tables* __restrict__ tab,
                                                               const int* __restrict__ order,
+                                                              const int4* __restrict__ rb, const T* __restrict__ rw,
+                                                              const T* __restrict__ rdw,
                                                               const T* __restrict__ phi, double* __restrict__ gcn,
                                                               double* __restrict__ gpos,
                                                               double* __restrict__ mcell_part) {
@@ -294,13 +339,15 @@ __global__ void __launch_bounds__(32 * kGatherWarps) k_gather(MeshDev g, int n, 
   double mc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (t < n) {
     const int i = order[t];
-    const int s = species[i];
-    int base[3];
-    T xl[3];
-    mesh_locate<T>(pos, i, ps, ci, g.n[0], g.n[1], g.n[2], P, base, xl);
-    T w[3][P], dw[3][P];
+    const int4 b4 = rb[t];
+    const int s = b4.w;
+    const int base[3] = {b4.x, b4.y, b4.z};
+    T w0[P], dw0[P];
 #pragma unroll
-    for (int a = 0; a < 3; ++a) stencil_weights<P, LAG, T>(xl[a], w[a], dw[a]);
+    for (int k = 0; k < P; ++k) {
+      w0[k] = rw[((size_t)t * 3) * P + k];
+      dw0[k] = rdw[((size_t)t * 3) * P + k];
+    }
     double cl[MAXR];
 #pragma unroll
     for (int r = 0; r < MAXR; ++r) cl[r] = r < R ? c6[(size_t)i * R + r] * tab->eigs[r] : 0.0;
@@ -319,12 +366,8 @@ __global__ void __launch_bounds__(32 * kGatherWarps) k_gather(MeshDev g, int n, 
     }
     for (int q = lane; q < P * P; q += 32) {
       const int ky = q / P, kz = q - ky * P;
-      T wy = T(0), dwy = T(0), wz = T(0), dwz = T(0);
-#pragma unroll
-      for (int k = 0; k < P; ++k) {
-        if (k == ky) { wy = w[1][k]; dwy = dw[1][k]; }
-        if (k == kz) { wz = w[2][k]; dwz = dw[2][k]; }
-      }
+      const T wy = rw[((size_t)t * 3 + 1) * P + ky], dwy = rdw[((size_t)t * 3 + 1) * P + ky];
+      const T wz = rw[((size_t)t * 3 + 2) * P + kz], dwz = rdw[((size_t)t * 3 + 2) * P + kz];
       int iy = base[1] + ky;
       while (iy >= g.n[1]) iy -= g.n[1];
       int iz = base[2] + kz;
@@ -333,10 +376,10 @@ __global__ void __launch_bounds__(32 * kGatherWarps) k_gather(MeshDev g, int n, 
 #pragma unroll
       for (int kx = 0; kx < P; ++kx) {
         const size_t m = ((size_t)ixs[kx] * g.n[1] + iy) * g.n[2] + iz;
-        const T W = w[0][kx] * wyz;
-        const T Wx = dw[0][kx] * wyz;
-        const T Wy = w[0][kx] * dyz;
-        const T Wz = w[0][kx] * ydz;
+        const T W = w0[kx] * wyz;
+        const T Wx = dw0[kx] * wyz;
+        const T Wy = w0[kx] * dyz;
+        const T Wz = w0[kx] * ydz;
         double cp = 0.0;
 #pragma unroll
         for (int r = 0; r < MAXR; ++r) {
@@ -399,21 +442,24 @@ __global__ void __launch_bounds__(32 * kGatherWarps) k_gather(MeshDev g, int n, 
 template <typename T, int P, bool LAG>
 static int gather_r(const MeshGeom& mg, int blocks, int n, const double* pos, double ps, const int32_t* species,
                     const double* c6, const double* dc6, const CellInfo* ci, const Tables* tab, const int* order,
-                    const T* phi, double* gcn, double* gpos, double* mcell, cudaStream_t s) {
+                    const MeshRecords& rec, const T* phi, double* gcn, double* gpos, double* mcell, cudaStream_t s) {
   const MeshDev g = to_dev(mg);
   const int tb = 32 * kGatherWarps;
+  const int4* rb = rec.b;
+  const T* rw = (const T*)rec.w;
+  const T* rdw = (const T*)rec.dw;
   if (mg.R <= 4)
-    k_gather<T, P, LAG, 4><<<blocks, tb, 0, s>>>(g, n, pos, ps, species, c6, dc6, ci, tab, order, phi, gcn, gpos,
-                                                  mcell);
+    k_gather<T, P, LAG, 4><<<blocks, tb, 0, s>>>(g, n, pos, ps, species, c6, dc6, ci, tab, order, rb, rw, rdw, phi,
+                                                  gcn, gpos, mcell);
   else if (mg.R <= 8)
-    k_gather<T, P, LAG, 8><<<blocks, tb, 0, s>>>(g, n, pos, ps, species, c6, dc6, ci, tab, order, phi, gcn, gpos,
-                                                  mcell);
+    k_gather<T, P, LAG, 8><<<blocks, tb, 0, s>>>(g, n, pos, ps, species, c6, dc6, ci, tab, order, rb, rw, rdw, phi,
+                                                  gcn, gpos, mcell);
   else if (mg.R <= 16)
-    k_gather<T, P, LAG, 16><<<blocks, tb, 0, s>>>(g, n, pos, ps, species, c6, dc6, ci, tab, order, phi, gcn, gpos,
-                                                   mcell);
+    k_gather<T, P, LAG, 16><<<blocks, tb, 0, s>>>(g, n, pos, ps, species, c6, dc6, ci, tab, order, rb, rw, rdw, phi,
+                                                   gcn, gpos, mcell);
   else
-    k_gather<T, P, LAG, 32><<<blocks, tb, 0, s>>>(g, n, pos, ps, species, c6, dc6, ci, tab, order, phi, gcn, gpos,
-                                                   mcell);
+    k_gather<T, P, LAG, 32><<<blocks, tb, 0, s>>>(g, n, pos, ps, species, c6, dc6, ci, tab, order, rb, rw, rdw, phi,
+                                                   gcn, gpos, mcell);
   FD3_LAUNCHED();
   return FD3_OK;
 }
@@ -421,16 +467,17 @@ static int gather_r(const MeshGeom& mg, int blocks, int n, const double* pos, do
 template <typename T>
 int launch_gather(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
                   const double* c6, const double* dc6, const CellInfo* ci, const Tables* tab, const int* order,
-                  const T* phi, double* gcn, double* gpos, double* mcell_part, int* n_blocks, cudaStream_t s) {
+                  const MeshRecords& rec, const T* phi, double* gcn, double* gpos, double* mcell_part,
+                  int* n_blocks, cudaStream_t s) {
   const int blocks = (n + kGatherWarps - 1) / kGatherWarps;
   *n_blocks = blocks;
   if (blocks == 0) return FD3_OK;
 #define FD3_GATHER_CASE(PP)                                                                                   \
   case PP:                                                                                                    \
     return mg.lagrange ? gather_r<T, PP, true>(mg, blocks, n, pos, pos_scale, species, c6, dc6, ci, tab, order, \
-                                               phi, gcn, gpos, mcell_part, s)                                 \
+                                               rec, phi, gcn, gpos, mcell_part, s)                            \
                        : gather_r<T, PP, false>(mg, blocks, n, pos, pos_scale, species, c6, dc6, ci, tab, order, \
-                                                phi, gcn, gpos, mcell_part, s);
+                                                rec, phi, gcn, gpos, mcell_part, s);
   switch (mg.order) {
     FD3_GATHER_CASE(1)
     FD3_GATHER_CASE(2)
@@ -444,4 +491,5 @@ int launch_gather(const MeshGeom& mg, int n, const double* pos, double pos_scale
 #undef FD3_GATHER_CASE
   return FD3_EINVAL;
 }
+
 }  // namespace fd3

@@ -2,6 +2,6 @@
 #include "fd3_mesh_impl.cuh"
 
 namespace fd3 {
-template int launch_spread<float>(const MeshGeom&, const double*, double, const int32_t*, const double*,
-                                  const CellInfo*, const int*, const int*, float*, cudaStream_t);
+template int launch_spread<float>(const MeshGeom&, int, const double*, double, const int32_t*, const double*,
+                                  const CellInfo*, const int*, const int*, const MeshRecords&, float*, cudaStream_t);
 }  // namespace fd3

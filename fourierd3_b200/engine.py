@@ -185,7 +185,7 @@ class Engine:
         gpos = torch.empty_like(pos) if need_grad else None
         gsh = torch.empty_like(sh) if need_grad else None
         gcell = torch.empty((3, 3), dtype=torch.float64, device=self.device) if need_grad else None
-        work = self.workspace(n, 1)
+        work = self.workspace(n, 0)
 
         def ptr(t):
             return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else None

@@ -271,7 +271,10 @@ void carve(const fd3_plan* p, int64_t N, int64_t K_in, Carver& c, Work& w) {
   w.gcn = c.take<double>(N);
   w.self_part = c.take<double>(nblk);
   w.cnv_part = c.take<double>(9 * nblk);
-  w.mcell_part = c.take<double>(9 * nblk);
+  // mesh-cell partials: one per gather CTA (atom warps or (tile, species) CTAs)
+  int64_t ngt = 1;
+  if (p->method != FD3_METHOD_EWALD) ngt = (int64_t)p->mg.nt[0] * p->mg.nt[1] * p->mg.nt[2] * p->S;
+  w.mcell_part = c.take<double>(9 * ((nblk > ngt ? nblk : ngt) + 1));
   const bool mesh = p->method != FD3_METHOD_EWALD;
   size_t Mh = 0, M = 0;
   int64_t Kmesh = 1;
@@ -380,8 +383,8 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
   else
     FD3_CUFFT(cufftExecC2R(p->inv, (cufftComplex*)hspec, (cufftReal*)w.rho));
   prof_mark(p, s, "fft_c2r");
-  FD3_TRY(launch_gather<T>(mg, N, pos, ps, species, w.c6, w.dc6, w.ci, p->d_tab, w.morder, w.rec, (const T*)w.rho,
-                           w.gcn, gpos, mcell, n_mcell, s));
+  FD3_TRY(launch_gather<T>(mg, N, pos, ps, species, w.c6, w.dc6, w.ci, p->d_tab, w.morder, w.mstart, w.rec,
+                           (const T*)w.rho, w.gcn, gpos, mcell, n_mcell, s));
   prof_mark(p, s, "gather");
   return FD3_OK;
 }

@@ -3,6 +3,6 @@
 
 namespace fd3 {
 template int launch_gather<float>(const MeshGeom&, int, const double*, double, const int32_t*, const double*,
-                                  const double*, const CellInfo*, const Tables*, const int*, const MeshRecords&,
-                                  const float*, double*, double*, double*, int*, cudaStream_t);
+                                  const double*, const CellInfo*, const Tables*, const int*, const int*,
+                                  const MeshRecords&, const float*, double*, double*, double*, int*, cudaStream_t);
 }  // namespace fd3

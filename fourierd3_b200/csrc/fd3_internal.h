@@ -134,8 +134,8 @@ int filter_max_blocks();
 template <typename T>
 int launch_gather(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
                   const double* c6, const double* dc6, const CellInfo* ci, const Tables* tab, const int* order,
-                  const MeshRecords& rec, const T* phi, double* gcn, double* gpos, double* mcell_part,
-                  int* n_blocks, cudaStream_t s);
+                  const int* key_start, const MeshRecords& rec, const T* phi, double* gcn, double* gpos,
+                  double* mcell_part, int* n_blocks, cudaStream_t s);
 
 // ---- finalisation ---------------------------------------------------------------
 struct Partials {

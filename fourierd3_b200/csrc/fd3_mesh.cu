@@ -83,14 +83,20 @@ __device__ __forceinline__ double sinc_pi(double x) { return x == 0.0 ? 1.0 : si
 // Geometry of rfft k-point k: k-vector (torch fftfreq order on x, y; rfftfreq on z), |k|, the
 // SPME window, the Hermitian weight (1 on the first and last z-plane, pair_pot.py:213-218) and,
 // on the self-conjugate planes, the |k| of the stored conjugate partner when it differs.
+// Per-k geometry in precision T (double for the plain form, float for the mixed form):
+// k-vector, |k|, the SPME window, the Hermitian weight (1 on the first and last z-plane,
+// pair_pot.py:213-218) and, on the self-conjugate planes, the |k| of the stored conjugate
+// partner when it differs. The reciprocal rows are hoisted into registers by the caller.
+template <typename T>
 struct KPoint {
-  double kv[3], knorm, sc, wk, kpart;
+  T kv[3], knorm, inv_sc, wk, kpart;
   bool partner;
 };
 
-__device__ __forceinline__ KPoint kpoint(const MeshDev& g, size_t k, const CellInfo* __restrict__ ci,
-                                         const float* __restrict__ deconv, int spme, int P) {
-  KPoint q;
+template <typename T>
+__device__ __forceinline__ KPoint<T> kpoint(const MeshDev& g, size_t k, const T (&rc)[9],
+                                            const float* __restrict__ deconv, int spme, int P) {
+  KPoint<T> q;
   const uint32_t kq = fdiv((uint32_t)k, g.div_nzh);
   const int iz = (int)((uint32_t)k - kq * (uint32_t)g.nzh);
   const uint32_t kqq = fdiv(kq, g.div_ny);
@@ -100,20 +106,21 @@ __device__ __forceinline__ KPoint kpoint(const MeshDev& g, size_t k, const CellI
   const int my = iy <= (g.n[1] - 1) / 2 ? iy : iy - g.n[1];
   const int mz = iz;
 #pragma unroll
-  for (int c = 0; c < 3; ++c) q.kv[c] = mx * ci->recip[c] + my * ci->recip[3 + c] + mz * ci->recip[6 + c];
+  for (int c = 0; c < 3; ++c) q.kv[c] = T(mx) * rc[c] + T(my) * rc[3 + c] + T(mz) * rc[6 + c];
   q.knorm = sqrt(q.kv[0] * q.kv[0] + q.kv[1] * q.kv[1] + q.kv[2] * q.kv[2]);
-  q.sc = 1.0;
+  double sc = 1.0;
   if (spme) {
     if (deconv) {
-      q.sc = (double)deconv[k];
+      sc = (double)deconv[k];
     } else {
       const double nzf = (double)(2 * (g.nzh - 1));
       double v = sinc_pi(mx / (double)g.n[0]) * sinc_pi(my / (double)g.n[1]) * sinc_pi(mz / nzf);
       v = pow(v, 2.0 * P);
-      q.sc = v < 1e-10 ? 1e-10 : v;
+      sc = v < 1e-10 ? 1e-10 : v;
     }
   }
-  q.wk = (iz == 0 || iz == g.nzh - 1) ? 1.0 : 2.0;
+  q.inv_sc = (T)(1.0 / sc);
+  q.wk = (iz == 0 || iz == g.nzh - 1) ? T(1) : T(2);
   // Self-conjugate planes (kz = 0 and the z-Nyquist plane): the entry at (ix, iy) and its conjugate
   // partner (-ix, -iy) are both stored, but at the Nyquist rows their k-vectors differ in a
   // triclinic cell, so G(k) != G(k'). The inverse FFT needs a Hermitian input; using
@@ -126,9 +133,9 @@ __device__ __forceinline__ KPoint kpoint(const MeshDev& g, size_t k, const CellI
     const int qx = px <= (g.n[0] - 1) / 2 ? px : px - g.n[0];
     const int qy = py <= (g.n[1] - 1) / 2 ? py : py - g.n[1];
     if (qx != -mx || qy != -my || mz != 0) {
-      double kp[3];
+      T kp[3];
 #pragma unroll
-      for (int c = 0; c < 3; ++c) kp[c] = qx * ci->recip[c] + qy * ci->recip[3 + c] + mz * ci->recip[6 + c];
+      for (int c = 0; c < 3; ++c) kp[c] = T(qx) * rc[c] + T(qy) * rc[3 + c] + T(mz) * rc[6 + c];
       q.kpart = sqrt(kp[0] * kp[0] + kp[1] * kp[1] + kp[2] * kp[2]);
       q.partner = q.kpart != q.knorm;
     }
@@ -136,15 +143,23 @@ __device__ __forceinline__ KPoint kpoint(const MeshDev& g, size_t k, const CellI
   return q;
 }
 
-__device__ __forceinline__ void virial_acc(const KPoint& q, double dq, double* acc) {
-  if (q.knorm > 0.0) {
-    const double f = q.wk * dq / q.knorm;
-    acc[1] += f * q.kv[0] * q.kv[0];
-    acc[2] += f * q.kv[1] * q.kv[1];
-    acc[3] += f * q.kv[2] * q.kv[2];
-    acc[4] += f * q.kv[0] * q.kv[1];
-    acc[5] += f * q.kv[0] * q.kv[2];
-    acc[6] += f * q.kv[1] * q.kv[2];
+template <typename T>
+__device__ __forceinline__ void load_recip(const CellInfo* __restrict__ ci, T (&rc)[9]) {
+#pragma unroll
+  for (int c = 0; c < 9; ++c) rc[c] = (T)ci->recip[c];
+}
+
+// Per-k virial term f k_a k_b / |k| (f = w_k dq), added to the float64 block accumulators.
+template <typename T>
+__device__ __forceinline__ void virial_acc(const KPoint<T>& q, T dq, double* acc) {
+  if (q.knorm > T(0)) {
+    const T f = q.wk * dq / q.knorm;
+    acc[1] += (double)(f * q.kv[0] * q.kv[0]);
+    acc[2] += (double)(f * q.kv[1] * q.kv[1]);
+    acc[3] += (double)(f * q.kv[2] * q.kv[2]);
+    acc[4] += (double)(f * q.kv[0] * q.kv[1]);
+    acc[5] += (double)(f * q.kv[0] * q.kv[2]);
+    acc[6] += (double)(f * q.kv[1] * q.kv[2]);
   }
 }
 
@@ -165,10 +180,10 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int
   const size_t Mh = (size_t)g.n[0] * g.n[1] * g.nzh;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   const T s6 = (T)tab->s6, s8 = (T)tab->s8;
+  T rc[9];
+  load_recip<T>(ci, rc);
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < Mh; k += (size_t)gridDim.x * blockDim.x) {
-    const KPoint q = kpoint(g, k, ci, deconv, spme, P);
-    const T kt = (T)q.knorm;
-    const double inv_sc = 1.0 / q.sc;
+    const KPoint<T> q = kpoint<T>(g, k, rc, deconv, spme, P);
     T G[MAXS][MAXS], dG[MAXS][MAXS], Gh[MAXS][MAXS];
 #pragma unroll
     for (int X = 0; X < MAXS; ++X)
@@ -176,27 +191,26 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int
       for (int Y = X; Y < MAXS; ++Y) {
         T gv = T(0), dv = T(0);
         if (X < S && Y < S) {
-          green_eval<T>(gp[X * S + Y], kt, s6, s8, gv, dv);
-          gv = (T)((double)gv * inv_sc);
-          dv = (T)((double)dv * inv_sc);
+          green_eval<T>(gp[X * S + Y], q.knorm, s6, s8, gv, dv);
+          gv *= q.inv_sc;
+          dv *= q.inv_sc;
         }
         G[X][Y] = G[Y][X] = gv;
         dG[X][Y] = dG[Y][X] = dv;
         Gh[X][Y] = Gh[Y][X] = gv;
       }
     if (q.partner) {
-      const T kpt = (T)q.kpart;
 #pragma unroll
       for (int X = 0; X < MAXS; ++X)
 #pragma unroll
         for (int Y = X; Y < MAXS; ++Y)
           if (X < S && Y < S) {
             T gv, dv;
-            green_eval<T>(gp[X * S + Y], kpt, s6, s8, gv, dv);
-            Gh[X][Y] = Gh[Y][X] = T(0.5) * (G[X][Y] + (T)((double)gv * inv_sc));
+            green_eval<T>(gp[X * S + Y], q.kpart, s6, s8, gv, dv);
+            Gh[X][Y] = Gh[Y][X] = T(0.5) * (G[X][Y] + gv * q.inv_sc);
           }
     }
-    double qq = 0.0, dq = 0.0;
+    T qq = T(0), dq = T(0);
     for (int r0 = 0; r0 < R; r0 += MAXR) {
       C2 sv[MAXR][MAXS];
 #pragma unroll
@@ -221,13 +235,14 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int
           if (X < S && r0 + r < R) spec[((size_t)X * R + r0 + r) * Mh + k] = C2{hre, him};
         }
         if (r0 + r < R) {
-          qq += tab->eigs[r0 + r] * (double)qr;
-          dq += tab->eigs[r0 + r] * (double)dqr;
+          const T lam = (T)tab->eigs[r0 + r];
+          qq += lam * qr;
+          dq += lam * dqr;
         }
       }
     }
-    acc[0] += q.wk * qq;
-    virial_acc(q, dq, acc);
+    acc[0] += (double)(q.wk * qq);
+    virial_acc<T>(q, dq, acc);
   }
   block_sum_store<7>(acc, part + 7 * blockIdx.x);
 }
@@ -249,10 +264,12 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_any(MeshDev g, int P,
   const size_t Mh = (size_t)g.n[0] * g.n[1] * g.nzh;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   const T s6 = (T)tab->s6, s8 = (T)tab->s8;
+  T rc[9];
+  load_recip<T>(ci, rc);
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < Mh; k += (size_t)gridDim.x * blockDim.x) {
-    const KPoint q = kpoint(g, k, ci, deconv, spme, P);
-    const T kt = (T)q.knorm, kpt = (T)q.kpart;
-    double qq = 0.0, dq = 0.0;
+    const KPoint<T> q = kpoint<T>(g, k, rc, deconv, spme, P);
+    const T kt = q.knorm, kpt = q.kpart;
+    T qq = T(0), dq = T(0);
     for (int r0 = 0; r0 < R; r0 += kAnyRC) {
       for (int X = 0; X < S; ++X) {
         C2 hq[kAnyRC], hd[kAnyRC], hh[kAnyRC];
@@ -261,13 +278,13 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_any(MeshDev g, int P,
         for (int Y = 0; Y < S; ++Y) {
           T gv, dv;
           green_eval<T>(gp[X * S + Y], kt, s6, s8, gv, dv);
-          gv = (T)((double)gv / q.sc);
-          dv = (T)((double)dv / q.sc);
+          gv *= q.inv_sc;
+          dv *= q.inv_sc;
           T gh = gv;
           if (q.partner) {
             T gpv, dpv;
             green_eval<T>(gp[X * S + Y], kpt, s6, s8, gpv, dpv);
-            gh = T(0.5) * (gv + (T)((double)gpv / q.sc));
+            gh = T(0.5) * (gv + gpv * q.inv_sc);
           }
 #pragma unroll
           for (int r = 0; r < kAnyRC; ++r) {
@@ -284,16 +301,16 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_any(MeshDev g, int P,
           if (r0 + r < R) {
             const size_t idx = ((size_t)X * R + r0 + r) * Mh + k;
             const C2 sx = spec[idx];
-            const double lam = tab->eigs[r0 + r];
-            qq += lam * ((double)sx.x * (double)hq[r].x + (double)sx.y * (double)hq[r].y);
-            dq += lam * ((double)sx.x * (double)hd[r].x + (double)sx.y * (double)hd[r].y);
+            const T lam = (T)tab->eigs[r0 + r];
+            qq += lam * (sx.x * hq[r].x + sx.y * hq[r].y);
+            dq += lam * (sx.x * hd[r].x + sx.y * hd[r].y);
             spec_out[idx] = hh[r];
           }
         }
       }
     }
-    acc[0] += q.wk * qq;
-    virial_acc(q, dq, acc);
+    acc[0] += (double)(q.wk * qq);
+    virial_acc<T>(q, dq, acc);
   }
   block_sum_store<7>(acc, part + 7 * blockIdx.x);
 }

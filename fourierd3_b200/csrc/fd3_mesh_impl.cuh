@@ -442,8 +442,11 @@ __global__ void __launch_bounds__(32 * kGatherWarps) k_gather(MeshDev g, int n, 
 template <typename T, int P, bool LAG>
 static int gather_r(const MeshGeom& mg, int blocks, int n, const double* pos, double ps, const int32_t* species,
                     const double* c6, const double* dc6, const CellInfo* ci, const Tables* tab, const int* order,
-                    const MeshRecords& rec, const T* phi, double* gcn, double* gpos, double* mcell, cudaStream_t s) {
+                    const int* key_start, const MeshRecords& rec, const T* phi, double* gcn, double* gpos,
+                    double* mcell, int* n_mcell, cudaStream_t s) {
   const MeshDev g = to_dev(mg);
+  (void)key_start;
+  *n_mcell = mcell ? blocks : 0;
   const int tb = 32 * kGatherWarps;
   const int4* rb = rec.b;
   const T* rw = (const T*)rec.w;
@@ -467,17 +470,17 @@ static int gather_r(const MeshGeom& mg, int blocks, int n, const double* pos, do
 template <typename T>
 int launch_gather(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
                   const double* c6, const double* dc6, const CellInfo* ci, const Tables* tab, const int* order,
-                  const MeshRecords& rec, const T* phi, double* gcn, double* gpos, double* mcell_part,
-                  int* n_blocks, cudaStream_t s) {
+                  const int* key_start, const MeshRecords& rec, const T* phi, double* gcn, double* gpos,
+                  double* mcell_part, int* n_blocks, cudaStream_t s) {
   const int blocks = (n + kGatherWarps - 1) / kGatherWarps;
-  *n_blocks = blocks;
+  *n_blocks = 0;
   if (blocks == 0) return FD3_OK;
 #define FD3_GATHER_CASE(PP)                                                                                   \
   case PP:                                                                                                    \
     return mg.lagrange ? gather_r<T, PP, true>(mg, blocks, n, pos, pos_scale, species, c6, dc6, ci, tab, order, \
-                                               rec, phi, gcn, gpos, mcell_part, s)                            \
+                                               key_start, rec, phi, gcn, gpos, mcell_part, n_blocks, s)       \
                        : gather_r<T, PP, false>(mg, blocks, n, pos, pos_scale, species, c6, dc6, ci, tab, order, \
-                                                rec, phi, gcn, gpos, mcell_part, s);
+                                                key_start, rec, phi, gcn, gpos, mcell_part, n_blocks, s);
   switch (mg.order) {
     FD3_GATHER_CASE(1)
     FD3_GATHER_CASE(2)

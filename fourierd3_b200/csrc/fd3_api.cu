@@ -97,6 +97,17 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
     for (int a = 0; a < 3; ++a)
       if (d->mesh[a] < 1) return FD3_EINVAL;
   }
+  if (!mesh) {
+    for (int a = 0; a < 3; ++a)
+      if (d->ewald_ns[a] < 1) {
+        set_error("fd3_plan_create", "ewald_ns must be >= 1 on every axis");
+        return FD3_EINVAL;
+      }
+    if ((int64_t)d->ewald_ns[0] * d->ewald_ns[1] * d->ewald_ns[2] > (int64_t)1 << 28) {
+      set_error("fd3_plan_create", "ewald k-vector box too large");
+      return FD3_EINVAL;
+    }
+  }
   fd3_plan* p = new (std::nothrow) fd3_plan();
   if (!p) return FD3_EINVAL;
   p->S = S;
@@ -253,6 +264,7 @@ struct Work {
   MeshRecords rec;
   CellList cl;
   HitStore hits;
+  EwaldWork ew;
   void *rho, *spec, *spec2, *fftw;
 };
 
@@ -315,6 +327,21 @@ void carve(const fd3_plan* p, int64_t N, int64_t K_in, Carver& c, Work& w) {
   // more than 8 species: the filter writes H out of place
   w.spec2 = c.take<char>(mesh && p->S > 8 ? C * Mh * 2 * es : 1);
   w.fftw = c.take<char>(p->fft_ws);
+  // direct Ewald sum
+  if (!mesh) {
+    const int64_t nk = (int64_t)p->ens[0] * p->ens[1] * p->ens[2];
+    const int64_t nchunk = ewald_chunks((int)nk);
+    w.ew.keys = c.take<int>(N);
+    w.ew.counts = c.take<int>(p->S);
+    w.ew.sp_start = c.take<int>(p->S + 1);
+    w.ew.order = c.take<int>(N);
+    w.ew.sp_of = c.take<int4>(N);
+    w.ew.frac = c.take<double>(3 * N);
+    w.ew.spec = c.take<char>((size_t)C * nk * 2 * es);
+    w.ew.hspec = c.take<char>((size_t)C * nk * 2 * es);
+    w.ew.kpart = w.kspc_part;
+    w.ew.gpart = c.take<double>((size_t)N * nchunk * (p->R + 3));
+  }
 }
 }  // namespace
 
@@ -391,6 +418,18 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
 
 static int run_mesh(fd3_plan* p, int N, const double* pos, double ps, const int32_t* species, Work& w,
                     bool need_grad, double* gpos, double* mcell, int* n_kspc, int* n_mcell, cudaStream_t s) {
+  if (p->method == FD3_METHOD_EWALD) {
+    EwaldGeom eg{{p->ens[0], p->ens[1], p->ens[2]}, p->S, p->R};
+    int rc;
+    if (p->precision == FD3_PREC_FP64)
+      rc = launch_ewald<double>(eg, N, pos, ps, species, w.c6, w.dc6, w.ci, p->d_green, p->d_tab, w.ew, need_grad,
+                                w.gcn, gpos, mcell, n_kspc, n_mcell, s);
+    else
+      rc = launch_ewald<float>(eg, N, pos, ps, species, w.c6, w.dc6, w.ci, p->d_green, p->d_tab, w.ew, need_grad,
+                               w.gcn, gpos, mcell, n_kspc, n_mcell, s);
+    prof_mark(p, s, "ewald");
+    return rc;
+  }
   if (p->precision == FD3_PREC_FP64)
     return mesh_pipeline<double>(p, N, pos, ps, species, w, need_grad, gpos, mcell, n_kspc, n_mcell, s);
   return mesh_pipeline<float>(p, N, pos, ps, species, w, need_grad, gpos, mcell, n_kspc, n_mcell, s);
@@ -405,10 +444,6 @@ extern "C" int fd3_energy_edges(fd3_plan* p, int64_t n_atoms, const double* d_po
     return FD3_EINVAL;
   if (n_edges < 0 || (n_edges > 0 && (!d_src || !d_dst || !d_shift))) return FD3_EINVAL;
   if (need_grad && (!d_gpos || !d_gcell || (n_edges > 0 && !d_gshift))) return FD3_EINVAL;
-  if (p->method == FD3_METHOD_EWALD) {
-    set_error("fd3_energy_edges", "method ewald is served by fd3_ewald_* entry points");
-    return FD3_EINVAL;
-  }
   cudaStream_t s = (cudaStream_t)stream;
   const int N = (int)n_atoms;
   Work w;
@@ -440,10 +475,6 @@ extern "C" int fd3_energy_forces_stress(fd3_plan* p, int64_t n_atoms, const doub
   if (!p || n_atoms < 1 || n_atoms > (int64_t)1 << 30 || !d_pos_ang || !d_species || !h_cell_ang || !d_cell_ang ||
       !d_energy || !d_forces || !d_stress)
     return FD3_EINVAL;
-  if (p->method == FD3_METHOD_EWALD) {
-    set_error("fd3_energy_forces_stress", "method ewald is served by fd3_ewald_* entry points");
-    return FD3_EINVAL;
-  }
   cudaStream_t s = (cudaStream_t)stream;
   const int N = (int)n_atoms;
   CellGrid g;

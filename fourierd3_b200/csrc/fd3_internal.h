@@ -137,6 +137,30 @@ int launch_gather(const MeshGeom& mg, int n, const double* pos, double pos_scale
                   const int* key_start, const MeshRecords& rec, const T* phi, double* gcn, double* gpos,
                   double* mcell_part, int* n_blocks, cudaStream_t s);
 
+// ---- direct Ewald k-sum --------------------------------------------------------------
+struct EwaldGeom {
+  int ns[3];   // Miller-index box (fftfreq order per axis)
+  int S, R;
+};
+struct EwaldWork {
+  int* keys;      // [N]
+  int* counts;    // [S]
+  int* sp_start;  // [S+1]
+  int* order;     // [N] atoms sorted by species
+  int4* sp_of;    // [N] species of each sorted slot
+  double* frac;   // [N*3] fractional coordinates, sorted order
+  void* spec;     // [S*R*nk] structure factors
+  void* hspec;    // [S*R*nk] H = G S
+  double* kpart;  // filter partials
+  double* gpart;  // [N * nchunk * (R+3)] gather partials
+};
+int ewald_chunks(int nk);
+template <typename T>
+int launch_ewald(const EwaldGeom& eg, int n, const double* pos, double ps, const int32_t* species,
+                 const double* c6, const double* dc6, const CellInfo* ci, const GreenPair* gp, const Tables* tab,
+                 const EwaldWork& w, bool need_grad, double* gcn, double* gpos, double* mcell_part, int* n_kspc,
+                 int* n_mcell, cudaStream_t s);
+
 // ---- finalisation ---------------------------------------------------------------
 struct Partials {
   const double* self;  int n_self;     // 1 value per block

@@ -13,7 +13,7 @@ def _energy(m, pos, cell):
     return float(e)
 
 
-@pytest.mark.parametrize("name", ["sio2_648_spme_p5", "hcno_240_spme_p6", "rand_96_pme_p6"])
+@pytest.mark.parametrize("name", ["sio2_648_spme_p5", "hcno_240_spme_p6", "rand_96_pme_p6", "rand_96_ewald_k3_tol1e-2"])
 def test_forces_and_stress_vs_central_differences(name, cuda_device):
     from fourierd3_b200 import D3Model
 

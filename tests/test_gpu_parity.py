@@ -15,7 +15,7 @@ from oracle.neighbours import neighbour_list_cells as oracle_nl
 
 pytestmark = pytest.mark.gpu
 
-MESH_CASES = [n for n in gc.names() if "ewald" not in n]
+ALL_CASES = gc.names()
 E_REL, F_ABS, S_ABS = 1e-10, 1e-8, 1e-9
 
 
@@ -43,7 +43,7 @@ def _strain_protocol(model, positions, cell, edge_index, unit_shifts, device):
     return float(e.detach()), (-pos.grad).cpu().numpy(), stress.cpu().numpy()
 
 
-@pytest.mark.parametrize("name", MESH_CASES)
+@pytest.mark.parametrize("name", ALL_CASES)
 def test_module_edges_fp64_matches_reference(name, cuda_device):
     from fourierd3_b200 import FourierD3
 
@@ -60,7 +60,7 @@ def test_module_edges_fp64_matches_reference(name, cuda_device):
     np.testing.assert_allclose(s, rec["stress"], rtol=0, atol=S_ABS)
 
 
-@pytest.mark.parametrize("name", MESH_CASES)
+@pytest.mark.parametrize("name", ALL_CASES)
 def test_fused_fp64_matches_reference(name, cuda_device):
     from fourierd3_b200 import D3Model
 
@@ -74,7 +74,7 @@ def test_fused_fp64_matches_reference(name, cuda_device):
     np.testing.assert_allclose(s.cpu().numpy(), rec["stress"], rtol=0, atol=S_ABS)
 
 
-@pytest.mark.parametrize("name", MESH_CASES)
+@pytest.mark.parametrize("name", ALL_CASES)
 def test_fused_mixed_precision_error(name, cuda_device):
     from fourierd3_b200 import D3Model
 

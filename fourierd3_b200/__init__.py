@@ -10,6 +10,8 @@ All compute runs in libfd3.so (hand-written sm_100a CUDA kernels + cuFFT).
 from fourierd3_b200.calculator import FourierD3ASECalculator
 from fourierd3_b200.core import FourierD3
 from fourierd3_b200.engine import neighbour_list
-from fourierd3_b200.functional import D3Model, forward
+from fourierd3_b200.batch import D3Batch
+from fourierd3_b200.functional import D3Model, forward, forward_batch
 
-__all__ = ("FourierD3", "FourierD3ASECalculator", "forward", "neighbour_list", "D3Model")
+__all__ = ("FourierD3", "FourierD3ASECalculator", "forward", "forward_batch", "neighbour_list", "D3Model",
+           "D3Batch")

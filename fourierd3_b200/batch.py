@@ -1,0 +1,311 @@
+"""Batched evaluation of many independent periodic structures, optionally as one CUDA graph.
+
+``D3Batch`` takes a list of structures (positions [A], cell [A], atomic numbers) of uneven
+atom counts, cells and mesh sizes and evaluates energy, forces and stress for all of them
+in one call -- the batched form of ``FourierD3ASECalculator.calculate``
+(src/fourierd3/calculator.py:125-192) applied to each structure independently.
+
+Layout on the device:
+
+* one packed positions buffer (sum N, 3) float64 and packed compact species ids; the
+  caller updates positions in place (``positions_view`` / ``set_positions``) between calls;
+* packed outputs: energy (B,), forces (sum N, 3), stress (B, 3, 3);
+* structures are split over ``lanes`` CUDA streams by a longest-processing-time rule on
+  the cost model N + M * S * r (atoms + mesh points x channels); each lane owns ONE
+  workspace buffer sized for the largest structure on that lane and runs its structures
+  back to back, so the device memory held is the sum over lanes of the lane maxima, not
+  the sum over all structures (with 54 species the mesh channels of a 256-structure batch
+  add up to hundreds of GB);
+* plans (species tables, cuFFT plans) are shared by structures with the same species
+  set, method, mesh and Ewald box.
+
+``capture()`` records every lane's launches into one ``torch.cuda.CUDAGraph`` (fork/join
+over the lane streams), after which a call is a single graph replay. The cells are fixed
+for the life of a capture (they set the cell-list grid and the mesh).
+
+``autotune_lanes`` times candidate lane counts under graph replay and caches the winner in
+a JSON file keyed by the batch's shape signature.
+"""
+from __future__ import annotations
+
+import hashlib
+import json
+import os
+import time
+from typing import List, Optional, Sequence, Tuple
+
+import numpy as np
+import torch
+
+from fourierd3_b200 import engine as _engine
+from fourierd3_b200 import geometry
+
+_ALIGN = 256
+
+
+def _mesh_and_box(cell_ang, method: str, mesh_spacing: float, k_cutoff: float):
+    cell_b = np.asarray(cell_ang, dtype=np.float64) * geometry.ANGSTROM_TO_BOHR
+    if method in ("spme", "pme"):
+        return geometry.ns_mesh(cell_b, mesh_spacing * geometry.ANGSTROM_TO_BOHR), (0, 0, 0)
+    return (1, 1, 1), geometry.ewald_ns(cell_b, k_cutoff)
+
+
+def structure_cost(numbers, cell_ang, *, method: str = "spme", mesh_spacing: float = 1.2,
+                   k_cutoff: float = 10.0, c6tol: float = 1.0) -> float:
+    """Cost model N + M * S * r used to balance lanes and ranks."""
+    setup = _engine.species_setup(np.asarray(numbers), c6tol)
+    mesh, ens = _mesh_and_box(cell_ang, method, mesh_spacing, k_cutoff)
+    m = mesh[0] * mesh[1] * mesh[2] if method in ("spme", "pme") else ens[0] * ens[1] * ens[2]
+    return float(len(numbers) + m * setup.n_species * setup.n_rank)
+
+
+def lpt_split(costs: Sequence[float], parts: int) -> List[List[int]]:
+    """Longest-processing-time assignment of items to ``parts`` bins (heaviest first)."""
+    bins: List[List[int]] = [[] for _ in range(parts)]
+    load = [0.0] * parts
+    for i in sorted(range(len(costs)), key=lambda k: (-costs[k], k)):
+        b = min(range(parts), key=lambda q: (load[q], q))
+        bins[b].append(i)
+        load[b] += costs[i]
+    return bins
+
+
+def shard(structures: Sequence, rank: int, world: int, **cost_kw) -> List[int]:
+    """Indices of the structures rank ``rank`` of ``world`` evaluates (LPT on the cost model)."""
+    if not 0 <= rank < world:
+        raise ValueError("rank must be in [0, world)")
+    costs = [structure_cost(z, c, **cost_kw) for (_, c, z) in structures]
+    return sorted(lpt_split(costs, world)[rank])
+
+
+class D3Batch:
+    """Energy, forces and stress of B independent structures per call."""
+
+    def __init__(self, structures: Sequence[Tuple[np.ndarray, np.ndarray, np.ndarray]], *,
+                 method: str = "spme", mesh_spacing: float = 1.2, interpolation_nodes: int = 5,
+                 c6tol: float = 1.0, params=None, r_cut: float = 6.0, k_cutoff: float = 10.0,
+                 precision: str = "mixed", lanes: int = 1, device: Optional[torch.device] = None):
+        if len(structures) == 0:
+            raise ValueError("empty batch")
+        self.device = torch.device(device) if device is not None else torch.device("cuda")
+        if self.device.type != "cuda":
+            raise RuntimeError("fourierd3_b200 computes on CUDA devices only (B200, sm_100a)")
+        if self.device.index is None:
+            self.device = torch.device("cuda", torch.cuda.current_device())
+        self.r_cut = float(r_cut)
+        self.method = method
+        self.precision = precision
+        self.n_struct = len(structures)
+        self._engines: dict = {}
+        self._graph = None
+        counts, cells, species, setups, keys, costs = [], [], [], [], [], []
+        for pos, cell, numbers in structures:
+            pos = np.asarray(pos, dtype=np.float64)
+            numbers = np.asarray(numbers)
+            cell = np.asarray(cell, dtype=np.float64)
+            if pos.ndim != 2 or pos.shape[1] != 3 or pos.shape[0] != numbers.shape[0] or pos.shape[0] < 1:
+                raise ValueError("each structure needs positions (N, 3) and N atomic numbers, N >= 1")
+            if cell.shape != (3, 3):
+                raise ValueError("each cell must be 3x3")
+            setup = _engine.species_setup(numbers, c6tol)
+            mesh, ens = _mesh_and_box(cell, method, mesh_spacing, k_cutoff)
+            key = (setup.types, mesh, ens)
+            if key not in self._engines:
+                self._engines[key] = _engine.Engine(
+                    setup, method=method, order=interpolation_nodes, mesh=mesh, ewald_ns=ens,
+                    precision=precision, r_cut_bohr=self.r_cut * geometry.ANGSTROM_TO_BOHR,
+                    params=params if params is not None else _engine.PBE_BJ, device=self.device)
+            counts.append(pos.shape[0])
+            cells.append(cell)
+            species.append(setup.species)
+            setups.append(setup)
+            keys.append(key)
+            m = mesh[0] * mesh[1] * mesh[2] if method in ("spme", "pme") else ens[0] * ens[1] * ens[2]
+            costs.append(float(pos.shape[0] + m * setup.n_species * setup.n_rank))
+        self.counts = counts
+        self.costs = costs
+        self.offsets = np.concatenate([[0], np.cumsum(counts)]).astype(np.int64)
+        total = int(self.offsets[-1])
+        dev = self.device
+        self.positions = torch.empty((total, 3), dtype=torch.float64, device=dev)
+        self.positions.copy_(torch.from_numpy(np.concatenate([np.asarray(p, dtype=np.float64)
+                                                              for p, _, _ in structures])))
+        self.species = torch.from_numpy(np.concatenate(species).astype(np.int32)).to(dev)
+        self.cells_host = np.stack(cells)
+        self.cells = torch.from_numpy(self.cells_host.reshape(-1, 9).copy()).to(dev)
+        self.energy = torch.zeros((self.n_struct,), dtype=torch.float64, device=dev)
+        self.forces = torch.zeros((total, 3), dtype=torch.float64, device=dev)
+        self.stress = torch.zeros((self.n_struct, 3, 3), dtype=torch.float64, device=dev)
+        self._keys = keys
+        self._need = [self._engines[k].workspace_bytes(counts[i], cells[i], self.r_cut)
+                      for i, k in enumerate(keys)]
+        self.lanes = 0
+        self.set_lanes(lanes)
+
+    # ------------------------------------------------------------------ lanes
+    def set_lanes(self, lanes: int) -> None:
+        """Split the structures over ``lanes`` streams, each with one workspace (drops a capture)."""
+        lanes = max(1, min(int(lanes), self.n_struct))
+        if lanes == self.lanes:
+            return
+        self._graph = None
+        self._work = None
+        torch.cuda.synchronize(self.device)
+        split = lpt_split(self.costs, lanes)
+        self.lane_of = np.zeros(self.n_struct, dtype=np.int64)
+        for q, items in enumerate(split):
+            self.lane_of[items] = q
+        sizes = [max(self._need[i] for i in items) if items else 0 for items in split]
+        self.workspace_bytes = int(sum(-(-s // _ALIGN) * _ALIGN for s in sizes))
+        self._work = torch.empty(max(self.workspace_bytes, 1), dtype=torch.uint8, device=self.device)
+        self._streams = [torch.cuda.Stream(self.device) for _ in range(lanes)]
+        self._lane_calls = []
+        base = 0
+        for q, items in enumerate(split):
+            wsl = self._work[base: base + sizes[q]]
+            base += -(-sizes[q] // _ALIGN) * _ALIGN
+            calls = []
+            # heaviest first inside a lane as well: the long mesh stages start early
+            for i in sorted(items, key=lambda k: (-self.costs[k], k)):
+                a, b = int(self.offsets[i]), int(self.offsets[i + 1])
+                calls.append((self._engines[self._keys[i]], self.positions[a:b], self.cells_host[i],
+                              self.cells[i], (self.energy[i], self.forces[a:b], self.stress[i]),
+                              self.species[a:b], wsl))
+            self._lane_calls.append(calls)
+        self.lanes = lanes
+
+    def _launch_all(self) -> None:
+        main = torch.cuda.current_stream(self.device)
+        fork = torch.cuda.Event()
+        fork.record(main)
+        joins = []
+        for st, calls in zip(self._streams, self._lane_calls):
+            st.wait_event(fork)
+            with torch.cuda.stream(st):
+                for eng, pos, cell_h, cell_d, out, spc, wsl in calls:
+                    eng.energy_forces_stress(pos, cell_h, self.r_cut, cell_dev=cell_d, out=out,
+                                             species=spc, work=wsl)
+                ev = torch.cuda.Event()
+                ev.record(st)
+            joins.append(ev)
+        for ev in joins:
+            main.wait_event(ev)
+
+    # ------------------------------------------------------------------ graph
+    def capture(self) -> None:
+        """Record the whole batch (all lanes) as one CUDA graph; later calls replay it."""
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(side):
+            self._launch_all()  # warm-up outside the capture: cuFFT and module loading
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self._launch_all()
+        torch.cuda.synchronize(self.device)
+        self._graph = g
+
+    @property
+    def captured(self) -> bool:
+        return self._graph is not None
+
+    # ------------------------------------------------------------------ calls
+    def positions_view(self, i: int) -> torch.Tensor:
+        a, b = int(self.offsets[i]), int(self.offsets[i + 1])
+        return self.positions[a:b]
+
+    def set_positions(self, positions) -> None:
+        """Copy new positions in: a packed (sum N, 3) tensor or a list of (N_i, 3) arrays."""
+        if isinstance(positions, (list, tuple)):
+            if len(positions) != self.n_struct:
+                raise ValueError("one positions array per structure expected")
+            for i, p in enumerate(positions):
+                t = torch.as_tensor(p, dtype=torch.float64)
+                if tuple(t.shape) != (self.counts[i], 3):
+                    raise ValueError(f"structure {i}: positions must be ({self.counts[i]}, 3)")
+                self.positions_view(i).copy_(t, non_blocking=True)
+        else:
+            t = torch.as_tensor(positions, dtype=torch.float64)
+            if tuple(t.shape) != tuple(self.positions.shape):
+                raise ValueError(f"packed positions must be {tuple(self.positions.shape)}")
+            self.positions.copy_(t, non_blocking=True)
+
+    def __call__(self, positions=None):
+        """(energy [eV] (B,), forces [eV/A] (sum N, 3), stress [eV/A^3] (B, 3, 3)) on the device.
+
+        The returned tensors are the batch's static output buffers: the next call overwrites them.
+        """
+        if positions is not None:
+            self.set_positions(positions)
+        if self._graph is not None:
+            self._graph.replay()
+        else:
+            self._launch_all()
+        return self.energy, self.forces, self.stress
+
+    def split_forces(self, forces: Optional[torch.Tensor] = None) -> List[torch.Tensor]:
+        f = self.forces if forces is None else forces
+        return [f[int(self.offsets[i]): int(self.offsets[i + 1])] for i in range(self.n_struct)]
+
+    # ------------------------------------------------------------------ autotuning
+    def signature(self) -> str:
+        h = hashlib.sha1()
+        h.update(json.dumps([self.method, self.precision, self.r_cut]).encode())
+        for i in range(self.n_struct):
+            k = self._keys[i]
+            h.update(json.dumps([self.counts[i], list(k[0]), list(k[1]), list(k[2])]).encode())
+        dev = torch.cuda.get_device_properties(self.device)
+        h.update(f"{dev.name}:{dev.multi_processor_count}".encode())
+        return h.hexdigest()[:20]
+
+    def time_replays(self, reps: int = 3) -> float:
+        """Milliseconds per graph replay (captures first if needed), median of ``reps``."""
+        if self._graph is None:
+            self.capture()
+        st = torch.cuda.current_stream(self.device)
+        times = []
+        for _ in range(reps):
+            a = torch.cuda.Event(enable_timing=True)
+            b = torch.cuda.Event(enable_timing=True)
+            a.record(st)
+            self._graph.replay()
+            b.record(st)
+            b.synchronize()
+            times.append(a.elapsed_time(b))
+        return float(np.median(times))
+
+
+def autotune_lanes(batch: D3Batch, candidates: Sequence[int] = (1, 2, 4, 8), *,
+                   cache: Optional[str] = None, reps: int = 3, mem_fraction: float = 0.6) -> int:
+    """Choose the lane count with the fastest graph replay; cache it per batch signature.
+
+    Candidates whose lane workspaces would exceed ``mem_fraction`` of the free device
+    memory are skipped. With ``cache`` (a JSON path) a known signature is not re-timed.
+    """
+    sig = batch.signature()
+    table = {}
+    if cache and os.path.exists(cache):
+        with open(cache) as f:
+            table = json.load(f)
+        if sig in table:
+            batch.set_lanes(int(table[sig]["lanes"]))
+            return batch.lanes
+    results = {}
+    for q in candidates:
+        split = lpt_split(batch.costs, max(1, min(q, batch.n_struct)))
+        need = sum(max(batch._need[i] for i in items) for items in split if items)
+        free, _ = torch.cuda.mem_get_info(batch.device)
+        if need > mem_fraction * (free + batch.workspace_bytes):
+            continue
+        batch.set_lanes(q)
+        results[batch.lanes] = batch.time_replays(reps)
+    best = min(results, key=results.get)
+    batch.set_lanes(best)
+    if cache:
+        table[sig] = {"lanes": best, "ms": results, "when": time.strftime("%Y-%m-%d %H:%M:%S")}
+        tmp = cache + ".tmp"
+        with open(tmp, "w") as f:
+            json.dump(table, f, indent=1, sort_keys=True)
+        os.replace(tmp, cache)
+    return best

@@ -195,20 +195,21 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
         }
       }
       // batched 3D real transforms over the S*R channels (only library call of the pipeline)
-      int n[3] = {m.n[0], m.n[1], m.n[2]};
-      const int C = S * R;
-      const int M = m.n[0] * m.n[1] * m.n[2];
-      const int Mhi = (int)Mh;
+      // 64-bit plan: C * M passes 2^31 elements for many-species boxes on 256^3 meshes
+      long long n[3] = {m.n[0], m.n[1], m.n[2]};
+      const long long C = (long long)S * R;
+      const long long M = (long long)m.n[0] * m.n[1] * m.n[2];
+      const long long Mhi = (long long)Mh;
       const bool dp = d->precision == FD3_PREC_FP64;
       size_t ws1 = 0, ws2 = 0;
       cufftResult fr;
       if ((fr = cufftCreate(&p->fwd)) != CUFFT_SUCCESS || (fr = cufftCreate(&p->inv)) != CUFFT_SUCCESS ||
           (fr = cufftSetAutoAllocation(p->fwd, 0)) != CUFFT_SUCCESS ||
           (fr = cufftSetAutoAllocation(p->inv, 0)) != CUFFT_SUCCESS ||
-          (fr = cufftMakePlanMany(p->fwd, 3, n, nullptr, 1, M, nullptr, 1, Mhi, dp ? CUFFT_D2Z : CUFFT_R2C, C,
-                                  &ws1)) != CUFFT_SUCCESS ||
-          (fr = cufftMakePlanMany(p->inv, 3, n, nullptr, 1, Mhi, nullptr, 1, M, dp ? CUFFT_Z2D : CUFFT_C2R, C,
-                                  &ws2)) != CUFFT_SUCCESS) {
+          (fr = cufftMakePlanMany64(p->fwd, 3, n, nullptr, 1, M, nullptr, 1, Mhi, dp ? CUFFT_D2Z : CUFFT_R2C, C,
+                                    &ws1)) != CUFFT_SUCCESS ||
+          (fr = cufftMakePlanMany64(p->inv, 3, n, nullptr, 1, Mhi, nullptr, 1, M, dp ? CUFFT_Z2D : CUFFT_C2R, C,
+                                    &ws2)) != CUFFT_SUCCESS) {
         char b[64];
         snprintf(b, sizeof(b), "cufft status %d", (int)fr);
         set_error("fd3_plan_create: cufft plan", b);

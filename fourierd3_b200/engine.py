@@ -145,6 +145,14 @@ class Engine:
             self._work = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
         return self._work
 
+    def workspace_bytes(self, n_atoms: int, cell_ang: np.ndarray, r_cut_ang: float) -> int:
+        """Bytes of device workspace one fused call on this structure shape needs."""
+        nb, _ = self.cell_grid(cell_ang, r_cut_ang)
+        nbytes = ctypes.c_size_t()
+        _native.check(_native.lib().fd3_workspace_size(self._plan, n_atoms, nb[0] * nb[1] * nb[2],
+                                                       ctypes.byref(nbytes)), "fd3_workspace_size")
+        return int(nbytes.value)
+
     @staticmethod
     def cell_grid(cell_ang: np.ndarray, r_cut_ang: float):
         c = np.ascontiguousarray(cell_ang, dtype=np.float64).reshape(9)
@@ -198,12 +206,21 @@ class Engine:
         return energy, gpos, gsh, gcell
 
     def energy_forces_stress(self, pos_ang: torch.Tensor, cell_ang: np.ndarray, r_cut_ang: float,
-                             cell_dev: Optional[torch.Tensor] = None, out=None):
-        """Fused path. Returns (energy [eV], forces [eV/A], stress [eV/A^3] 3x3)."""
+                             cell_dev: Optional[torch.Tensor] = None, out=None,
+                             species: Optional[torch.Tensor] = None, work: Optional[torch.Tensor] = None):
+        """Fused path. Returns (energy [eV], forces [eV/A], stress [eV/A^3] 3x3).
+
+        ``species`` (int32 compact ids on the device) and ``work`` (a uint8 device buffer of
+        at least ``workspace_bytes``) let a caller that owns its buffers -- the batch runner,
+        a captured CUDA graph -- keep every pointer fixed; by default the engine's own are used.
+        """
         n = pos_ang.shape[0]
         cell_h = np.ascontiguousarray(cell_ang, dtype=np.float64).reshape(9)
-        (nb, _) = self.cell_grid(cell_h, r_cut_ang)
-        work = self.workspace(n, nb[0] * nb[1] * nb[2])
+        if work is None:
+            (nb, _) = self.cell_grid(cell_h, r_cut_ang)
+            work = self.workspace(n, nb[0] * nb[1] * nb[2])
+        if species is None:
+            species = self.species_tensor()
         if cell_dev is None:
             cell_dev = torch.as_tensor(cell_h, dtype=torch.float64).to(self.device, non_blocking=False)
         if out is None:
@@ -213,7 +230,7 @@ class Engine:
         else:
             energy, forces, stress = out
         rc = _native.lib().fd3_energy_forces_stress(
-            self._plan, n, ctypes.c_void_p(pos_ang.data_ptr()), ctypes.c_void_p(self.species_tensor().data_ptr()),
+            self._plan, n, ctypes.c_void_p(pos_ang.data_ptr()), ctypes.c_void_p(species.data_ptr()),
             _native.dptr(cell_h), ctypes.c_void_p(cell_dev.data_ptr()), float(r_cut_ang),
             ctypes.c_void_p(work.data_ptr()), work.numel(), ctypes.c_void_p(energy.data_ptr()),
             ctypes.c_void_p(forces.data_ptr()), ctypes.c_void_p(stress.data_ptr()),

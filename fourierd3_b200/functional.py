@@ -66,3 +66,37 @@ def forward(positions, cell, numbers, **kwargs):
         model = D3Model(nums, cell_np, **kwargs)
         _CACHE[key] = model
     return model(positions, cell_np)
+
+
+_BATCH_CACHE: dict = {}
+
+
+def forward_batch(structures, *, graph: bool = True, lanes: int = 1, **kwargs):
+    """Batched ``forward``: ``structures`` is a list of (positions, cell, numbers).
+
+    Returns a list of (energy [eV] 0-d, forces [eV/A] (N_i, 3), stress [eV/A^3] (3, 3))
+    device tensors, one per structure (views into the batch's output buffers, overwritten
+    by the next call on the same batch). The batch (plans, workspaces and, with ``graph``,
+    the captured CUDA graph) is cached per list of atomic numbers and cells, so repeated
+    calls with new positions are a copy plus one graph replay.
+    """
+    from fourierd3_b200.batch import D3Batch
+
+    host = []
+    for pos, cell, numbers in structures:
+        cell_np = np.asarray(cell.detach().cpu() if torch.is_tensor(cell) else cell, dtype=np.float64)
+        nums = np.asarray(numbers.cpu() if torch.is_tensor(numbers) else numbers)
+        host.append((pos, cell_np, nums))
+    key = (tuple((n.tobytes(), c.tobytes()) for _, c, n in host), lanes, graph,
+           tuple(sorted(kwargs.items())))
+    batch = _BATCH_CACHE.get(key)
+    if batch is None:
+        first = [(np.asarray(p.detach().cpu() if torch.is_tensor(p) else p, dtype=np.float64), c, n)
+                 for p, c, n in host]
+        batch = D3Batch(first, lanes=lanes, **kwargs)
+        if graph:
+            batch.capture()
+        _BATCH_CACHE[key] = batch
+    e, f, s = batch([p for p, _, _ in host])
+    fs = batch.split_forces(f)
+    return [(e[i], fs[i], s[i]) for i in range(batch.n_struct)]

@@ -226,7 +226,7 @@ BATCH_WORKLOAD = "batch256_N32-4096_Z1-54_spme_p5_h1.2_E+F+stress"
 def run_batch(args, ws, rank, local):
     """Batch workload: structures sharded over ranks (LPT on N + M*S*r), one graph per rank."""
     from fourierd3_b200 import _native, structures as st
-    from fourierd3_b200.batch import D3Batch, autotune_lanes, lpt_split
+    from fourierd3_b200.batch import D3Batch, autotune_filter, autotune_lanes, lpt_split
 
     device = torch.device("cuda", local)
     structs = st.batch_boxes(args.batch_size, seed=0)
@@ -246,10 +246,12 @@ def run_batch(args, ws, rank, local):
     setup_s = time.perf_counter() - t0
     steps = max(1, min(args.steps, 5))
     warm = max(3, min(args.warmup, 3))
+    # per-structure launches, default tiles: the untuned eager baseline
     res["mixed_eager_1lane"] = max_over_ranks(time_steps(lambda: plain(), steps, warm, ws, device), ws, device)
     del plain
     torch.cuda.empty_cache()
     b = D3Batch(sub, precision="mixed", lanes=1, device=device, **kw)
+    ftune = autotune_filter(b, reps=1)
     lanes = autotune_lanes(b, (1, 2, 4), reps=2)
     if not b.captured:
         b.capture()
@@ -299,7 +301,9 @@ def run_batch(args, ws, rank, local):
         "data": "synthetic",
         "config": {"workload": BATCH_WORKLOAD, "n_structures": len(structs), "n_atoms": n_total,
                    "n_atoms_rank0": n_local, "lanes": lanes, "mesh_channel_points_rank0": mesh_pts,
-                   "l2": "inputs larger than L2", "parallelism": f"shard{ws}", "setup_s": setup_s},
+                   "l2": "inputs larger than L2", "parallelism": f"shard{ws}", "setup_s": setup_s,
+                   "filter_tile_by_species_class": {str(k): v[0] for k, v in ftune.items()},
+                   "filter_tile_ms": {str(k): v[1] for k, v in ftune.items()}},
         "per_structure_eager": {"value": n_total / (res["mixed_eager_1lane"] * 1e-3),
                                 "ms_per_step": res["mixed_eager_1lane"]},
         "graph_over_eager": res["mixed_eager_1lane"] / ms,

@@ -15,6 +15,7 @@ _LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "_lib", "li
 FD3_OK, FD3_EINVAL, FD3_ECAPACITY, FD3_ECUDA, FD3_ECUFFT, FD3_ENOMEM = range(6)
 METHODS = {"spme": 0, "pme": 1, "ewald": 2}
 PREC_FP64, PREC_MIXED = 0, 1
+TUNE_FILTER_KT = 0
 
 _c_int32 = ctypes.c_int32
 _c_int64 = ctypes.c_int64
@@ -37,6 +38,8 @@ class PlanDesc(ctypes.Structure):
 _SIGS = {
     "fd3_plan_create": (ctypes.c_int, [ctypes.POINTER(PlanDesc), ctypes.POINTER(_vp)]),
     "fd3_plan_destroy": (ctypes.c_int, [_vp]),
+    "fd3_plan_set_tuning": (ctypes.c_int, [_vp, _c_int32, _c_int32]),
+    "fd3_plan_get_tuning": (ctypes.c_int, [_vp, _c_int32, ctypes.POINTER(_c_int32)]),
     "fd3_workspace_size": (ctypes.c_int, [_vp, _c_int64, _c_int64, ctypes.POINTER(ctypes.c_size_t)]),
     "fd3_cell_grid": (ctypes.c_int, [_dp, _c_double, ctypes.POINTER(_c_int32), ctypes.POINTER(_c_int32)]),
     "fd3_energy_edges": (ctypes.c_int, [_vp, _c_int64, _vp, _vp, _vp, _c_int64, _vp, _vp, _vp, _c_int32, _vp,

@@ -276,6 +276,58 @@ class D3Batch:
         return float(np.median(times))
 
 
+def _profiled_stage(batch: "D3Batch", i: int, stage: str, reps: int = 2) -> float:
+    """Milliseconds of one pipeline stage of structure ``i`` (eager, profiled calls)."""
+    q = int(batch.lane_of[i])
+    for call in batch._lane_calls[q]:
+        eng, pos, cell_h, cell_d, out, spc, wsl = call
+        if pos.data_ptr() == batch.positions_view(i).data_ptr():
+            eng.profile(True)
+            best = float("inf")
+            for _ in range(reps + 1):
+                eng.energy_forces_stress(pos, cell_h, batch.r_cut, cell_dev=cell_d, out=out, species=spc, work=wsl)
+                best = min(best, eng.stage_times().get(stage, float("inf")))
+            eng.profile(False)
+            return best
+    raise KeyError(i)
+
+
+def autotune_filter(batch: "D3Batch", candidates: Sequence[int] = (0, 1, 2, 4, 8, 16), reps: int = 2) -> dict:
+    """Pick the filter k-tile per species-count class from the heaviest structure of each class.
+
+    Classes: up to 8 species, 9-24, 25-64. Each class is timed on its heaviest structure
+    (profiled eager calls) and its best tile is set on every engine of that class where it
+    is valid. Returns {class: (tile, {tile: ms})}. Drops a captured graph.
+    """
+    batch._graph = None
+    classes: dict = {}
+    for i, key in enumerate(batch._keys):
+        s = len(key[0])
+        c = 0 if s <= 8 else (1 if s <= 24 else 2)
+        if c not in classes or batch.costs[i] > batch.costs[classes[c]]:
+            classes[c] = i
+    out = {}
+    for c, i in sorted(classes.items()):
+        eng = batch._engines[batch._keys[i]]
+        times = {}
+        for kt in candidates:
+            try:
+                eng.set_tuning(filter_kt=kt)
+            except ValueError:
+                continue
+            times[kt] = _profiled_stage(batch, i, "filter", reps)
+        best = min(times, key=times.get)
+        for key, e in batch._engines.items():
+            s = len(key[0])
+            if (0 if s <= 8 else (1 if s <= 24 else 2)) == c:
+                try:
+                    e.set_tuning(filter_kt=best)
+                except ValueError:
+                    e.set_tuning(filter_kt=-1)
+        out[c] = (best, times)
+    return out
+
+
 def autotune_lanes(batch: D3Batch, candidates: Sequence[int] = (1, 2, 4, 8), *,
                    cache: Optional[str] = None, reps: int = 3, mem_fraction: float = 0.6) -> int:
     """Choose the lane count with the fastest graph replay; cache it per batch signature.

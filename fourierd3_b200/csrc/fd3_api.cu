@@ -185,6 +185,7 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
       m.lagrange = d->method == FD3_METHOD_PME;
       m.S = S;
       m.R = R;
+      m.filter_kt = -1;
       const size_t Mh = (size_t)m.n[0] * m.n[1] * m.nzh;
       if (d->method == FD3_METHOD_SPME && d->deconv) {
         if (cudaMalloc(&p->d_deconv, sizeof(float) * Mh) != cudaSuccess ||
@@ -229,6 +230,35 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
   return FD3_OK;
 }
 
+extern "C" int fd3_plan_set_tuning(fd3_plan* p, int32_t knob, int32_t value) {
+  if (!p) return FD3_EINVAL;
+  if (knob == FD3_TUNE_FILTER_KT) {
+    if (p->method == FD3_METHOD_EWALD) return FD3_OK;   // no mesh filter
+    const size_t ts = p->precision == FD3_PREC_FP64 ? 8 : 4;
+    if (value != -1 && !filter_kt_valid(value, p->S, p->R, ts)) {
+      set_error("fd3_plan_set_tuning", "filter k-tile must be -1, 0 (<= 8 species) or 1/2/4/8/16 within shared memory");
+      return FD3_EINVAL;
+    }
+    p->mg.filter_kt = value;
+    return FD3_OK;
+  }
+  set_error("fd3_plan_set_tuning", "unknown knob");
+  return FD3_EINVAL;
+}
+
+extern "C" int fd3_plan_get_tuning(const fd3_plan* p, int32_t knob, int32_t* value) {
+  if (!p || !value) return FD3_EINVAL;
+  if (knob == FD3_TUNE_FILTER_KT) {
+    const size_t ts = p->precision == FD3_PREC_FP64 ? 8 : 4;
+    *value = p->method == FD3_METHOD_EWALD ? -1
+             : p->mg.filter_kt >= 0        ? p->mg.filter_kt
+                                           : filter_default_kt(p->S, p->R, ts);
+    return FD3_OK;
+  }
+  set_error("fd3_plan_get_tuning", "unknown knob");
+  return FD3_EINVAL;
+}
+
 extern "C" int fd3_plan_destroy(fd3_plan* p) {
   if (!p) return FD3_OK;
   for (int k = 0; k < fd3_plan::kMaxMarks; ++k)
@@ -266,7 +296,7 @@ struct Work {
   CellList cl;
   HitStore hits;
   EwaldWork ew;
-  void *rho, *spec, *spec2, *fftw;
+  void *rho, *spec, *fftw;
 };
 
 // K = number of cell-list bins of the fused path, 0 for the edge-list path (no cell list).
@@ -325,8 +355,6 @@ void carve(const fd3_plan* p, int64_t N, int64_t K_in, Carver& c, Work& w) {
   const size_t C = (size_t)p->S * p->R;
   w.rho = c.take<char>(mesh ? C * M * es : 1);
   w.spec = c.take<char>(mesh ? C * Mh * 2 * es : 1);
-  // more than 8 species: the filter writes H out of place
-  w.spec2 = c.take<char>(mesh && p->S > 8 ? C * Mh * 2 * es : 1);
   w.fftw = c.take<char>(p->fft_ws);
   // direct Ewald sum
   if (!mesh) {
@@ -398,9 +426,9 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
   else
     FD3_CUFFT(cufftExecR2C(p->fwd, (cufftReal*)w.rho, (cufftComplex*)w.spec));
   prof_mark(p, s, "fft_r2c");
-  void* hspec = p->S > 8 ? w.spec2 : w.spec;
+  void* hspec = w.spec;   // the filter overwrites the spectrum with H in place
   FD3_TRY(launch_filter<T>(mg, w.ci, p->d_green, p->d_tab, p->d_deconv, p->method == FD3_METHOD_SPME, w.spec,
-                           hspec, w.kspc_part, n_kspc, s));
+                           w.kspc_part, n_kspc, s));
   prof_mark(p, s, "filter");
   *n_mcell = 0;
   if (!need_grad) return FD3_OK;

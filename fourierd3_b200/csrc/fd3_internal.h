@@ -110,6 +110,7 @@ struct MeshGeom {
   int order;      // p
   int lagrange;   // 0: B-spline (spme), 1: Lagrange (pme)
   int S, R;
+  int filter_kt;  // filter k-tile width (0: register kernel), -1: default for (S, R)
 };
 int launch_cellinfo(const double* cell, double scale, CellInfo* ci, cudaStream_t s);
 int launch_mesh_keys(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
@@ -128,9 +129,10 @@ int launch_spread(const MeshGeom& mg, int n, const double* pos, double pos_scale
                   const MeshRecords& rec, T* rho, cudaStream_t s);
 template <typename T>
 int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab,
-                  const float* deconv, int spme, void* spec, void* spec_out, double* part, int* n_blocks,
-                  cudaStream_t s);
+                  const float* deconv, int spme, void* spec, double* part, int* n_blocks, cudaStream_t s);
 int filter_max_blocks();
+int filter_default_kt(int S, int R, size_t tsize);
+bool filter_kt_valid(int kt, int S, int R, size_t tsize);
 template <typename T>
 int launch_gather(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
                   const double* c6, const double* dc6, const CellInfo* ci, const Tables* tab, const int* order,

@@ -247,123 +247,243 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int
   block_sum_store<7>(acc, part + 7 * blockIdx.x);
 }
 
-// Any number of species (<= 64): G_XY evaluated per pair on the fly, H written out of place
-// (spec_out), ranks in chunks of 8 held in registers.
-constexpr int kAnyRC = 8;
-template <typename T>
-__global__ void __launch_bounds__(kFilterThreads) k_filter_any(MeshDev g, int P, int spme,
-                                                               const CellInfo* __restrict__ ci,
-                                                               const GreenPair* __restrict__ gp,
-                                                               const Tables* __restrict__ tab,
-                                                               const float* __restrict__ deconv,
-                                                               const typename Cplx<T>::type* __restrict__ spec,
-                                                               typename Cplx<T>::type* __restrict__ spec_out,
-                                                               double* __restrict__ part) {
+// Many species (<= 64), any rank: k-tiled filter. One CTA takes KT consecutive rfft k-points at a
+// time and stages their S*R spectrum values in shared memory (one coalesced read of the tile).
+//   phase B: the S(S+1)/2 species pairs X <= Y are spread over the CTA's 256/KT thread slots,
+//            each thread keeping one k column: G_XY, dG_XY (and the conjugate-partner average on
+//            the self-conjugate planes) are evaluated ONCE per pair and k, the pair's share of
+//            the energy and virial  w_XY G_XY sum_r lambda_r Re(S_Xr S_Yr*)  (w = 1 on the
+//            diagonal, 2 off it) is accumulated, and the Hermitian-averaged G is kept in
+//            shared memory;
+//   phase C: thread (X, k) forms H_Xr = sum_Y Gh_XY S_Yr from shared memory and writes it over
+//            the spectrum tile it came from (in place: no other CTA reads these k columns).
+// Green evaluations per k fall from S^2 to S(S+1)/2 and the spectrum is read from HBM once,
+// instead of once per X from L2.
+struct FilterTileSmem {
+  static size_t bytes(int S, int R, int kt, size_t tsize) {
+    const size_t C = (size_t)S * R, np = (size_t)S * (S + 1) / 2;
+    size_t b = C * kt * 2 * tsize;              // spectrum tile
+    b += 32 * tsize;                            // lambda_r
+    b += np * kt * tsize;                       // Gh tile
+    b += np * sizeof(uint32_t);                 // pair -> (X, Y)
+    b += (size_t)S * sizeof(int);               // first pair index of row X
+    return (b + 15) & ~(size_t)15;
+  }
+};
+
+template <typename T, int KT>
+__global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int P, int spme,
+                                                                 const CellInfo* __restrict__ ci,
+                                                                 const GreenPair* __restrict__ gp,
+                                                                 const Tables* __restrict__ tab,
+                                                                 const float* __restrict__ deconv,
+                                                                 typename Cplx<T>::type* __restrict__ spec,
+                                                                 double* __restrict__ part) {
   using C2 = typename Cplx<T>::type;
-  const int S = g.S, R = g.R;
+  constexpr int NSLOT = kFilterThreads / KT;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int S = g.S, R = g.R, C = S * R, NP = S * (S + 1) / 2;
+  // sections in decreasing alignment: T-sized arrays first, then the 4-byte tables
+  C2* ss = reinterpret_cast<C2*>(smem_raw);                  // [C][KT]
+  T* lam = reinterpret_cast<T*>(ss + (size_t)C * KT);        // [32]
+  T* gs = lam + 32;                                          // [NP][KT]
+  uint32_t* pxy = reinterpret_cast<uint32_t*>(gs + (size_t)NP * KT);
+  int* row0 = reinterpret_cast<int*>(pxy + NP);
+  for (int X = threadIdx.x; X < S; X += blockDim.x) row0[X] = X * S - X * (X - 1) / 2;
+  for (int X = 0; X < S; ++X)
+    for (int Y = X + threadIdx.x; Y < S; Y += blockDim.x) pxy[X * S - X * (X - 1) / 2 + (Y - X)] = (X << 16) | Y;
+  for (int r = threadIdx.x; r < R; r += blockDim.x) lam[r] = (T)tab->eigs[r];
   const size_t Mh = (size_t)g.n[0] * g.n[1] * g.nzh;
-  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  const size_t ntile = (Mh + KT - 1) / KT;
+  const int kk = threadIdx.x % KT, slot = threadIdx.x / KT;
   const T s6 = (T)tab->s6, s8 = (T)tab->s8;
   T rc[9];
   load_recip<T>(ci, rc);
-  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < Mh; k += (size_t)gridDim.x * blockDim.x) {
-    const KPoint<T> q = kpoint<T>(g, k, rc, deconv, spme, P);
-    const T kt = q.knorm, kpt = q.kpart;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};
+  for (size_t tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+    const size_t k0 = tile * KT;
+    __syncthreads();   // the previous tile's phase C has finished with ss / gs (and the tables are set)
+    for (int e = threadIdx.x; e < C * KT; e += kFilterThreads) {
+      const int c = e / KT, j = e % KT;
+      const size_t k = k0 + j;
+      ss[e] = k < Mh ? spec[(size_t)c * Mh + k] : C2{T(0), T(0)};
+    }
+    const size_t k = k0 + kk;
+    const bool valid = k < Mh;
+    const KPoint<T> q = kpoint<T>(g, valid ? k : 0, rc, deconv, spme, P);
+    __syncthreads();
     T qq = T(0), dq = T(0);
-    for (int r0 = 0; r0 < R; r0 += kAnyRC) {
-      for (int X = 0; X < S; ++X) {
-        C2 hq[kAnyRC], hd[kAnyRC], hh[kAnyRC];
+    for (int pi = slot; pi < NP; pi += NSLOT) {
+      const uint32_t xy = pxy[pi];
+      const int X = (int)(xy >> 16), Y = (int)(xy & 0xffffu);
+      T gv, dv;
+      green_eval<T>(gp[X * S + Y], q.knorm, s6, s8, gv, dv);
+      gv *= q.inv_sc;
+      dv *= q.inv_sc;
+      T gh = gv;
+      if (q.partner) {
+        T gpv, dpv;
+        green_eval<T>(gp[X * S + Y], q.kpart, s6, s8, gpv, dpv);
+        gh = T(0.5) * (gv + gpv * q.inv_sc);
+      }
+      const C2* sx = ss + (size_t)X * R * KT + kk;
+      const C2* sy = ss + (size_t)Y * R * KT + kk;
+      T pr = T(0);
+      for (int r = 0; r < R; ++r) {
+        const C2 a = sx[r * KT], b = sy[r * KT];
+        pr += lam[r] * (a.x * b.x + a.y * b.y);
+      }
+      const T w = X == Y ? T(1) : T(2);
+      qq += w * gv * pr;
+      dq += w * dv * pr;
+      gs[pi * KT + kk] = gh;
+    }
+    if (valid) {
+      acc[0] += (double)(q.wk * qq);
+      virial_acc<T>(q, dq, acc);
+    }
+    __syncthreads();
+    for (int X = slot; X < S; X += NSLOT) {
+      for (int r0 = 0; r0 < R; r0 += 8) {
+        C2 h[8];
 #pragma unroll
-        for (int r = 0; r < kAnyRC; ++r) hq[r] = hd[r] = hh[r] = C2{T(0), T(0)};
+        for (int r = 0; r < 8; ++r) h[r] = C2{T(0), T(0)};
         for (int Y = 0; Y < S; ++Y) {
-          T gv, dv;
-          green_eval<T>(gp[X * S + Y], kt, s6, s8, gv, dv);
-          gv *= q.inv_sc;
-          dv *= q.inv_sc;
-          T gh = gv;
-          if (q.partner) {
-            T gpv, dpv;
-            green_eval<T>(gp[X * S + Y], kpt, s6, s8, gpv, dpv);
-            gh = T(0.5) * (gv + gpv * q.inv_sc);
-          }
+          const int pi = X <= Y ? row0[X] + (Y - X) : row0[Y] + (X - Y);
+          const T gh = gs[pi * KT + kk];
+          const C2* sy = ss + ((size_t)Y * R + r0) * KT + kk;
 #pragma unroll
-          for (int r = 0; r < kAnyRC; ++r) {
+          for (int r = 0; r < 8; ++r)
             if (r0 + r < R) {
-              const C2 sy = spec[((size_t)Y * R + r0 + r) * Mh + k];
-              hq[r].x += gv * sy.x; hq[r].y += gv * sy.y;
-              hd[r].x += dv * sy.x; hd[r].y += dv * sy.y;
-              hh[r].x += gh * sy.x; hh[r].y += gh * sy.y;
+              const C2 b = sy[r * KT];
+              h[r].x += gh * b.x;
+              h[r].y += gh * b.y;
             }
-          }
         }
+        if (valid) {
 #pragma unroll
-        for (int r = 0; r < kAnyRC; ++r) {
-          if (r0 + r < R) {
-            const size_t idx = ((size_t)X * R + r0 + r) * Mh + k;
-            const C2 sx = spec[idx];
-            const T lam = (T)tab->eigs[r0 + r];
-            qq += lam * (sx.x * hq[r].x + sx.y * hq[r].y);
-            dq += lam * (sx.x * hd[r].x + sx.y * hd[r].y);
-            spec_out[idx] = hh[r];
-          }
+          for (int r = 0; r < 8; ++r)
+            if (r0 + r < R) spec[((size_t)X * R + r0 + r) * Mh + k] = h[r];
         }
       }
     }
-    acc[0] += (double)(q.wk * qq);
-    virial_acc<T>(q, dq, acc);
   }
   block_sum_store<7>(acc, part + 7 * blockIdx.x);
 }
 
-static int filter_grid(size_t Mh) {
+static int device_sms() {
   static int sms = 0;
   if (sms == 0) {
     int dev = 0;
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
   }
+  return sms;
+}
+
+static int filter_grid(size_t Mh) {
   const size_t need = (Mh + kFilterThreads - 1) / kFilterThreads;
-  const size_t cap = (size_t)sms * 8;
+  const size_t cap = (size_t)device_sms() * 8;
   return (int)(need < cap ? need : cap);
 }
 
 int filter_max_blocks() { return 148 * 8 * 4; }
 
-template <typename T>
-int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab,
-                  const float* deconv, int spme, void* spec, void* spec_out, double* part, int* n_blocks,
-                  cudaStream_t s) {
-  using C2 = typename Cplx<T>::type;
+// Largest k-tile width whose shared-memory tile fits (the default when no tuning is set).
+int filter_default_kt(int S, int R, size_t tsize) {
+  if (S <= 4) return 0;   // register kernel
+  for (int kt = 8; kt >= 1; kt >>= 1)
+    if (FilterTileSmem::bytes(S, R, kt, tsize) <= 100 * 1024) return kt;
+  return 1;
+}
+
+bool filter_kt_valid(int kt, int S, int R, size_t tsize) {
+  if (kt == 0) return S <= 8;
+  if (kt != 1 && kt != 2 && kt != 4 && kt != 8 && kt != 16) return false;
+  return FilterTileSmem::bytes(S, R, kt, tsize) <= 220 * 1024;
+}
+
+template <typename T, int KT>
+static int launch_tiled(const MeshDev& g, const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp,
+                        const Tables* tab, const float* deconv, int spme, typename Cplx<T>::type* sp, double* part,
+                        int* n_blocks, cudaStream_t s) {
+  const size_t smem = FilterTileSmem::bytes(mg.S, mg.R, KT, sizeof(T));
+  // per instantiation, once (outside any stream capture in practice: the first call is eager):
+  // allow the device's whole opt-in shared memory minus the kernel's static part
+  static int allowed = -1;
+  if (allowed < 0) {
+    int dev = 0, optin = 0;
+    cudaFuncAttributes fa{};
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
+        cudaFuncGetAttributes(&fa, k_filter_tiled<T, KT>) != cudaSuccess ||
+        cudaFuncSetAttribute(k_filter_tiled<T, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             optin - (int)fa.sharedSizeBytes) != cudaSuccess) {
+      set_error("filter", "could not raise the shared-memory limit of the tiled filter");
+      return FD3_ECUDA;
+    }
+    allowed = optin - (int)fa.sharedSizeBytes;
+  }
+  if (smem > (size_t)allowed) {
+    set_error("filter", "shared-memory tile too large for this device; choose a smaller filter k-tile");
+    return FD3_EINVAL;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_filter_tiled<T, KT>, kFilterThreads, smem) !=
+          cudaSuccess || per_sm < 1)
+    per_sm = 1;
   const size_t Mh = (size_t)mg.n[0] * mg.n[1] * mg.nzh;
-  const int blocks = filter_grid(Mh);
-  *n_blocks = blocks;
-  const MeshDev g = to_dev(mg);
-  C2* sp = reinterpret_cast<C2*>(spec);
-#define FD3_FILTER(SS, RR) \
-  k_filter<T, SS, RR><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gp, tab, deconv, sp, part)
-  if (mg.S <= 1)
-    FD3_FILTER(1, 4);
-  else if (mg.S <= 2 && mg.R <= 4)
-    FD3_FILTER(2, 4);
-  else if (mg.S <= 2)
-    FD3_FILTER(2, 2);
-  else if (mg.S <= 4 && mg.R <= 4)
-    FD3_FILTER(4, 4);
-  else if (mg.S <= 4)
-    FD3_FILTER(4, 2);
-  else if (mg.S <= 8)
-    FD3_FILTER(8, 1);
-  else
-    k_filter_any<T><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gp, tab, deconv, sp,
-                                                      reinterpret_cast<C2*>(spec_out), part);
-#undef FD3_FILTER
+  const size_t ntile = (Mh + KT - 1) / KT;
+  size_t blocks = (size_t)device_sms() * per_sm;
+  if (blocks > ntile) blocks = ntile;
+  if (blocks > (size_t)filter_max_blocks()) blocks = filter_max_blocks();
+  *n_blocks = (int)blocks;
+  k_filter_tiled<T, KT><<<(int)blocks, kFilterThreads, smem, s>>>(g, mg.order, spme, ci, gp, tab, deconv, sp, part);
   FD3_LAUNCHED();
   return FD3_OK;
 }
+
+template <typename T>
+int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab,
+                  const float* deconv, int spme, void* spec, double* part, int* n_blocks, cudaStream_t s) {
+  using C2 = typename Cplx<T>::type;
+  const size_t Mh = (size_t)mg.n[0] * mg.n[1] * mg.nzh;
+  const MeshDev g = to_dev(mg);
+  C2* sp = reinterpret_cast<C2*>(spec);
+  const int kt = mg.filter_kt >= 0 ? mg.filter_kt : filter_default_kt(mg.S, mg.R, sizeof(T));
+  if (kt == 0 && mg.S <= 8) {
+    const int blocks = filter_grid(Mh);
+    *n_blocks = blocks;
+#define FD3_FILTER(SS, RR) \
+  k_filter<T, SS, RR><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gp, tab, deconv, sp, part)
+    if (mg.S <= 1)
+      FD3_FILTER(1, 4);
+    else if (mg.S <= 2 && mg.R <= 4)
+      FD3_FILTER(2, 4);
+    else if (mg.S <= 2)
+      FD3_FILTER(2, 2);
+    else if (mg.S <= 4 && mg.R <= 4)
+      FD3_FILTER(4, 4);
+    else if (mg.S <= 4)
+      FD3_FILTER(4, 2);
+    else
+      FD3_FILTER(8, 1);
+#undef FD3_FILTER
+    FD3_LAUNCHED();
+    return FD3_OK;
+  }
+  switch (kt) {
+    case 16: return launch_tiled<T, 16>(g, mg, ci, gp, tab, deconv, spme, sp, part, n_blocks, s);
+    case 8: return launch_tiled<T, 8>(g, mg, ci, gp, tab, deconv, spme, sp, part, n_blocks, s);
+    case 4: return launch_tiled<T, 4>(g, mg, ci, gp, tab, deconv, spme, sp, part, n_blocks, s);
+    case 2: return launch_tiled<T, 2>(g, mg, ci, gp, tab, deconv, spme, sp, part, n_blocks, s);
+    default: return launch_tiled<T, 1>(g, mg, ci, gp, tab, deconv, spme, sp, part, n_blocks, s);
+  }
+}
 template int launch_filter<double>(const MeshGeom&, const CellInfo*, const GreenPair*, const Tables*, const float*,
-                                   int, void*, void*, double*, int*, cudaStream_t);
+                                   int, void*, double*, int*, cudaStream_t);
 template int launch_filter<float>(const MeshGeom&, const CellInfo*, const GreenPair*, const Tables*, const float*,
-                                  int, void*, void*, double*, int*, cudaStream_t);
+                                  int, void*, double*, int*, cudaStream_t);
 
 // ------------------------------------------------------------------ finalize
 // mode 0: energy [Hartree] and dE/dcell [Hartree/Bohr] with positions/shifts fixed (edge path)

@@ -161,6 +161,18 @@ class Engine:
         _native.check(_native.lib().fd3_cell_grid(_native.dptr(c), float(r_cut_ang), nb, rr), "fd3_cell_grid")
         return tuple(nb), tuple(rr)
 
+    def set_tuning(self, filter_kt: Optional[int] = None) -> None:
+        """Launch-shape knobs (results agree to rounding): ``filter_kt`` = k-points per filter tile."""
+        if filter_kt is not None:
+            _native.check(_native.lib().fd3_plan_set_tuning(self._plan, _native.TUNE_FILTER_KT, int(filter_kt)),
+                          "fd3_plan_set_tuning")
+
+    def tuning(self) -> dict:
+        v = ctypes.c_int32()
+        _native.check(_native.lib().fd3_plan_get_tuning(self._plan, _native.TUNE_FILTER_KT, ctypes.byref(v)),
+                      "fd3_plan_get_tuning")
+        return {"filter_kt": int(v.value)}
+
     def profile(self, on: bool = True) -> None:
         """Record CUDA events between pipeline stages of the following calls."""
         _native.check(_native.lib().fd3_profile_enable(self._plan, 1 if on else 0), "fd3_profile_enable")

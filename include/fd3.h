@@ -77,6 +77,18 @@ typedef struct {
 FD3_API int fd3_plan_create(const fd3_plan_desc* desc, fd3_plan** out);
 FD3_API int fd3_plan_destroy(fd3_plan* plan);
 
+/* Launch-shape knobs an autotuner may set per plan (no reference counterpart: the
+ * reference's torch ops choose their own launches). They change only how the work is
+ * mapped onto the GPU; results agree with the defaults to rounding (a different
+ * summation order), and every value is checked against the plan's sizes.
+ *   FD3_TUNE_FILTER_KT  k-points per shared-memory tile of the reciprocal-space filter:
+ *                       0 = per-thread register kernel (at most 8 species), 1, 2, 4, 8
+ *                       or 16 = tiled kernel, -1 = the default for (species, rank).
+ * fd3_plan_get_tuning returns the value in effect (the default resolved). */
+#define FD3_TUNE_FILTER_KT 0
+FD3_API int fd3_plan_set_tuning(fd3_plan* plan, int32_t knob, int32_t value);
+FD3_API int fd3_plan_get_tuning(const fd3_plan* plan, int32_t knob, int32_t* value);
+
 /* Workspace bytes for a call with n_atoms atoms. n_bins: cell-list bins of the
  * fused path (0 for the edge path; see fd3_cell_grid). */
 FD3_API int fd3_workspace_size(const fd3_plan* plan, int64_t n_atoms, int64_t n_bins, size_t* bytes);

@@ -1,0 +1,63 @@
+"""GPU checks of the launch-shape knobs: every filter k-tile width (and the per-thread register
+kernel where it applies) gives the same energy, forces and stress to rounding, for many-species
+and few-species boxes, in float64 and in the mixed form."""
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+KW = dict(method="spme", mesh_spacing=1.2, interpolation_nodes=5, c6tol=1.0, r_cut=6.0)
+
+
+@pytest.mark.parametrize("precision,z_max,n", [("fp64", 54, 160), ("mixed", 54, 160), ("fp64", 8, 120),
+                                               ("mixed", 8, 120)])
+def test_filter_tiles_agree(precision, z_max, n, cuda_device):
+    from fourierd3_b200 import D3Model, structures as st
+
+    pos, cell, z = st.random_box(41, n, z_max=z_max)
+    m = D3Model(z, cell, precision=precision, device=cuda_device, **KW)
+    e0, f0, s0 = (t.clone() for t in m(pos, cell))
+    tol_e = 1e-12 if precision == "fp64" else 2e-6
+    tol_f = 1e-10 if precision == "fp64" else 1e-5
+    tried = []
+    for kt in (0, 1, 2, 4, 8, 16):
+        try:
+            m.engine.set_tuning(filter_kt=kt)
+        except ValueError:
+            # the register kernel takes at most 8 species; wide float64 tiles outgrow shared memory
+            assert (kt == 0 and len(np.unique(z)) > 8) or (kt >= 8 and precision == "fp64")
+            continue
+        assert m.engine.tuning()["filter_kt"] == kt
+        e, f, s = m(pos, cell)
+        assert abs(float(e) - float(e0)) <= tol_e * abs(float(e0)), (kt, float(e), float(e0))
+        assert (f - f0).abs().max().item() <= tol_f, kt
+        assert (s - s0).abs().max().item() <= tol_f, kt
+        tried.append(kt)
+    assert len(tried) >= 3
+
+
+def test_bad_tile_rejected(cuda_device):
+    from fourierd3_b200 import D3Model, structures as st
+
+    pos, cell, z = st.random_box(42, 60, z_max=54)
+    m = D3Model(z, cell, precision="mixed", device=cuda_device, **KW)
+    with pytest.raises(ValueError):
+        m.engine.set_tuning(filter_kt=3)
+    with pytest.raises(ValueError):
+        m.engine.set_tuning(filter_kt=0)    # register kernel: at most 8 species
+
+
+def test_autotune_filter_sets_a_valid_tile(cuda_device):
+    from fourierd3_b200.batch import D3Batch, autotune_filter
+    from fourierd3_b200 import structures as st
+
+    structs = [st.random_box(50 + k, 40 + 30 * k, z_max=54 if k % 2 else 6) for k in range(4)]
+    b = D3Batch(structs, precision="mixed", device=cuda_device, **KW)
+    e0 = b()[0].clone()
+    res = autotune_filter(b, reps=1)
+    assert res
+    for c, (best, times) in res.items():
+        assert best in times
+    e1 = b()[0]
+    assert torch.allclose(e0, e1, rtol=2e-6, atol=0)

@@ -18,6 +18,8 @@ struct fd3_plan {
   Tables* d_tab = nullptr;
   double* d_eigvecs = nullptr;
   GreenPair* d_green = nullptr;
+  GreenPairF* d_green_f = nullptr;
+  float4* d_green_f4 = nullptr;   // {R, s6 c6pre, 3 s8 qq c8pre, 0}: folded mixed-form constants
   float* d_deconv = nullptr;
   cufftHandle fwd = 0, inv = 0;
   bool has_fft = false;
@@ -155,18 +157,30 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
         t.selfcont[X] = t.s6 / R6 + 3.0 * t.s8 * g.qq / R8;
       }
     }
+  GreenPairF* gpf = new GreenPairF[S * S];
+  for (int k = 0; k < S * S; ++k)
+    gpf[k] = GreenPairF{(float)gp[k].R, (float)gp[k].qq, (float)gp[k].c6s1, (float)gp[k].c6s2, (float)gp[k].c6pre,
+                        (float)gp[k].c8s1, (float)gp[k].c8s2, (float)gp[k].c8pre};
+  float4* gf4 = new float4[S * S];
+  for (int k = 0; k < S * S; ++k)
+    gf4[k] = make_float4((float)gp[k].R, (float)(t.s6 * gp[k].c6pre), (float)(3.0 * t.s8 * gp[k].qq * gp[k].c8pre),
+                         0.f);
   int rc = FD3_OK;
   do {
     if (cudaMalloc(&p->d_tab, sizeof(Tables)) != cudaSuccess ||
         cudaMalloc(&p->d_eigvecs, sizeof(double) * S * 7 * R) != cudaSuccess ||
-        cudaMalloc(&p->d_green, sizeof(GreenPair) * S * S) != cudaSuccess) {
+        cudaMalloc(&p->d_green, sizeof(GreenPair) * S * S) != cudaSuccess ||
+        cudaMalloc(&p->d_green_f, sizeof(GreenPairF) * S * S) != cudaSuccess ||
+        cudaMalloc(&p->d_green_f4, sizeof(float4) * S * S) != cudaSuccess) {
       set_error("fd3_plan_create", "cudaMalloc of the species tables failed");
       rc = FD3_ECUDA;
       break;
     }
     if (cudaMemcpy(p->d_tab, &t, sizeof(Tables), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(p->d_eigvecs, d->eigvecs, sizeof(double) * S * 7 * R, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(p->d_green, gp, sizeof(GreenPair) * S * S, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaMemcpy(p->d_green, gp, sizeof(GreenPair) * S * S, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(p->d_green_f, gpf, sizeof(GreenPairF) * S * S, cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(p->d_green_f4, gf4, sizeof(float4) * S * S, cudaMemcpyHostToDevice) != cudaSuccess) {
       set_error("fd3_plan_create", "upload of the species tables failed");
       rc = FD3_ECUDA;
       break;
@@ -222,6 +236,8 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
     }
   } while (0);
   delete[] gp;
+  delete[] gpf;
+  delete[] gf4;
   if (rc) {
     fd3_plan_destroy(p);
     return rc;
@@ -268,6 +284,8 @@ extern "C" int fd3_plan_destroy(fd3_plan* p) {
   cudaFree(p->d_tab);
   cudaFree(p->d_eigvecs);
   cudaFree(p->d_green);
+  cudaFree(p->d_green_f);
+  cudaFree(p->d_green_f4);
   cudaFree(p->d_deconv);
   delete p;
   return FD3_OK;
@@ -427,7 +445,7 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
     FD3_CUFFT(cufftExecR2C(p->fwd, (cufftReal*)w.rho, (cufftComplex*)w.spec));
   prof_mark(p, s, "fft_r2c");
   void* hspec = w.spec;   // the filter overwrites the spectrum with H in place
-  FD3_TRY(launch_filter<T>(mg, w.ci, p->d_green, p->d_tab, p->d_deconv, p->method == FD3_METHOD_SPME, w.spec,
+  FD3_TRY(launch_filter<T>(mg, w.ci, p->d_green, p->d_green_f, p->d_green_f4, p->d_tab, p->d_deconv, p->method == FD3_METHOD_SPME, w.spec,
                            w.kspc_part, n_kspc, s));
   prof_mark(p, s, "filter");
   *n_mcell = 0;

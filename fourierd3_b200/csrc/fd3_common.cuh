@@ -30,6 +30,12 @@ struct CellInfo {
 struct GreenPair {
   double R, qq, c6s1, c6s2, c6pre, c8s1, c8s2, c8pre;
 };
+// The same constants rounded to float once, for the mixed-form filter (no per-use conversion).
+struct GreenPairF {
+  float R, qq, c6s1, c6s2, c6pre, c8s1, c8s2, c8pre;
+};
+template <typename T> struct GreenPairOf { using type = GreenPair; };
+template <> struct GreenPairOf<float> { using type = GreenPairF; };
 
 // Device-resident per-plan tables (uploaded once by fd3_plan_create).
 struct Tables {
@@ -119,7 +125,33 @@ __device__ __forceinline__ double exp_t(double x) { return exp(x); }
 __device__ __forceinline__ float exp_t(float x) { return __expf(x); }
 __device__ __forceinline__ double rcp_t(double x) { return 1.0 / x; }
 __device__ __forceinline__ void sincospi_t(double x, double* s, double* c) { sincospi(x, s, c); }
-__device__ __forceinline__ void sincospi_t(float x, float* s, float* c) { sincospif(x, s, c); }
+// sin(pi x) and cos(pi x) in float for the mixed form. Exact reduction by quarter turns,
+// x = n/2 + f with n = rint(2x) and |f| <= 1/4 (f is exact: Sterbenz), then the Taylor series of
+// sin(pi f) to f^9 and of cos(pi f) to f^10 (truncation below 2e-9 on |f| <= 1/4; coefficients
+// (-1)^k pi^(2k+1)/(2k+1)! and (-1)^k pi^(2k)/(2k)! rounded to float), and the rotation by the
+// quadrant n mod 4. Valid for |x| < 2^22; measured error below 1 ulp of 1.
+__device__ __forceinline__ void sincospi_t(float x, float* s, float* c) {
+  const float n = rintf(2.0f * x);
+  const float f = fmaf(-0.5f, n, x);
+  const float f2 = f * f;
+  float ps = 0.08214588463306427f;
+  ps = fmaf(ps, f2, -0.5992645025253296f);
+  ps = fmaf(ps, f2, 2.550163984298706f);
+  ps = fmaf(ps, f2, -5.167712688446045f);
+  ps = fmaf(ps, f2, 3.1415927410125732f);
+  const float sv = ps * f;
+  float pc = -0.025806890800595284f;
+  pc = fmaf(pc, f2, 0.23533062636852264f);
+  pc = fmaf(pc, f2, -1.3352627754211426f);
+  pc = fmaf(pc, f2, 4.058712005615234f);
+  pc = fmaf(pc, f2, -4.934802055358887f);
+  const float cv = fmaf(pc, f2, 1.0f);
+  const int q = ((int)n) & 3;
+  const float so = (q & 1) ? cv : sv;
+  const float co = (q & 1) ? sv : cv;
+  *s = (q & 2) ? -so : so;
+  *c = ((q + 1) & 2) ? -co : co;
+}
 __device__ __forceinline__ float rcp_t(float x) { return __frcp_rn(x); }
 
 // The same CN edge function from the squared distance r2 > 1e-12 Bohr^2 (the reference zeroes
@@ -199,8 +231,8 @@ __device__ __forceinline__ void lagrange(T x, T* w, T* dw) {
 }
 
 // Green's function G_XY(k) and dG/dk for one species pair (pair_pot.py:142-178).
-template <typename T>
-__device__ __forceinline__ void green_eval(const GreenPair& g, T k, T s6, T s8, T& G, T& dG) {
+template <typename T, typename GP>
+__device__ __forceinline__ void green_eval(const GP& g, T k, T s6, T s8, T& G, T& dG) {
   const T R = T(g.R);
   const T ksq = k * k;
   if (k * R < T(1e-15)) {
@@ -238,6 +270,31 @@ __device__ __forceinline__ void green_eval(const GreenPair& g, T k, T s6, T s8, 
   const T d8 = T(3) * s8 * T(g.c8pre) * (R * dn8 * invk - n8 * invk * invk);
   G = f6 + T(g.qq) * f8;
   dG = d6 + T(g.qq) * d8;
+}
+
+// Mixed-form Green's function for the tiled filter: the same closed form as green_eval with the
+// pair constants folded, g = {R, A6 = s6 c6pre, A8 = 3 s8 qq c8pre, unused}, and 1/k given.
+//   G = (A6 n6(u) + A8 n8(u)) / k,   dG/dk = (R (A6 n6'(u) + A8 n8'(u)) - G) / k,   u = k R,
+// which is f6 + qq f8 and d6 + qq d8 of green_eval regrouped. The k R < 1e-15 (Taylor) branch is
+// left to green_eval on the full constants.
+__device__ __forceinline__ void green_eval_folded(float4 g, float k, float invk, float& G, float& dG) {
+  const float R = g.x, A6 = g.y, A8 = g.z;
+  const float u = k * R;
+  const float e2 = __expf(-u * 0.5f);
+  const float e1 = e2 * e2;
+  float sa, ca;
+  sincospi_t(1.0f / 3.0f + u * 0.27566444771089604f, &sa, &ca);
+  const float n6 = e1 - 2.0f * e2 * ca;
+  const float dn6 = -e1 + e2 * ca + 1.7320508075688772935f * e2 * sa;
+  const float e3 = __expf(-u * 0.38268343236508977173f);
+  const float e4 = __expf(-u * 0.92387953251128675613f);
+  float s1, c1, s2, c2;
+  sincospi_t(0.25f + u * 0.29407998884120140f, &s1, &c1);
+  sincospi_t(0.75f + u * 0.12181191980055409f, &s2, &c2);
+  const float n8 = e3 * c1 + e4 * c2;
+  const float dn8 = -0.38268343236508977173f * (e3 * c1 + e4 * s2) - 0.92387953251128675613f * (e3 * s1 + e4 * c2);
+  G = invk * (A6 * n6 + A8 * n8);
+  dG = invk * (R * (A6 * dn6 + A8 * dn8) - G);
 }
 
 // Division of 32-bit unsigned values by a runtime-invariant divisor (round-up multiplier method):

@@ -128,8 +128,9 @@ int launch_spread(const MeshGeom& mg, int n, const double* pos, double pos_scale
                   const double* c6, const CellInfo* ci, const int* key_start, const int* order,
                   const MeshRecords& rec, T* rho, cudaStream_t s);
 template <typename T>
-int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab,
-                  const float* deconv, int spme, void* spec, double* part, int* n_blocks, cudaStream_t s);
+int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const GreenPairF* gpf,
+                  const float4* g4, const Tables* tab, const float* deconv, int spme, void* spec, double* part,
+                  int* n_blocks, cudaStream_t s);
 int filter_max_blocks();
 int filter_default_kt(int S, int R, size_t tsize);
 bool filter_kt_valid(int kt, int S, int R, size_t tsize);

@@ -170,7 +170,7 @@ __device__ __forceinline__ void virial_acc(const KPoint<T>& q, T dq, double* acc
 template <typename T, int MAXS, int MAXR>
 __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int spme,
                                                            const CellInfo* __restrict__ ci,
-                                                           const GreenPair* __restrict__ gp,
+                                                           const typename GreenPairOf<T>::type* __restrict__ gp,
                                                            const Tables* __restrict__ tab,
                                                            const float* __restrict__ deconv,
                                                            typename Cplx<T>::type* __restrict__ spec,
@@ -249,32 +249,40 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int
 
 // Many species (<= 64), any rank: k-tiled filter. One CTA takes KT consecutive rfft k-points at a
 // time and stages their S*R spectrum values in shared memory (one coalesced read of the tile).
-//   phase B: the S(S+1)/2 species pairs X <= Y are spread over the CTA's 256/KT thread slots,
-//            each thread keeping one k column: G_XY, dG_XY (and the conjugate-partner average on
-//            the self-conjugate planes) are evaluated ONCE per pair and k, the pair's share of
-//            the energy and virial  w_XY G_XY sum_r lambda_r Re(S_Xr S_Yr*)  (w = 1 on the
-//            diagonal, 2 off it) is accumulated, and the Hermitian-averaged G is kept in
-//            shared memory;
+// Each thread keeps one k column of the tile (kk = thread % KT) and one of 256/KT slots.
+//   phase B: the species pairs X <= Y are grouped in units (X, Y0..Y0+3), ordered by Y0 then X,
+//            so that the slots of one warp share their Y rows (broadcast shared-memory reads)
+//            and each keeps lambda_r S_Xr in registers for the unit. Per pair and k: G_XY, dG_XY
+//            (and the conjugate-partner average on the self-conjugate planes) are evaluated ONCE,
+//            the pair's share w_XY G_XY sum_r lambda_r Re(S_Xr S_Yr*) of the energy and virial
+//            is accumulated (w = 1 on the diagonal, 2 off it), and the Hermitian-averaged G is
+//            kept in shared memory;
 //   phase C: thread (X, k) forms H_Xr = sum_Y Gh_XY S_Yr from shared memory and writes it over
 //            the spectrum tile it came from (in place: no other CTA reads these k columns).
-// Green evaluations per k fall from S^2 to S(S+1)/2 and the spectrum is read from HBM once,
-// instead of once per X from L2.
+// Green evaluations per k fall from S^2 to S(S+1)/2 and the spectrum is read from HBM once.
+constexpr int kUnitY = 4;
+static int filter_units(int S) {
+  int n = 0;
+  for (int y0 = 0; y0 < S; y0 += kUnitY) n += (y0 + kUnitY < S ? y0 + kUnitY : S);
+  return n;
+}
 struct FilterTileSmem {
   static size_t bytes(int S, int R, int kt, size_t tsize) {
     const size_t C = (size_t)S * R, np = (size_t)S * (S + 1) / 2;
-    size_t b = C * kt * 2 * tsize;              // spectrum tile
-    b += 32 * tsize;                            // lambda_r
-    b += np * kt * tsize;                       // Gh tile
-    b += np * sizeof(uint32_t);                 // pair -> (X, Y)
-    b += (size_t)S * sizeof(int);               // first pair index of row X
+    size_t b = C * kt * 2 * tsize;                  // spectrum tile
+    b += 32 * tsize;                                // lambda_r
+    b += np * kt * tsize;                           // Gh tile
+    b += (size_t)filter_units(S) * sizeof(uint32_t); // units (X, Y0)
+    b += (size_t)S * sizeof(int);                   // first pair index of row X
     return (b + 15) & ~(size_t)15;
   }
 };
 
 template <typename T, int KT>
-__global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int P, int spme,
+__global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int P, int spme, int n_units,
                                                                  const CellInfo* __restrict__ ci,
-                                                                 const GreenPair* __restrict__ gp,
+                                                                 const typename GreenPairOf<T>::type* __restrict__ gp,
+                                                                 const float4* __restrict__ g4,
                                                                  const Tables* __restrict__ tab,
                                                                  const float* __restrict__ deconv,
                                                                  typename Cplx<T>::type* __restrict__ spec,
@@ -287,12 +295,17 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
   C2* ss = reinterpret_cast<C2*>(smem_raw);                  // [C][KT]
   T* lam = reinterpret_cast<T*>(ss + (size_t)C * KT);        // [32]
   T* gs = lam + 32;                                          // [NP][KT]
-  uint32_t* pxy = reinterpret_cast<uint32_t*>(gs + (size_t)NP * KT);
-  int* row0 = reinterpret_cast<int*>(pxy + NP);
+  uint32_t* units = reinterpret_cast<uint32_t*>(gs + (size_t)NP * KT);
+  int* row0 = reinterpret_cast<int*>(units + n_units);
   for (int X = threadIdx.x; X < S; X += blockDim.x) row0[X] = X * S - X * (X - 1) / 2;
-  for (int X = 0; X < S; ++X)
-    for (int Y = X + threadIdx.x; Y < S; Y += blockDim.x) pxy[X * S - X * (X - 1) / 2 + (Y - X)] = (X << 16) | Y;
-  for (int r = threadIdx.x; r < R; r += blockDim.x) lam[r] = (T)tab->eigs[r];
+  if (threadIdx.x == 0) {
+    int u = 0;
+    for (int y0 = 0; y0 < S; y0 += kUnitY) {
+      const int xe = y0 + kUnitY < S ? y0 + kUnitY : S;
+      for (int X = 0; X < xe; ++X) units[u++] = ((uint32_t)X << 16) | (uint32_t)y0;
+    }
+  }
+  for (int r = threadIdx.x; r < 32; r += blockDim.x) lam[r] = r < R ? (T)tab->eigs[r] : T(0);
   const size_t Mh = (size_t)g.n[0] * g.n[1] * g.nzh;
   const size_t ntile = (Mh + KT - 1) / KT;
   const int kk = threadIdx.x % KT, slot = threadIdx.x / KT;
@@ -311,32 +324,84 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
     const size_t k = k0 + kk;
     const bool valid = k < Mh;
     const KPoint<T> q = kpoint<T>(g, valid ? k : 0, rc, deconv, spme, P);
+    const T invk = q.knorm > T(0) ? T(1) / q.knorm : T(0);
+    const T invkp = q.kpart > T(0) ? T(1) / q.kpart : T(0);
     __syncthreads();
     T qq = T(0), dq = T(0);
-    for (int pi = slot; pi < NP; pi += NSLOT) {
-      const uint32_t xy = pxy[pi];
-      const int X = (int)(xy >> 16), Y = (int)(xy & 0xffffu);
-      T gv, dv;
-      green_eval<T>(gp[X * S + Y], q.knorm, s6, s8, gv, dv);
-      gv *= q.inv_sc;
-      dv *= q.inv_sc;
-      T gh = gv;
-      if (q.partner) {
-        T gpv, dpv;
-        green_eval<T>(gp[X * S + Y], q.kpart, s6, s8, gpv, dpv);
-        gh = T(0.5) * (gv + gpv * q.inv_sc);
+    for (int u = slot; u < n_units; u += NSLOT) {
+      const uint32_t xy = units[u];
+      const int X = (int)(xy >> 16), Y0 = (int)(xy & 0xffffu);
+      const int ya = X > Y0 ? X : Y0;
+      const int yb = Y0 + kUnitY < S ? Y0 + kUnitY : S;
+      // mixed form: the unit's folded pair constants are requested before the rank loop
+      float4 gq[kUnitY];
+      if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int y = 0; y < kUnitY; ++y) gq[y] = Y0 + y < yb ? g4[X * S + Y0 + y] : make_float4(0.f, 0.f, 0.f, 0.f);
       }
-      const C2* sx = ss + (size_t)X * R * KT + kk;
-      const C2* sy = ss + (size_t)Y * R * KT + kk;
-      T pr = T(0);
-      for (int r = 0; r < R; ++r) {
-        const C2 a = sx[r * KT], b = sy[r * KT];
-        pr += lam[r] * (a.x * b.x + a.y * b.y);
+      T pr[kUnitY];
+#pragma unroll
+      for (int y = 0; y < kUnitY; ++y) pr[y] = T(0);
+      for (int r0 = 0; r0 < R; r0 += 8) {
+        C2 xl[8];
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+          if (r0 + r < R) {
+            const C2 a = ss[((size_t)X * R + r0 + r) * KT + kk];
+            const T l = lam[r0 + r];
+            xl[r] = C2{l * a.x, l * a.y};
+          } else {
+            xl[r] = C2{T(0), T(0)};
+          }
+        }
+#pragma unroll
+        for (int y = 0; y < kUnitY; ++y) {
+          const int Y = Y0 + y;
+          if (Y >= ya && Y < yb) {
+            const C2* sy = ss + ((size_t)Y * R + r0) * KT + kk;
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+              if (r0 + r < R) {
+                const C2 b = sy[r * KT];
+                pr[y] += xl[r].x * b.x + xl[r].y * b.y;
+              }
+          }
+        }
       }
-      const T w = X == Y ? T(1) : T(2);
-      qq += w * gv * pr;
-      dq += w * dv * pr;
-      gs[pi * KT + kk] = gh;
+#pragma unroll
+      for (int y = 0; y < kUnitY; ++y) {
+        const int Y = Y0 + y;
+        if (Y >= ya && Y < yb) {
+          T gv, dv;
+          if constexpr (sizeof(T) == 4) {
+            if (q.knorm * gq[y].x < 1e-15f)
+              green_eval<T>(gp[X * S + Y], q.knorm, s6, s8, gv, dv);
+            else
+              green_eval_folded(gq[y], q.knorm, invk, gv, dv);
+          } else {
+            green_eval<T>(gp[X * S + Y], q.knorm, s6, s8, gv, dv);
+          }
+          gv *= q.inv_sc;
+          dv *= q.inv_sc;
+          T gh = gv;
+          if (q.partner) {
+            T gpv, dpv;
+            if constexpr (sizeof(T) == 4) {
+              if (q.kpart * gq[y].x < 1e-15f)
+                green_eval<T>(gp[X * S + Y], q.kpart, s6, s8, gpv, dpv);
+              else
+                green_eval_folded(gq[y], q.kpart, invkp, gpv, dpv);
+            } else {
+              green_eval<T>(gp[X * S + Y], q.kpart, s6, s8, gpv, dpv);
+            }
+            gh = T(0.5) * (gv + gpv * q.inv_sc);
+          }
+          const T w = X == Y ? T(1) : T(2);
+          qq += w * gv * pr[y];
+          dq += w * dv * pr[y];
+          gs[(row0[X] + (Y - X)) * KT + kk] = gh;
+        }
+      }
     }
     if (valid) {
       acc[0] += (double)(q.wk * qq);
@@ -348,8 +413,9 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
         C2 h[8];
 #pragma unroll
         for (int r = 0; r < 8; ++r) h[r] = C2{T(0), T(0)};
+        // Y < X: pair index row0[Y] + (X - Y); Y >= X: row0[X] + (Y - X), contiguous
         for (int Y = 0; Y < S; ++Y) {
-          const int pi = X <= Y ? row0[X] + (Y - X) : row0[Y] + (X - Y);
+          const int pi = Y < X ? row0[Y] + (X - Y) : row0[X] + (Y - X);
           const T gh = gs[pi * KT + kk];
           const C2* sy = ss + ((size_t)Y * R + r0) * KT + kk;
 #pragma unroll
@@ -404,9 +470,10 @@ bool filter_kt_valid(int kt, int S, int R, size_t tsize) {
 }
 
 template <typename T, int KT>
-static int launch_tiled(const MeshDev& g, const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp,
-                        const Tables* tab, const float* deconv, int spme, typename Cplx<T>::type* sp, double* part,
-                        int* n_blocks, cudaStream_t s) {
+static int launch_tiled(const MeshDev& g, const MeshGeom& mg, const CellInfo* ci,
+                        const typename GreenPairOf<T>::type* gp, const float4* g4, const Tables* tab,
+                        const float* deconv, int spme, typename Cplx<T>::type* sp, double* part, int* n_blocks,
+                        cudaStream_t s) {
   const size_t smem = FilterTileSmem::bytes(mg.S, mg.R, KT, sizeof(T));
   // per instantiation, once (outside any stream capture in practice: the first call is eager):
   // allow the device's whole opt-in shared memory minus the kernel's static part
@@ -438,15 +505,19 @@ static int launch_tiled(const MeshDev& g, const MeshGeom& mg, const CellInfo* ci
   if (blocks > ntile) blocks = ntile;
   if (blocks > (size_t)filter_max_blocks()) blocks = filter_max_blocks();
   *n_blocks = (int)blocks;
-  k_filter_tiled<T, KT><<<(int)blocks, kFilterThreads, smem, s>>>(g, mg.order, spme, ci, gp, tab, deconv, sp, part);
+  k_filter_tiled<T, KT><<<(int)blocks, kFilterThreads, smem, s>>>(g, mg.order, spme, filter_units(mg.S), ci, gp,
+                                                                  g4, tab, deconv, sp, part);
   FD3_LAUNCHED();
   return FD3_OK;
 }
 
 template <typename T>
-int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab,
-                  const float* deconv, int spme, void* spec, double* part, int* n_blocks, cudaStream_t s) {
+int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const GreenPairF* gpf,
+                  const float4* g4, const Tables* tab, const float* deconv, int spme, void* spec, double* part,
+                  int* n_blocks, cudaStream_t s) {
   using C2 = typename Cplx<T>::type;
+  using GP = typename GreenPairOf<T>::type;
+  const GP* gpt = reinterpret_cast<const GP*>(sizeof(T) == 8 ? (const void*)gp : (const void*)gpf);
   const size_t Mh = (size_t)mg.n[0] * mg.n[1] * mg.nzh;
   const MeshDev g = to_dev(mg);
   C2* sp = reinterpret_cast<C2*>(spec);
@@ -455,7 +526,7 @@ int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, c
     const int blocks = filter_grid(Mh);
     *n_blocks = blocks;
 #define FD3_FILTER(SS, RR) \
-  k_filter<T, SS, RR><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gp, tab, deconv, sp, part)
+  k_filter<T, SS, RR><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gpt, tab, deconv, sp, part)
     if (mg.S <= 1)
       FD3_FILTER(1, 4);
     else if (mg.S <= 2 && mg.R <= 4)
@@ -473,17 +544,19 @@ int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, c
     return FD3_OK;
   }
   switch (kt) {
-    case 16: return launch_tiled<T, 16>(g, mg, ci, gp, tab, deconv, spme, sp, part, n_blocks, s);
-    case 8: return launch_tiled<T, 8>(g, mg, ci, gp, tab, deconv, spme, sp, part, n_blocks, s);
-    case 4: return launch_tiled<T, 4>(g, mg, ci, gp, tab, deconv, spme, sp, part, n_blocks, s);
-    case 2: return launch_tiled<T, 2>(g, mg, ci, gp, tab, deconv, spme, sp, part, n_blocks, s);
-    default: return launch_tiled<T, 1>(g, mg, ci, gp, tab, deconv, spme, sp, part, n_blocks, s);
+    case 16: return launch_tiled<T, 16>(g, mg, ci, gpt, g4, tab, deconv, spme, sp, part, n_blocks, s);
+    case 8: return launch_tiled<T, 8>(g, mg, ci, gpt, g4, tab, deconv, spme, sp, part, n_blocks, s);
+    case 4: return launch_tiled<T, 4>(g, mg, ci, gpt, g4, tab, deconv, spme, sp, part, n_blocks, s);
+    case 2: return launch_tiled<T, 2>(g, mg, ci, gpt, g4, tab, deconv, spme, sp, part, n_blocks, s);
+    default: return launch_tiled<T, 1>(g, mg, ci, gpt, g4, tab, deconv, spme, sp, part, n_blocks, s);
   }
 }
-template int launch_filter<double>(const MeshGeom&, const CellInfo*, const GreenPair*, const Tables*, const float*,
-                                   int, void*, double*, int*, cudaStream_t);
-template int launch_filter<float>(const MeshGeom&, const CellInfo*, const GreenPair*, const Tables*, const float*,
-                                  int, void*, double*, int*, cudaStream_t);
+template int launch_filter<double>(const MeshGeom&, const CellInfo*, const GreenPair*, const GreenPairF*,
+                                   const float4*, const Tables*, const float*, int, void*, double*, int*,
+                                   cudaStream_t);
+template int launch_filter<float>(const MeshGeom&, const CellInfo*, const GreenPair*, const GreenPairF*,
+                                  const float4*, const Tables*, const float*, int, void*, double*, int*,
+                                  cudaStream_t);
 
 // ------------------------------------------------------------------ finalize
 // mode 0: energy [Hartree] and dE/dcell [Hartree/Bohr] with positions/shifts fixed (edge path)

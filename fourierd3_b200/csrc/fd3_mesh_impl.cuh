@@ -12,6 +12,8 @@
 //           adjoint and the spline-gradient force.
 #include <math.h>
 
+#include <type_traits>
+
 #pragma once
 #include "fd3_internal.h"
 
@@ -439,6 +441,159 @@ __global__ void __launch_bounds__(32 * kGatherWarps) k_gather(MeshDev g, int n, 
   if (mcell_part) block_sum_store<9>(mc, mcell_part + 9 * blockIdx.x);
 }
 
+// Fused-path gather, z-run form: lanes over the (x, y) stencil columns; each lane reads the P
+// z-values of its column from every rank channel with aligned 16-byte vector loads (the column
+// start is rounded down to the vector boundary; a warp-uniform offset O in [0, 16/sizeof(T))
+// selects the run, so every register index stays static) and forms
+//   zr_r = sum_z w_z phi_r,  cp_z = sum_r lambda_r c_r phi_r,  s0 = sum_z w_z cp_z,  s2 = sum_z w'_z cp_z,
+// in T, then accumulates P_r = sum W phi_r and the three spline-gradient sums in float64.
+// A column that wraps the periodic z edge (or a mesh whose nz is not a multiple of the vector
+// width) is read element by element with the offset 0.
+template <typename T, int P, int MAXR, int O, int NE>
+__device__ __forceinline__ void zrun_sums(const T (&v)[MAXR][NE], int R, const T (&wz)[P], const T (&cl)[MAXR],
+                                          T (&zr)[MAXR], T (&cp)[P]) {
+#pragma unroll
+  for (int r = 0; r < MAXR; ++r) {
+    if (r < R) {
+      T a = T(0);
+#pragma unroll
+      for (int kz = 0; kz < P; ++kz) {
+        const T f = v[r][O + kz];
+        a += wz[kz] * f;
+        cp[kz] += cl[r] * f;
+      }
+      zr[r] = a;
+    }
+  }
+}
+
+template <typename T, int P, int MAXR>
+__global__ void __launch_bounds__(32 * kGatherWarps) k_gather_z(MeshDev g, int n, const double* __restrict__ c6,
+                                                                const double* __restrict__ dc6,
+                                                                const CellInfo* __restrict__ ci,
+                                                                const Tables* __restrict__ tab,
+                                                                const int* __restrict__ order,
+                                                                const int4* __restrict__ rb,
+                                                                const T* __restrict__ rw, const T* __restrict__ rdw,
+                                                                const T* __restrict__ phi, double* __restrict__ gcn,
+                                                                double* __restrict__ gpos) {
+  constexpr int VW = 16 / (int)sizeof(T);          // elements per 16-byte vector
+  constexpr int NV = (VW - 1 + P + VW - 1) / VW;   // vectors covering a run at any offset
+  constexpr int NE = NV * VW;
+  using V = typename std::conditional<sizeof(T) == 4, float4, double2>::type;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int t = blockIdx.x * kGatherWarps + wid;
+  if (t >= n) return;
+  const int R = g.R;
+  const int i = order[t];
+  const int4 b4 = rb[t];
+  const int s = b4.w;
+  const T* wr = rw + (size_t)t * 3 * P;
+  const T* dwr = rdw + (size_t)t * 3 * P;
+  T wz[P], dwz[P];
+#pragma unroll
+  for (int k = 0; k < P; ++k) {
+    wz[k] = wr[2 * P + k];
+    dwz[k] = dwr[2 * P + k];
+  }
+  T cl[MAXR];
+#pragma unroll
+  for (int r = 0; r < MAXR; ++r) cl[r] = r < R ? (T)(c6[(size_t)i * R + r] * tab->eigs[r]) : T(0);
+  const int n2 = g.n[2];
+  const int iz0 = b4.z;
+  const bool scalar = iz0 + P > n2 || (n2 % VW) != 0;   // warp-uniform
+  const int o = scalar ? 0 : iz0 % VW;
+  const int za = iz0 - o;
+  const int nvec = (o + P + VW - 1) / VW;
+  const size_t M = (size_t)g.n[0] * g.n[1] * n2;
+  double pr[MAXR];
+#pragma unroll
+  for (int r = 0; r < MAXR; ++r) pr[r] = 0.0;
+  double gu0 = 0.0, gu1 = 0.0, gu2 = 0.0;
+  for (int q = lane; q < P * P; q += 32) {
+    const int kx = q / P, ky = q - kx * P;
+    int ix = b4.x + kx;
+    while (ix >= g.n[0]) ix -= g.n[0];   // a stencil wider than the mesh wraps more than once
+    int iy = b4.y + ky;
+    while (iy >= g.n[1]) iy -= g.n[1];
+    const T wx = wr[kx], dwx = dwr[kx], wy = wr[P + ky], dwy = dwr[P + ky];
+    const T* col = phi + (size_t)s * R * M + ((size_t)ix * g.n[1] + iy) * n2;
+    T v[MAXR][NE];
+#pragma unroll
+    for (int r = 0; r < MAXR; ++r) {
+      if (r < R) {
+        const T* src = col + (size_t)r * M;
+        if (!scalar) {
+          const V* vs = reinterpret_cast<const V*>(src + za);
+#pragma unroll
+          for (int j = 0; j < NV; ++j)
+            if (j < nvec) *reinterpret_cast<V*>(&v[r][j * VW]) = vs[j];
+        } else {
+#pragma unroll
+          for (int kz = 0; kz < P; ++kz) {
+            int iz = iz0 + kz;
+            while (iz >= n2) iz -= n2;
+            v[r][kz] = src[iz];
+          }
+        }
+      }
+    }
+    T zr[MAXR], cp[P];
+#pragma unroll
+    for (int kz = 0; kz < P; ++kz) cp[kz] = T(0);
+#pragma unroll
+    for (int r = 0; r < MAXR; ++r) zr[r] = T(0);
+    if constexpr (VW == 4) {
+      switch (o) {
+        case 0: zrun_sums<T, P, MAXR, 0, NE>(v, R, wz, cl, zr, cp); break;
+        case 1: zrun_sums<T, P, MAXR, 1, NE>(v, R, wz, cl, zr, cp); break;
+        case 2: zrun_sums<T, P, MAXR, 2, NE>(v, R, wz, cl, zr, cp); break;
+        default: zrun_sums<T, P, MAXR, 3, NE>(v, R, wz, cl, zr, cp); break;
+      }
+    } else {
+      if (o == 0)
+        zrun_sums<T, P, MAXR, 0, NE>(v, R, wz, cl, zr, cp);
+      else
+        zrun_sums<T, P, MAXR, 1, NE>(v, R, wz, cl, zr, cp);
+    }
+    T s0 = T(0), s2 = T(0);
+#pragma unroll
+    for (int kz = 0; kz < P; ++kz) {
+      s0 += wz[kz] * cp[kz];
+      s2 += dwz[kz] * cp[kz];
+    }
+    const T wxy = wx * wy;
+#pragma unroll
+    for (int r = 0; r < MAXR; ++r) pr[r] += (double)(wxy * zr[r]);
+    gu0 += (double)(dwx * wy * s0);
+    gu1 += (double)(wx * dwy * s0);
+    gu2 += (double)(wxy * s2);
+  }
+#pragma unroll
+  for (int r = 0; r < MAXR; ++r) pr[r] = warp_sum(pr[r]);
+  gu0 = warp_sum(gu0);
+  gu1 = warp_sum(gu1);
+  gu2 = warp_sum(gu2);
+  if (lane != 0) return;
+  const double inv_vol = 1.0 / ci->volume;
+  double gsum = 0.0;
+#pragma unroll
+  for (int r = 0; r < MAXR; ++r) {
+    if (r < R) {
+      const double lam = tab->eigs[r];
+      const double c = c6[(size_t)i * R + r];
+      const double dEdc = -lam * inv_vol * pr[r] + lam * c * tab->selfcont[s];
+      gsum += dEdc * dc6[(size_t)i * R + r];
+    }
+  }
+  const double du[3] = {-inv_vol * gu0, -inv_vol * gu1, -inv_vol * gu2};
+  gcn[i] = gsum;
+#pragma unroll
+  for (int b = 0; b < 3; ++b)
+    gpos[3 * i + b] = du[0] * g.n[0] * ci->inv[3 * b + 0] + du[1] * g.n[1] * ci->inv[3 * b + 1] +
+                      du[2] * g.n[2] * ci->inv[3 * b + 2];
+}
+
 template <typename T, int P, bool LAG>
 static int gather_r(const MeshGeom& mg, int blocks, int n, const double* pos, double ps, const int32_t* species,
                     const double* c6, const double* dc6, const CellInfo* ci, const Tables* tab, const int* order,
@@ -451,6 +606,18 @@ static int gather_r(const MeshGeom& mg, int blocks, int n, const double* pos, do
   const int4* rb = rec.b;
   const T* rw = (const T*)rec.w;
   const T* rdw = (const T*)rec.dw;
+  // z-run gather where its register arrays (ranks x run) stay small: float up to 4 ranks at any
+  // order or 8 ranks up to order 5; double up to 4 ranks up to order 5
+  constexpr bool z4 = sizeof(T) == 4 || P <= 5;
+  constexpr bool z8 = sizeof(T) == 4 && P <= 5;
+  if (!mcell && ((mg.R <= 4 && z4) || (mg.R <= 8 && z8))) {
+    if (mg.R <= 4)
+      k_gather_z<T, P, 4><<<blocks, tb, 0, s>>>(g, n, c6, dc6, ci, tab, order, rb, rw, rdw, phi, gcn, gpos);
+    else if constexpr (z8)
+      k_gather_z<T, P, 8><<<blocks, tb, 0, s>>>(g, n, c6, dc6, ci, tab, order, rb, rw, rdw, phi, gcn, gpos);
+    FD3_LAUNCHED();
+    return FD3_OK;
+  }
   if (mg.R <= 4)
     k_gather<T, P, LAG, 4><<<blocks, tb, 0, s>>>(g, n, pos, ps, species, c6, dc6, ci, tab, order, rb, rw, rdw, phi,
                                                   gcn, gpos, mcell);

@@ -430,12 +430,43 @@ struct HitList {
 // CN of the atoms of one bin from the shared-memory stage (raw CN, before cncorr), plus the
 // pair records. Bins whose neighbourhood does not fit the stage mark their atoms n = -2 and
 // leave them to k_cn_global.
+// Per atom (one warp) the staged candidates are first tested against the cutoff 32 at a time
+// (float64 distances); the indices of the pairs inside are compacted in order into a per-warp
+// ring of 64, and whenever 32 are waiting all lanes evaluate the CN function for them and write
+// their records contiguously. The CN function and the record stores thus run on full warps
+// instead of on the ~15 % of lanes that hit in a given candidate batch.
+constexpr int kCnRing = 64;
+
+template <typename TE, typename TC>
+__device__ __forceinline__ void cn_hit(const BinStage& st, int c, double w0, double w1, double w2, TC rci, TC rc,
+                                       const Tables* __restrict__ tab, HitList<TE>& hl, size_t hb, int h,
+                                       TC& acc) {
+  const double4 pj = st.p[c];
+  const TC v0 = (TC)((pj.x - w0) * kAngToBohr);
+  const TC v1 = (TC)((pj.y - w1) * kAngToBohr);
+  const TC v2 = (TC)((pj.z - w2) * kAngToBohr);
+  const TC r2 = v0 * v0 + v1 * v1 + v2 * v2;
+  TC f = TC(0), a = TC(0);
+  if (r2 > TC(1e-12)) {
+    cn_pair<TC>(r2, rci + (TC)tab->rcov[(int)pj.w], rc, f, a);
+    acc += f;
+  }
+  if (h < hl.cap) {
+    hl.j[hb + h] = st.j[c];
+    hl.a[hb + h] = (TE)a;
+    hl.d[3 * (hb + h)] = (TE)v0;
+    hl.d[3 * (hb + h) + 1] = (TE)v1;
+    hl.d[3 * (hb + h) + 2] = (TE)v2;
+  }
+}
+
 template <typename TE, typename TC>
 __global__ void __launch_bounds__(256) k_cn_bins(GridDev g, const int* __restrict__ bin_start,
                                                 const double4* __restrict__ xs, const int4* __restrict__ meta,
                                                 const Tables* __restrict__ tab, double* __restrict__ cn,
                                                 HitList<TE> hl, int* __restrict__ ovf) {
   __shared__ BinStage st;
+  __shared__ int ring[kWarpsPerBlock][kCnRing];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int b = blockIdx.x;
   const int total = stage_bin(g, b, bin_start, xs, meta, st, nullptr, nullptr);
@@ -447,6 +478,7 @@ __global__ void __launch_bounds__(256) k_cn_bins(GridDev g, const int* __restric
   }
   const unsigned lt = (1u << lane) - 1u;
   const TC rc = (TC)tab->r_cut;
+  int* rg = ring[wid];
   for (int t = s0 + wid; t < s1; t += kWarpsPerBlock) {
     const double4 xi = xs[t];
     const int4 mi = meta[t];
@@ -454,43 +486,36 @@ __global__ void __launch_bounds__(256) k_cn_bins(GridDev g, const int* __restric
     wrapped_pos(g, xi, mi, w0, w1, w2);
     const TC rci = (TC)tab->rcov[(int)xi.w];
     TC acc = TC(0);
-    int cnt = 0;
+    int produced = 0, consumed = 0;
     const size_t hb = (size_t)t * hl.cap;
     for (int c0 = 0; c0 < total; c0 += 32) {
       const int c = c0 + lane;
       bool hit = false;
-      TC v0 = 0, v1 = 0, v2 = 0, a = 0;
       if (c < total) {
         const double4 pj = st.p[c];
         const double d0 = pj.x - w0, d1 = pj.y - w1, d2 = pj.z - w2;
-        if (d0 * d0 + d1 * d1 + d2 * d2 < g.rc2) {
-          v0 = (TC)(d0 * kAngToBohr);
-          v1 = (TC)(d1 * kAngToBohr);
-          v2 = (TC)(d2 * kAngToBohr);
-          const TC r2 = v0 * v0 + v1 * v1 + v2 * v2;
-          if (r2 > TC(1e-12)) {
-            TC f;
-            cn_pair<TC>(r2, rci + (TC)tab->rcov[(int)pj.w], rc, f, a);
-            acc += f;
-            hit = a != TC(0);
-          }
-        }
+        hit = d0 * d0 + d1 * d1 + d2 * d2 < g.rc2;
       }
       const unsigned m = __ballot_sync(0xffffffffu, hit);
-      const int pos = cnt + __popc(m & lt);
-      if (hit && pos < hl.cap) {
-        hl.j[hb + pos] = st.j[c];
-        hl.a[hb + pos] = (TE)a;
-        hl.d[3 * (hb + pos)] = (TE)v0;
-        hl.d[3 * (hb + pos) + 1] = (TE)v1;
-        hl.d[3 * (hb + pos) + 2] = (TE)v2;
+      if (hit) rg[(produced + __popc(m & lt)) & (kCnRing - 1)] = c;
+      produced += __popc(m);
+      __syncwarp();
+      if (produced - consumed >= 32) {
+        const int h = consumed + lane;
+        cn_hit<TE, TC>(st, rg[h & (kCnRing - 1)], w0, w1, w2, rci, rc, tab, hl, hb, h, acc);
+        consumed += 32;
+        __syncwarp();
       }
-      cnt += __popc(m);
     }
+    if (consumed + lane < produced) {
+      const int h = consumed + lane;
+      cn_hit<TE, TC>(st, rg[h & (kCnRing - 1)], w0, w1, w2, rci, rc, tab, hl, hb, h, acc);
+    }
+    __syncwarp();
     const double cnv = warp_sum((double)acc);
     if (lane == 0) {
-      hl.n[t] = cnt <= hl.cap ? cnt : -1;
-      if (cnt > hl.cap) atomicAdd(ovf, 1);
+      hl.n[t] = produced <= hl.cap ? produced : -1;
+      if (produced > hl.cap) atomicAdd(ovf, 1);
       cn[mi.w] = cnv;
     }
   }

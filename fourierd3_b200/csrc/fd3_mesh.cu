@@ -108,18 +108,22 @@ __device__ __forceinline__ KPoint<T> kpoint(const MeshDev& g, size_t k, const T 
 #pragma unroll
   for (int c = 0; c < 3; ++c) q.kv[c] = T(mx) * rc[c] + T(my) * rc[3 + c] + T(mz) * rc[6 + c];
   q.knorm = sqrt(q.kv[0] * q.kv[0] + q.kv[1] * q.kv[1] + q.kv[2] * q.kv[2]);
-  double sc = 1.0;
-  if (spme) {
-    if (deconv) {
-      sc = (double)deconv[k];
-    } else {
-      const double nzf = (double)(2 * (g.nzh - 1));
-      double v = sinc_pi(mx / (double)g.n[0]) * sinc_pi(my / (double)g.n[1]) * sinc_pi(mz / nzf);
-      v = pow(v, 2.0 * P);
-      sc = v < 1e-10 ? 1e-10 : v;
+  if (sizeof(T) == 4 && spme && deconv) {
+    q.inv_sc = T(1.0f / deconv[k]);   // mixed form: the float32 window inverted in float
+  } else {
+    double sc = 1.0;
+    if (spme) {
+      if (deconv) {
+        sc = (double)deconv[k];
+      } else {
+        const double nzf = (double)(2 * (g.nzh - 1));
+        double v = sinc_pi(mx / (double)g.n[0]) * sinc_pi(my / (double)g.n[1]) * sinc_pi(mz / nzf);
+        v = pow(v, 2.0 * P);
+        sc = v < 1e-10 ? 1e-10 : v;
+      }
     }
+    q.inv_sc = (T)(1.0 / sc);
   }
-  q.inv_sc = (T)(1.0 / sc);
   q.wk = (iz == 0 || iz == g.nzh - 1) ? T(1) : T(2);
   // Self-conjugate planes (kz = 0 and the z-Nyquist plane): the entry at (ix, iy) and its conjugate
   // partner (-ix, -iy) are both stored, but at the Nyquist rows their k-vectors differ in a
@@ -168,9 +172,10 @@ __device__ __forceinline__ void virial_acc(const KPoint<T>& q, T dq, double* acc
 // arithmetic. Per-k terms are formed in T and accumulated in float64. Grid-stride over k-points;
 // one partial (energy + 6 virial components) per block.
 template <typename T, int MAXS, int MAXR>
-__global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int spme,
+__global__ void __launch_bounds__(kFilterThreads, sizeof(T) == 8 ? 2 : (MAXS <= 2 ? 3 : 1)) k_filter(MeshDev g, int P, int spme,
                                                            const CellInfo* __restrict__ ci,
                                                            const typename GreenPairOf<T>::type* __restrict__ gp,
+                                                           const float4* __restrict__ g4,
                                                            const Tables* __restrict__ tab,
                                                            const float* __restrict__ deconv,
                                                            typename Cplx<T>::type* __restrict__ spec,
@@ -184,6 +189,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int
   load_recip<T>(ci, rc);
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < Mh; k += (size_t)gridDim.x * blockDim.x) {
     const KPoint<T> q = kpoint<T>(g, k, rc, deconv, spme, P);
+    const T invk = q.knorm > T(0) ? T(1) / q.knorm : T(0);
     T G[MAXS][MAXS], dG[MAXS][MAXS], Gh[MAXS][MAXS];
 #pragma unroll
     for (int X = 0; X < MAXS; ++X)
@@ -191,7 +197,15 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter(MeshDev g, int P, int
       for (int Y = X; Y < MAXS; ++Y) {
         T gv = T(0), dv = T(0);
         if (X < S && Y < S) {
-          green_eval<T>(gp[X * S + Y], q.knorm, s6, s8, gv, dv);
+          if constexpr (sizeof(T) == 4) {
+            const float4 c4 = g4[X * S + Y];
+            if (q.knorm * c4.x < 1e-15f)
+              green_eval<T>(gp[X * S + Y], q.knorm, s6, s8, gv, dv);
+            else
+              green_eval_folded(c4, q.knorm, invk, gv, dv);
+          } else {
+            green_eval<T>(gp[X * S + Y], q.knorm, s6, s8, gv, dv);
+          }
           gv *= q.inv_sc;
           dv *= q.inv_sc;
         }
@@ -526,7 +540,7 @@ int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, c
     const int blocks = filter_grid(Mh);
     *n_blocks = blocks;
 #define FD3_FILTER(SS, RR) \
-  k_filter<T, SS, RR><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gpt, tab, deconv, sp, part)
+  k_filter<T, SS, RR><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gpt, g4, tab, deconv, sp, part)
     if (mg.S <= 1)
       FD3_FILTER(1, 4);
     else if (mg.S <= 2 && mg.R <= 4)

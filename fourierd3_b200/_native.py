@@ -16,6 +16,8 @@ FD3_OK, FD3_EINVAL, FD3_ECAPACITY, FD3_ECUDA, FD3_ECUFFT, FD3_ENOMEM = range(6)
 METHODS = {"spme": 0, "pme": 1, "ewald": 2}
 PREC_FP64, PREC_MIXED = 0, 1
 TUNE_FILTER_KT = 0
+TUNE_SPREAD_ZC = 1
+TUNE_SPREAD_CAP = 2
 
 _c_int32 = ctypes.c_int32
 _c_int64 = ctypes.c_int64

@@ -200,6 +200,8 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
       m.S = S;
       m.R = R;
       m.filter_kt = -1;
+      m.spread_zc = -1;
+      m.spread_cap = 0;
       const size_t Mh = (size_t)m.n[0] * m.n[1] * m.nzh;
       if (d->method == FD3_METHOD_SPME && d->deconv) {
         if (cudaMalloc(&p->d_deconv, sizeof(float) * Mh) != cudaSuccess ||
@@ -258,6 +260,22 @@ extern "C" int fd3_plan_set_tuning(fd3_plan* p, int32_t knob, int32_t value) {
     p->mg.filter_kt = value;
     return FD3_OK;
   }
+  if (knob == FD3_TUNE_SPREAD_ZC) {
+    if (value < -1 || value > 64) {
+      set_error("fd3_plan_set_tuning", "spread z-chunk must be -1 (default), 0 (per-tile kernel) or 1..64");
+      return FD3_EINVAL;
+    }
+    p->mg.spread_zc = value;
+    return FD3_OK;
+  }
+  if (knob == FD3_TUNE_SPREAD_CAP) {
+    if (value != 0 && value < 256) {
+      set_error("fd3_plan_set_tuning", "spread staging cap must be 0 (shared-memory bound) or >= 256");
+      return FD3_EINVAL;
+    }
+    p->mg.spread_cap = value;
+    return FD3_OK;
+  }
   set_error("fd3_plan_set_tuning", "unknown knob");
   return FD3_EINVAL;
 }
@@ -269,6 +287,15 @@ extern "C" int fd3_plan_get_tuning(const fd3_plan* p, int32_t knob, int32_t* val
     *value = p->method == FD3_METHOD_EWALD ? -1
              : p->mg.filter_kt >= 0        ? p->mg.filter_kt
                                            : filter_default_kt(p->S, p->R, ts);
+    return FD3_OK;
+  }
+  if (knob == FD3_TUNE_SPREAD_ZC) {
+    *value = p->method == FD3_METHOD_EWALD ? -1
+                                           : spread_chunk_in_effect(p->mg, p->precision == FD3_PREC_FP64 ? 8 : 4);
+    return FD3_OK;
+  }
+  if (knob == FD3_TUNE_SPREAD_CAP) {
+    *value = p->mg.spread_cap;
     return FD3_OK;
   }
   set_error("fd3_plan_get_tuning", "unknown knob");

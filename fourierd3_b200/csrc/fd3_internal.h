@@ -111,6 +111,8 @@ struct MeshGeom {
   int lagrange;   // 0: B-spline (spme), 1: Lagrange (pme)
   int S, R;
   int filter_kt;  // filter k-tile width (0: register kernel), -1: default for (S, R)
+  int spread_zc;  // z-tiles per column chunk of the spread (0: per-tile kernel), -1: default
+  int spread_cap; // staged atoms per column chunk at most (0: as many as shared memory holds)
 };
 int launch_cellinfo(const double* cell, double scale, CellInfo* ci, cudaStream_t s);
 int launch_mesh_keys(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
@@ -133,6 +135,7 @@ int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, c
                   int* n_blocks, cudaStream_t s);
 int filter_max_blocks();
 int filter_default_kt(int S, int R, size_t tsize);
+int spread_chunk_in_effect(const MeshGeom& mg, size_t tsize);
 bool filter_kt_valid(int kt, int S, int R, size_t tsize);
 template <typename T>
 int launch_gather(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,

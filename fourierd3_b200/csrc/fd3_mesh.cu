@@ -469,6 +469,11 @@ static int filter_grid(size_t Mh) {
 
 int filter_max_blocks() { return 148 * 8 * 4; }
 
+int spread_chunk_in_effect(const MeshGeom& mg, size_t tsize) {
+  const int cap = tsize == 8 ? spread_col_cap<double>(mg) : spread_col_cap<float>(mg);
+  return cap >= kColMinCap ? spread_zc(mg) : 0;
+}
+
 // Largest k-tile width whose shared-memory tile fits (the default when no tuning is set).
 int filter_default_kt(int S, int R, size_t tsize) {
   if (S <= 4) return 0;   // register kernel

@@ -276,6 +276,357 @@ __global__ void __launch_bounds__(kSpThreads, sizeof(T) == 8 ? 2 : 4) k_spread(M
   }
 }
 
+// Column spread. A CTA owns a column of 16 x 16 points in (x, y) and a chunk of ZC z-tiles of one
+// species; thread (lx, ly) owns the z-row of 8 points of the current z-tile. The atoms whose x and
+// y stencils reach the column are staged ONCE per chunk, in counting-sorted segment order with the
+// source z-tile outermost, as tile-local x and y weight rows, rank factors, and two z rows: the
+// part of the z stencil inside the atom's own z-tile and the part spilling into the next one
+// (a stencil of P <= t_z + 1 nodes spans at most two tiles). The atoms reaching z-tile T are then
+// two contiguous ranges of the staged list, those of source tile T (own rows) and of T - 1 (spill
+// rows), so the CTA sweeps its z-tiles from shared memory with no selection and no barrier.
+// Global loads and the candidate search happen once per ZC tiles. A chunk whose staged set
+// exceeds `cap` falls back, inside the same CTA, to staging per tile in pieces of `cap`. Each
+// mesh value is written exactly once in a fixed summation order (no atomics); results are
+// independent of ZC up to the summation order.
+constexpr int kColMaxSeg = 64;
+
+template <typename T>
+struct ColSmem {
+  T* wx;      // [cap][16]
+  T* wy;      // [cap][16]
+  T* wzo;     // [cap][8] z row inside the atom's own z-tile
+  T* wzn;     // [cap][8] z row spilling into the next z-tile
+  T* cc;      // [cap][R]
+  int* zi;    // [cap] source z-tile (index into the chunk's source range); bit 30: spills
+  int* zst;   // [kColMaxSeg + 1] first staged slot of each source z-tile
+};
+
+template <typename T>
+__host__ __device__ inline size_t col_smem_bytes(int cap, int R) {
+  size_t b = (size_t)cap * (16 + 16 + 2 * kSpTZ + R) * sizeof(T);
+  b += (size_t)cap * sizeof(int) + (kColMaxSeg + 1) * sizeof(int);
+  return (b + 15) & ~(size_t)15;
+}
+
+template <typename T>
+__device__ __forceinline__ ColSmem<T> col_carve(unsigned char* base, int cap, int R) {
+  ColSmem<T> m;
+  T* t = reinterpret_cast<T*>(base);
+  m.wx = t;
+  m.wy = m.wx + (size_t)cap * 16;
+  m.wzo = m.wy + (size_t)cap * 16;
+  m.wzn = m.wzo + (size_t)cap * kSpTZ;
+  m.cc = m.wzn + (size_t)cap * kSpTZ;
+  m.zi = reinterpret_cast<int*>(m.cc + (size_t)cap * R);
+  m.zst = m.zi + cap;
+  return m;
+}
+
+constexpr int kZiSpill = 1 << 30;
+
+// Block-wide ordered compaction of one flag per thread: returns this thread's slot (among the
+// set flags, in thread order) and writes the block total to *tot. Two barriers.
+__device__ __forceinline__ int block_compact(bool keep, int* s_wcnt, int* tot) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const unsigned bal = __ballot_sync(0xffffffffu, keep);
+  if (lane == 0) s_wcnt[wid] = __popc(bal);
+  __syncthreads();
+  int off = 0, t = 0;
+#pragma unroll
+  for (int w = 0; w < kSpThreads / 32; ++w) {
+    off += w < wid ? s_wcnt[w] : 0;
+    t += s_wcnt[w];
+  }
+  __syncthreads();
+  *tot = t;
+  return off + __popc(bal & ((1u << lane) - 1u));
+}
+
+// Stage candidates [from, total) whose stencil reaches the column in x and y (and z-tile tzt when
+// tzt >= 0) into slots [0, cap). Segment e covers source z-tile e / seg_per_z of the chunk.
+// Returns the number staged; *next is the first candidate not yet examined or staged (== total
+// when all were taken).
+template <typename T, int P>
+__device__ int col_stage(const MeshDev& g, const int* s_a0, const int* s_pref, int nseg, int seg_per_z, int total,
+                         int from, const int (&t0)[3], int tzt, int cap, const int4* __restrict__ rb,
+                         const T* __restrict__ rw, const T* __restrict__ rc, const ColSmem<T>& m, int* s_wcnt,
+                         int* s_next, int* next) {
+  const int R = g.R;
+  int staged = 0;
+  int c0 = from;
+  bool full = false;
+  if (threadIdx.x == 0) *s_next = total;
+  for (; c0 < total; c0 += kSpThreads) {
+    const int ca = c0 + threadIdx.x;
+    bool keep = false;
+    int u = 0, seg = 0;
+    int4 b4 = make_int4(0, 0, 0, 0);
+    if (ca < total) {
+      int lo = 0, hi = nseg - 1;   // last segment with pref <= ca
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (s_pref[mid] <= ca) lo = mid; else hi = mid - 1;
+      }
+      seg = lo;
+      u = s_a0[lo] + (ca - s_pref[lo]);
+      b4 = rb[u];
+      keep = true;
+      const int base[3] = {b4.x, b4.y, b4.z};
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        if (a == 2 && tzt < 0) break;
+        const int ta = a == 2 ? tzt * g.t[2] : t0[a];
+        int d = ta - base[a];
+        if (d < 0) d += g.n[a];
+        const int pf = P < g.n[a] ? P : g.n[a];
+        if (!(d < pf || d + g.t[a] > g.n[a])) keep = false;
+      }
+    }
+    int tot;
+    const int slot = staged + block_compact(keep, s_wcnt, &tot);
+    if (keep && slot < cap) {
+      // tile-local x and y rows (stencil nodes that wrap onto the same point are summed)
+      T* wxr = m.wx + (size_t)slot * 16;
+      T* wyr = m.wy + (size_t)slot * 16;
+      T* zo = m.wzo + (size_t)slot * kSpTZ;
+      T* zn = m.wzn + (size_t)slot * kSpTZ;
+#pragma unroll
+      for (int z = 0; z < 16; ++z) {
+        wxr[z] = T(0);
+        wyr[z] = T(0);
+      }
+#pragma unroll
+      for (int z = 0; z < kSpTZ; ++z) {
+        zo[z] = T(0);
+        zn[z] = T(0);
+      }
+      const T* w = rw + (size_t)u * 3 * P;
+      const int oz = b4.z % g.t[2];   // offset of the base inside its own z-tile
+      bool spill = false;
+#pragma unroll
+      for (int k = 0; k < P; ++k) {
+        int ix = b4.x + k - t0[0];
+        while (ix < 0) ix += g.n[0];
+        while (ix >= g.n[0]) ix -= g.n[0];
+        int iy = b4.y + k - t0[1];
+        while (iy < 0) iy += g.n[1];
+        while (iy >= g.n[1]) iy -= g.n[1];
+        if (ix < g.t[0]) wxr[ix] += w[k];
+        if (iy < g.t[1]) wyr[iy] += w[P + k];
+        const int z = oz + k;
+        if (z < g.t[2]) {
+          zo[z] = w[2 * P + k];
+        } else {
+          zn[z - g.t[2]] = w[2 * P + k];
+          spill = true;
+        }
+      }
+      m.zi[slot] = seg / seg_per_z + (spill ? kZiSpill : 0);
+      for (int r = 0; r < R; ++r) m.cc[(size_t)slot * R + r] = rc[(size_t)u * R + r];
+    }
+    if (keep && slot >= cap) atomicMin(s_next, ca);
+    staged += tot;
+    if (staged >= cap) {
+      full = true;
+      break;
+    }
+  }
+  __syncthreads();
+  int nx = *s_next;   // first kept candidate that found no slot, else total
+  if (full && c0 + kSpThreads < nx) nx = c0 + kSpThreads;   // the pass filled cap exactly
+  *next = nx;
+  __syncthreads();
+  return staged < cap ? staged : cap;
+}
+
+// acc[z][r] += w_x(lx) w_y(ly) w_z(z) c_{r0+r} over staged atoms [a0, a1) whose source z-tile
+// is zsrc, with their own-tile rows (spill = false) or spill rows (spill = true).
+template <typename T>
+__device__ __forceinline__ void col_accumulate(const ColSmem<T>& m, int a0, int a1, int zsrc, bool spill, int R,
+                                               int r0, int lx, int ly, T (&acc)[kSpTZ][kSpRC]) {
+  const T* zrows = spill ? m.wzn : m.wzo;
+  for (int a = a0; a < a1; ++a) {
+    const int zi = m.zi[a];
+    if ((zi & ~kZiSpill) != zsrc || (spill && !(zi & kZiSpill))) continue;
+    const T wxy = m.wx[(size_t)a * 16 + lx] * m.wy[(size_t)a * 16 + ly];
+    if (wxy != T(0)) {
+      T cr[kSpRC];
+#pragma unroll
+      for (int r = 0; r < kSpRC; ++r) cr[r] = r0 + r < R ? wxy * m.cc[(size_t)a * R + r0 + r] : T(0);
+      const T* zr = zrows + (size_t)a * kSpTZ;
+#pragma unroll
+      for (int z = 0; z < kSpTZ; ++z) {
+        const T wz = zr[z];
+#pragma unroll
+        for (int r = 0; r < kSpRC; ++r) acc[z][r] += wz * cr[r];
+      }
+    }
+  }
+}
+
+template <typename T>
+__device__ __forceinline__ void col_store(const MeshDev& g, int X, int r0, const int (&t0)[3], int tzt, int lx,
+                                          int ly, const T (&acc)[kSpTZ][kSpRC], T* __restrict__ rho) {
+  if (lx >= g.t[0] || ly >= g.t[1]) return;
+  const size_t M = (size_t)g.n[0] * g.n[1] * g.n[2];
+  const size_t m0 = ((size_t)(t0[0] + lx) * g.n[1] + (t0[1] + ly)) * g.n[2] + (size_t)tzt * g.t[2];
+#pragma unroll
+  for (int r = 0; r < kSpRC; ++r) {
+    if (r0 + r >= g.R) break;
+    T* dst = rho + ((size_t)X * g.R + r0 + r) * M + m0;
+    if (g.t[2] == kSpTZ) {
+      if (sizeof(T) == 4) {
+        float4* v = reinterpret_cast<float4*>(dst);
+        v[0] = make_float4((float)acc[0][r], (float)acc[1][r], (float)acc[2][r], (float)acc[3][r]);
+        v[1] = make_float4((float)acc[4][r], (float)acc[5][r], (float)acc[6][r], (float)acc[7][r]);
+      } else {
+        double2* v = reinterpret_cast<double2*>(dst);
+#pragma unroll
+        for (int z = 0; z < kSpTZ; z += 2) v[z / 2] = make_double2((double)acc[z][r], (double)acc[z + 1][r]);
+      }
+    } else {
+#pragma unroll
+      for (int z = 0; z < kSpTZ; ++z)
+        if (z < g.t[2]) dst[z] = acc[z][r];
+    }
+  }
+}
+
+template <typename T, int P>
+__global__ void __launch_bounds__(kSpThreads, sizeof(T) == 8 ? 2 : 3) k_spread_col(
+    MeshDev g, int zc, int cap, const int4* __restrict__ rb, const T* __restrict__ rw, const T* __restrict__ rc,
+    const int* __restrict__ key_start, T* __restrict__ rho) {
+  extern __shared__ __align__(16) unsigned char col_raw[];
+  __shared__ int s_a0[kColMaxSeg], s_pref[kColMaxSeg + 1];
+  __shared__ int s_wcnt[kSpThreads / 32];
+  __shared__ int s_next;
+  const ColSmem<T> m = col_carve<T>(col_raw, cap, g.R);
+  const int tid = threadIdx.x;
+  const int X = blockIdx.y;
+  const int nzc = (g.nt[2] + zc - 1) / zc;
+  const int zch = blockIdx.x % nzc;
+  const int cxy = blockIdx.x / nzc;
+  const int ty = cxy % g.nt[1], tx = cxy / g.nt[1];
+  const int tz0 = zch * zc;
+  const int tz1 = tz0 + zc < g.nt[2] ? tz0 + zc : g.nt[2];
+  const int t0[3] = {tx * g.t[0], ty * g.t[1], 0};
+  const int lx = tid / kSpTY, ly = tid % kSpTY;
+  // source z-tiles of the chunk: tz - 1 and tz for tz in [tz0, tz1), each once
+  int nzs = (tz1 - tz0) + 1;
+  int zs0 = tz0 - 1;
+  if (nzs >= g.nt[2]) {
+    nzs = g.nt[2];
+    zs0 = 0;
+  }
+  const int spz = g.ns[0] * g.ns[1];   // segments per source z-tile
+  const int nseg = spz * nzs;
+  for (int e = tid; e < nseg; e += kSpThreads) {
+    const int zi = e / spz, xo = (e % spz) / g.ns[1], yo = e % g.ns[1];
+    const int sx = posmod(tx - xo, g.nt[0]), sy = posmod(ty - yo, g.nt[1]), sz = posmod(zs0 + zi, g.nt[2]);
+    const int key = ((sx * g.nt[1] + sy) * g.nt[2] + sz) * g.S + X;
+    const int a0 = key_start[key];
+    s_a0[e] = a0;
+    s_pref[e + 1] = key_start[key + 1] - a0;
+  }
+  __syncthreads();
+  if (tid < 32) {   // inclusive warp scan of the segment sizes (nseg <= 64)
+    int v0 = tid + 1 <= nseg ? s_pref[tid + 1] : 0;
+    int v1 = tid + 33 <= nseg ? s_pref[tid + 33] : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int a = __shfl_up_sync(0xffffffffu, v0, o);
+      const int b = __shfl_up_sync(0xffffffffu, v1, o);
+      if (tid >= o) {
+        v0 += a;
+        v1 += b;
+      }
+    }
+    const int carry = __shfl_sync(0xffffffffu, v0, 31);
+    if (tid + 1 <= nseg) s_pref[tid + 1] = v0;
+    if (tid + 33 <= nseg) s_pref[tid + 33] = v1 + carry;
+    if (tid == 0) s_pref[0] = 0;
+  }
+  __syncthreads();
+  const int total = s_pref[nseg];
+  int next = 0;
+  const int staged = col_stage<T, P>(g, s_a0, s_pref, nseg, spz, total, 0, t0, -1, cap, rb, rw, rc, m, s_wcnt,
+                                     &s_next, &next);
+  if (next >= total) {
+    // first staged slot of each source z-tile (the staged list is ordered by source z-tile)
+    for (int zi = tid; zi <= nzs; zi += kSpThreads) {
+      int lo = 0, hi = staged;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if ((m.zi[mid] & ~kZiSpill) < zi) lo = mid + 1; else hi = mid;
+      }
+      m.zst[zi] = lo;
+    }
+    __syncthreads();
+    for (int tzt = tz0; tzt < tz1; ++tzt) {
+      const int zown = nzs == g.nt[2] ? tzt : tzt - zs0;
+      const int zprev = nzs == g.nt[2] ? (tzt + g.nt[2] - 1) % g.nt[2] : zown - 1;
+      for (int r0 = 0; r0 < g.R; r0 += kSpRC) {
+        T acc[kSpTZ][kSpRC];
+#pragma unroll
+        for (int z = 0; z < kSpTZ; ++z)
+#pragma unroll
+          for (int r = 0; r < kSpRC; ++r) acc[z][r] = T(0);
+        col_accumulate<T>(m, m.zst[zprev], m.zst[zprev + 1], zprev, true, g.R, r0, lx, ly, acc);
+        col_accumulate<T>(m, m.zst[zown], m.zst[zown + 1], zown, false, g.R, r0, lx, ly, acc);
+        col_store<T>(g, X, r0, t0, tzt, lx, ly, acc, rho);
+      }
+    }
+    return;
+  }
+  // dense column: per z-tile, stage the atoms reaching that tile in pieces of `cap`
+  for (int tzt = tz0; tzt < tz1; ++tzt) {
+    const int zown = nzs == g.nt[2] ? tzt : tzt - zs0;
+    const int zprev = nzs == g.nt[2] ? (tzt + g.nt[2] - 1) % g.nt[2] : zown - 1;
+    for (int r0 = 0; r0 < g.R; r0 += kSpRC) {
+      T acc[kSpTZ][kSpRC];
+#pragma unroll
+      for (int z = 0; z < kSpTZ; ++z)
+#pragma unroll
+        for (int r = 0; r < kSpRC; ++r) acc[z][r] = T(0);
+      int from = 0;
+      while (from < total) {
+        const int st = col_stage<T, P>(g, s_a0, s_pref, nseg, spz, total, from, t0, tzt, cap, rb, rw, rc, m,
+                                       s_wcnt, &s_next, &from);
+        col_accumulate<T>(m, 0, st, zprev, true, g.R, r0, lx, ly, acc);
+        col_accumulate<T>(m, 0, st, zown, false, g.R, r0, lx, ly, acc);
+        __syncthreads();
+      }
+      col_store<T>(g, X, r0, t0, tzt, lx, ly, acc, rho);
+    }
+  }
+}
+
+// Staged atoms per column chunk: as many as let 3 (float) or 2 (double) CTAs share an SM.
+template <typename T>
+inline int spread_col_cap(const MeshGeom& mg) {
+  constexpr int per_sm = sizeof(T) == 8 ? 2 : 3;
+  const size_t fixed = col_smem_bytes<T>(0, mg.R);
+  const size_t per_atom = col_smem_bytes<T>(64, mg.R) / 64;
+  int cap = (int)((size_t)(220 * 1024 / per_sm - 2048 - fixed) / per_atom);
+  if (cap > 1024) cap = 1024;
+  if (mg.spread_cap > 0 && mg.spread_cap < cap) cap = mg.spread_cap;
+  return cap;
+}
+constexpr int kColMinCap = 128;
+
+// z-tiles per column chunk in effect for this mesh (0: per-tile kernel).
+inline int spread_zc(const MeshGeom& mg) {
+  // the column form needs stencils that span at most two z-tiles of a mesh with >= 2 z-tiles
+  if (mg.spread_zc == 0 || mg.ns[0] > 2 || mg.ns[1] > 2 || mg.nt[2] < 2 || mg.order > mg.t[2] + 1 ||
+      mg.t[2] > kSpTZ)
+    return 0;
+  int zc = mg.spread_zc > 0 ? mg.spread_zc : 8;
+  const int lim = kColMaxSeg / (mg.ns[0] * mg.ns[1]) - 1;
+  if (zc > lim) zc = lim;
+  if (zc > mg.nt[2]) zc = mg.nt[2];
+  return zc < 1 ? 0 : zc;
+}
+
 template <typename T, int P, bool LAG>
 static int spread_r(const MeshGeom& mg, dim3 grid, int n, const double* pos, double ps, const int32_t* species,
                     const double* c6, const CellInfo* ci, const int* ks, const int* order, const MeshRecords& rec,
@@ -285,6 +636,29 @@ static int spread_r(const MeshGeom& mg, dim3 grid, int n, const double* pos, dou
     k_mesh_records<T, P, LAG><<<(n + 255) / 256, 256, 0, s>>>(g, n, pos, ps, species, c6, ci, order, rec.b, (T*)rec.w,
                                                               (T*)rec.dw, (T*)rec.c);
     FD3_LAUNCHED();
+  }
+  const int zc = spread_zc(mg);
+  if (zc > 0) {
+    // staged atoms per chunk: as many as let 3 (float) or 2 (double) CTAs share an SM
+    const int cap = spread_col_cap<T>(mg);
+    if (cap >= kColMinCap) {
+      const size_t smem = col_smem_bytes<T>(cap, mg.R);
+      static bool attr = false;
+      if (!attr) {
+        if (cudaFuncSetAttribute(k_spread_col<T, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024) !=
+            cudaSuccess) {
+          set_error("spread", "could not raise the shared-memory limit of the column spread");
+          return FD3_ECUDA;
+        }
+        attr = true;
+      }
+      const int nzc = (mg.nt[2] + zc - 1) / zc;
+      const dim3 cgrid(mg.nt[0] * mg.nt[1] * nzc, mg.S);
+      k_spread_col<T, P><<<cgrid, kSpThreads, smem, s>>>(g, zc, cap, rec.b, (const T*)rec.w, (const T*)rec.c, ks,
+                                                        rho);
+      FD3_LAUNCHED();
+      return FD3_OK;
+    }
   }
   k_spread<T, P><<<grid, kSpThreads, 0, s>>>(g, rec.b, (const T*)rec.w, (const T*)rec.c, ks, rho);
   FD3_LAUNCHED();

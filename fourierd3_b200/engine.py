@@ -161,17 +161,26 @@ class Engine:
         _native.check(_native.lib().fd3_cell_grid(_native.dptr(c), float(r_cut_ang), nb, rr), "fd3_cell_grid")
         return tuple(nb), tuple(rr)
 
-    def set_tuning(self, filter_kt: Optional[int] = None) -> None:
-        """Launch-shape knobs (results agree to rounding): ``filter_kt`` = k-points per filter tile."""
-        if filter_kt is not None:
-            _native.check(_native.lib().fd3_plan_set_tuning(self._plan, _native.TUNE_FILTER_KT, int(filter_kt)),
-                          "fd3_plan_set_tuning")
+    _KNOBS = {"filter_kt": _native.TUNE_FILTER_KT, "spread_zc": _native.TUNE_SPREAD_ZC,
+              "spread_cap": _native.TUNE_SPREAD_CAP}
+
+    def set_tuning(self, filter_kt: Optional[int] = None, spread_zc: Optional[int] = None,
+                   spread_cap: Optional[int] = None) -> None:
+        """Launch-shape knobs (results agree to rounding): ``filter_kt`` = k-points per filter
+        tile, ``spread_zc`` = z-tiles per column chunk of the spread, ``spread_cap`` = staged
+        atoms per chunk at most; -1 (0 for the cap) restores a default."""
+        for name, val in (("filter_kt", filter_kt), ("spread_zc", spread_zc), ("spread_cap", spread_cap)):
+            if val is not None:
+                _native.check(_native.lib().fd3_plan_set_tuning(self._plan, self._KNOBS[name], int(val)),
+                              "fd3_plan_set_tuning")
 
     def tuning(self) -> dict:
-        v = ctypes.c_int32()
-        _native.check(_native.lib().fd3_plan_get_tuning(self._plan, _native.TUNE_FILTER_KT, ctypes.byref(v)),
-                      "fd3_plan_get_tuning")
-        return {"filter_kt": int(v.value)}
+        out = {}
+        for name, knob in self._KNOBS.items():
+            v = ctypes.c_int32()
+            _native.check(_native.lib().fd3_plan_get_tuning(self._plan, knob, ctypes.byref(v)), "fd3_plan_get_tuning")
+            out[name] = int(v.value)
+        return out
 
     def profile(self, on: bool = True) -> None:
         """Record CUDA events between pipeline stages of the following calls."""

@@ -84,8 +84,16 @@ FD3_API int fd3_plan_destroy(fd3_plan* plan);
  *   FD3_TUNE_FILTER_KT  k-points per shared-memory tile of the reciprocal-space filter:
  *                       0 = per-thread register kernel (at most 8 species), 1, 2, 4, 8
  *                       or 16 = tiled kernel, -1 = the default for (species, rank).
+ *   FD3_TUNE_SPREAD_ZC  z-tiles per column chunk of the mesh spread: 0 = one CTA per
+ *                       16x16x8 tile, 1..64 = one CTA per 16x16 column chunk (capped by
+ *                       the mesh), -1 = the default (8).
+ *   FD3_TUNE_SPREAD_CAP staged atoms per column chunk at most: 0 = what shared memory
+ *                       holds, >= 256 = a lower bound (denser chunks take the per-tile
+ *                       staging path inside the same CTA).
  * fd3_plan_get_tuning returns the value in effect (the default resolved). */
 #define FD3_TUNE_FILTER_KT 0
+#define FD3_TUNE_SPREAD_ZC 1
+#define FD3_TUNE_SPREAD_CAP 2
 FD3_API int fd3_plan_set_tuning(fd3_plan* plan, int32_t knob, int32_t value);
 FD3_API int fd3_plan_get_tuning(const fd3_plan* plan, int32_t knob, int32_t* value);
 

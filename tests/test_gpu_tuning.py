@@ -61,3 +61,29 @@ def test_autotune_filter_sets_a_valid_tile(cuda_device):
         assert best in times
     e1 = b()[0]
     assert torch.allclose(e0, e1, rtol=2e-6, atol=0)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_spread_column_chunks_agree(precision, cuda_device):
+    """Per-tile spread (zc = 0) against column chunks of several lengths, and the per-tile staging
+    fallback of a column chunk that exceeds its staging cap (all oxygen atoms of the 648-atom box
+    fall into one 16x16 column of a 16^3 mesh)."""
+    from fourierd3_b200 import D3Model, structures as st
+
+    tol_e = 1e-12 if precision == "fp64" else 2e-6
+    tol_f = 1e-10 if precision == "fp64" else 1e-5
+    for kw, zcs in ((KW, (1, 3, 8)), (dict(KW, mesh_spacing=4.8), (1, 2))):
+        pos, cell, z = st.sio2_box(0)
+        m = D3Model(z, cell, precision=precision, device=cuda_device, **kw)
+        m.engine.set_tuning(spread_zc=0)
+        e0, f0, s0 = (t.clone() for t in m(pos, cell))
+        for zc in zcs:
+            for cap in (0, 256):
+                m.engine.set_tuning(spread_zc=zc, spread_cap=cap)
+                assert m.engine.tuning()["spread_zc"] == zc   # the column kernel runs
+                e, f, s = m(pos, cell)
+                assert abs(float(e) - float(e0)) <= tol_e * abs(float(e0)), (zc, cap)
+                assert (f - f0).abs().max().item() <= tol_f, (zc, cap)
+                assert (s - s0).abs().max().item() <= tol_f, (zc, cap)
+    with pytest.raises(ValueError):
+        m.engine.set_tuning(spread_cap=100)

@@ -439,28 +439,51 @@ __device__ int col_stage(const MeshDev& g, const int* s_a0, const int* s_pref, i
   return staged < cap ? staged : cap;
 }
 
-// acc[z][r] += w_x(lx) w_y(ly) w_z(z) c_{r0+r} over staged atoms [a0, a1) whose source z-tile
-// is zsrc, with their own-tile rows (spill = false) or spill rows (spill = true).
-template <typename T>
+// acc[z][r] += w_x(lx) w_y(ly) w_z(z) c_{r0+r} over staged atoms [a0, a1), with their own-tile
+// z rows (spill = false) or spill rows (spill = true). CHECK: the range may hold atoms of other
+// source z-tiles (per-tile staging), skip those whose source tile is not zsrc. Atoms are taken
+// four at a time so that their x/y weight loads are in flight together; an atom with no spill
+// has an all-zero spill row and adds exact zeros.
+template <typename T, bool CHECK>
+__device__ __forceinline__ void col_atom(const ColSmem<T>& m, const T* zrows, int a, T wxy, int zsrc, int R, int r0,
+                                         T (&acc)[kSpTZ][kSpRC]) {
+  if (CHECK && (m.zi[a] & ~kZiSpill) != zsrc) return;
+  T cr[kSpRC];
+#pragma unroll
+  for (int r = 0; r < kSpRC; ++r) cr[r] = r0 + r < R ? wxy * m.cc[(size_t)a * R + r0 + r] : T(0);
+  T zr[kSpTZ];
+  if (sizeof(T) == 4) {
+    const float4* v = reinterpret_cast<const float4*>(zrows + (size_t)a * kSpTZ);
+    const float4 p0 = v[0], p1 = v[1];
+    const float t8[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
+#pragma unroll
+    for (int z = 0; z < kSpTZ; ++z) zr[z] = (T)t8[z];
+  } else {
+#pragma unroll
+    for (int z = 0; z < kSpTZ; ++z) zr[z] = zrows[(size_t)a * kSpTZ + z];
+  }
+#pragma unroll
+  for (int z = 0; z < kSpTZ; ++z)
+#pragma unroll
+    for (int r = 0; r < kSpRC; ++r) acc[z][r] += zr[z] * cr[r];
+}
+
+template <typename T, bool CHECK>
 __device__ __forceinline__ void col_accumulate(const ColSmem<T>& m, int a0, int a1, int zsrc, bool spill, int R,
                                                int r0, int lx, int ly, T (&acc)[kSpTZ][kSpRC]) {
   const T* zrows = spill ? m.wzn : m.wzo;
-  for (int a = a0; a < a1; ++a) {
-    const int zi = m.zi[a];
-    if ((zi & ~kZiSpill) != zsrc || (spill && !(zi & kZiSpill))) continue;
+  int a = a0;
+  for (; a + 4 <= a1; a += 4) {
+    T wxy[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) wxy[u] = m.wx[(size_t)(a + u) * 16 + lx] * m.wy[(size_t)(a + u) * 16 + ly];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      if (wxy[u] != T(0)) col_atom<T, CHECK>(m, zrows, a + u, wxy[u], zsrc, R, r0, acc);
+  }
+  for (; a < a1; ++a) {
     const T wxy = m.wx[(size_t)a * 16 + lx] * m.wy[(size_t)a * 16 + ly];
-    if (wxy != T(0)) {
-      T cr[kSpRC];
-#pragma unroll
-      for (int r = 0; r < kSpRC; ++r) cr[r] = r0 + r < R ? wxy * m.cc[(size_t)a * R + r0 + r] : T(0);
-      const T* zr = zrows + (size_t)a * kSpTZ;
-#pragma unroll
-      for (int z = 0; z < kSpTZ; ++z) {
-        const T wz = zr[z];
-#pragma unroll
-        for (int r = 0; r < kSpRC; ++r) acc[z][r] += wz * cr[r];
-      }
-    }
+    if (wxy != T(0)) col_atom<T, CHECK>(m, zrows, a, wxy, zsrc, R, r0, acc);
   }
 }
 
@@ -571,8 +594,8 @@ __global__ void __launch_bounds__(kSpThreads, sizeof(T) == 8 ? 2 : 3) k_spread_c
         for (int z = 0; z < kSpTZ; ++z)
 #pragma unroll
           for (int r = 0; r < kSpRC; ++r) acc[z][r] = T(0);
-        col_accumulate<T>(m, m.zst[zprev], m.zst[zprev + 1], zprev, true, g.R, r0, lx, ly, acc);
-        col_accumulate<T>(m, m.zst[zown], m.zst[zown + 1], zown, false, g.R, r0, lx, ly, acc);
+        col_accumulate<T, false>(m, m.zst[zprev], m.zst[zprev + 1], zprev, true, g.R, r0, lx, ly, acc);
+        col_accumulate<T, false>(m, m.zst[zown], m.zst[zown + 1], zown, false, g.R, r0, lx, ly, acc);
         col_store<T>(g, X, r0, t0, tzt, lx, ly, acc, rho);
       }
     }
@@ -592,8 +615,8 @@ __global__ void __launch_bounds__(kSpThreads, sizeof(T) == 8 ? 2 : 3) k_spread_c
       while (from < total) {
         const int st = col_stage<T, P>(g, s_a0, s_pref, nseg, spz, total, from, t0, tzt, cap, rb, rw, rc, m,
                                        s_wcnt, &s_next, &from);
-        col_accumulate<T>(m, 0, st, zprev, true, g.R, r0, lx, ly, acc);
-        col_accumulate<T>(m, 0, st, zown, false, g.R, r0, lx, ly, acc);
+        col_accumulate<T, true>(m, 0, st, zprev, true, g.R, r0, lx, ly, acc);
+        col_accumulate<T, true>(m, 0, st, zown, false, g.R, r0, lx, ly, acc);
         __syncthreads();
       }
       col_store<T>(g, X, r0, t0, tzt, lx, ly, acc, rho);

@@ -19,7 +19,6 @@ struct fd3_plan {
   double* d_eigvecs = nullptr;
   GreenPair* d_green = nullptr;
   GreenPairF* d_green_f = nullptr;
-  float4* d_green_f4 = nullptr;   // {R, s6 c6pre, 3 s8 qq c8pre, 0}: folded mixed-form constants
   float* d_deconv = nullptr;
   cufftHandle fwd = 0, inv = 0;
   bool has_fft = false;
@@ -161,17 +160,12 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
   for (int k = 0; k < S * S; ++k)
     gpf[k] = GreenPairF{(float)gp[k].R, (float)gp[k].qq, (float)gp[k].c6s1, (float)gp[k].c6s2, (float)gp[k].c6pre,
                         (float)gp[k].c8s1, (float)gp[k].c8s2, (float)gp[k].c8pre};
-  float4* gf4 = new float4[S * S];
-  for (int k = 0; k < S * S; ++k)
-    gf4[k] = make_float4((float)gp[k].R, (float)(t.s6 * gp[k].c6pre), (float)(3.0 * t.s8 * gp[k].qq * gp[k].c8pre),
-                         0.f);
   int rc = FD3_OK;
   do {
     if (cudaMalloc(&p->d_tab, sizeof(Tables)) != cudaSuccess ||
         cudaMalloc(&p->d_eigvecs, sizeof(double) * S * 7 * R) != cudaSuccess ||
         cudaMalloc(&p->d_green, sizeof(GreenPair) * S * S) != cudaSuccess ||
-        cudaMalloc(&p->d_green_f, sizeof(GreenPairF) * S * S) != cudaSuccess ||
-        cudaMalloc(&p->d_green_f4, sizeof(float4) * S * S) != cudaSuccess) {
+        cudaMalloc(&p->d_green_f, sizeof(GreenPairF) * S * S) != cudaSuccess) {
       set_error("fd3_plan_create", "cudaMalloc of the species tables failed");
       rc = FD3_ECUDA;
       break;
@@ -179,8 +173,7 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
     if (cudaMemcpy(p->d_tab, &t, sizeof(Tables), cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(p->d_eigvecs, d->eigvecs, sizeof(double) * S * 7 * R, cudaMemcpyHostToDevice) != cudaSuccess ||
         cudaMemcpy(p->d_green, gp, sizeof(GreenPair) * S * S, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(p->d_green_f, gpf, sizeof(GreenPairF) * S * S, cudaMemcpyHostToDevice) != cudaSuccess ||
-        cudaMemcpy(p->d_green_f4, gf4, sizeof(float4) * S * S, cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaMemcpy(p->d_green_f, gpf, sizeof(GreenPairF) * S * S, cudaMemcpyHostToDevice) != cudaSuccess) {
       set_error("fd3_plan_create", "upload of the species tables failed");
       rc = FD3_ECUDA;
       break;
@@ -239,7 +232,6 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
   } while (0);
   delete[] gp;
   delete[] gpf;
-  delete[] gf4;
   if (rc) {
     fd3_plan_destroy(p);
     return rc;
@@ -312,7 +304,6 @@ extern "C" int fd3_plan_destroy(fd3_plan* p) {
   cudaFree(p->d_eigvecs);
   cudaFree(p->d_green);
   cudaFree(p->d_green_f);
-  cudaFree(p->d_green_f4);
   cudaFree(p->d_deconv);
   delete p;
   return FD3_OK;
@@ -342,6 +333,7 @@ struct Work {
   HitStore hits;
   EwaldWork ew;
   void *rho, *spec, *fftw;
+  void* gtab;   // mixed-form Green table
 };
 
 // K = number of cell-list bins of the fused path, 0 for the edge-list path (no cell list).
@@ -401,6 +393,7 @@ void carve(const fd3_plan* p, int64_t N, int64_t K_in, Carver& c, Work& w) {
   w.rho = c.take<char>(mesh ? C * M * es : 1);
   w.spec = c.take<char>(mesh ? C * Mh * 2 * es : 1);
   w.fftw = c.take<char>(p->fft_ws);
+  w.gtab = c.take<char>(mesh && p->precision == FD3_PREC_MIXED ? green_table_bytes(p->S) : 1);
   // direct Ewald sum
   if (!mesh) {
     const int64_t nk = (int64_t)p->ens[0] * p->ens[1] * p->ens[2];
@@ -472,7 +465,8 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
     FD3_CUFFT(cufftExecR2C(p->fwd, (cufftReal*)w.rho, (cufftComplex*)w.spec));
   prof_mark(p, s, "fft_r2c");
   void* hspec = w.spec;   // the filter overwrites the spectrum with H in place
-  FD3_TRY(launch_filter<T>(mg, w.ci, p->d_green, p->d_green_f, p->d_green_f4, p->d_tab, p->d_deconv, p->method == FD3_METHOD_SPME, w.spec,
+  if (sizeof(T) == 4) FD3_TRY(launch_green_table(mg, w.ci, p->d_green, p->d_tab, w.gtab, s));
+  FD3_TRY(launch_filter<T>(mg, w.ci, p->d_green, p->d_green_f, (const float4*)w.gtab, p->d_tab, p->d_deconv, p->method == FD3_METHOD_SPME, w.spec,
                            w.kspc_part, n_kspc, s));
   prof_mark(p, s, "filter");
   *n_mcell = 0;

@@ -124,12 +124,29 @@ __global__ void __launch_bounds__(256) k_scatter(const int* __restrict__ keys, i
   }
 }
 
-// Insertion sort of each key segment by atom id: makes the order (and every sum taken in
-// that order) independent of the atomic slot assignment above.
+// Sort each key segment by atom id: makes the order (and every sum taken in that order)
+// independent of the atomic slot assignment above. One warp per segment: a segment of at most
+// 32 ids is ranked in registers (rank = number of smaller ids, the ids being distinct) and
+// written back in one step; a longer one is insertion-sorted by lane 0.
 __global__ void __launch_bounds__(256) k_sort_segments(const int* __restrict__ starts, int K, int* __restrict__ order) {
-  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  const int k = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (k >= K) return;
-  const int a = starts[k], b = starts[k + 1];
+  const int a = starts[k], b = starts[k + 1], m = b - a;
+  if (m <= 1) return;
+  if (m <= 32) {
+    const int v = lane < m ? order[a + lane] : 0x7fffffff;
+    int rank = 0;
+#pragma unroll 8
+    for (int j = 0; j < 32; ++j) {
+      const int u = __shfl_sync(0xffffffffu, v, j);
+      rank += (j < m && u < v) ? 1 : 0;
+    }
+    __syncwarp();
+    if (lane < m) order[a + rank] = v;
+    return;
+  }
+  if (lane != 0) return;
   for (int u = a + 1; u < b; ++u) {
     const int v = order[u];
     int w = u - 1;
@@ -155,7 +172,7 @@ int counting_sort(const int* keys, int n, int K, int* counts, int* starts, int* 
     k_scatter<<<(n + tb - 1) / tb, tb, 0, s>>>(keys, n, starts, counts, order);
     FD3_LAUNCHED();
   }
-  k_sort_segments<<<(K + tb - 1) / tb, tb, 0, s>>>(starts, K, order);
+  k_sort_segments<<<(K + tb / 32 - 1) / (tb / 32), tb, 0, s>>>(starts, K, order);
   FD3_LAUNCHED();
   return FD3_OK;
 }

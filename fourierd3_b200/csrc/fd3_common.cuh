@@ -272,29 +272,57 @@ __device__ __forceinline__ void green_eval(const GP& g, T k, T s6, T s8, T& G, T
   dG = d6 + T(g.qq) * d8;
 }
 
-// Mixed-form Green's function for the tiled filter: the same closed form as green_eval with the
-// pair constants folded, g = {R, A6 = s6 c6pre, A8 = 3 s8 qq c8pre, unused}, and 1/k given.
-//   G = (A6 n6(u) + A8 n8(u)) / k,   dG/dk = (R (A6 n6'(u) + A8 n8'(u)) - G) / k,   u = k R,
-// which is f6 + qq f8 and d6 + qq d8 of green_eval regrouped. The k R < 1e-15 (Taylor) branch is
-// left to green_eval on the full constants.
-__device__ __forceinline__ void green_eval_folded(float4 g, float k, float invk, float& G, float& dG) {
-  const float R = g.x, A6 = g.y, A8 = g.z;
-  const float u = k * R;
-  const float e2 = __expf(-u * 0.5f);
-  const float e1 = e2 * e2;
-  float sa, ca;
-  sincospi_t(1.0f / 3.0f + u * 0.27566444771089604f, &sa, &ca);
-  const float n6 = e1 - 2.0f * e2 * ca;
-  const float dn6 = -e1 + e2 * ca + 1.7320508075688772935f * e2 * sa;
-  const float e3 = __expf(-u * 0.38268343236508977173f);
-  const float e4 = __expf(-u * 0.92387953251128675613f);
-  float s1, c1, s2, c2;
-  sincospi_t(0.25f + u * 0.29407998884120140f, &s1, &c1);
-  sincospi_t(0.75f + u * 0.12181191980055409f, &s2, &c2);
-  const float n8 = e3 * c1 + e4 * c2;
-  const float dn8 = -0.38268343236508977173f * (e3 * c1 + e4 * s2) - 0.92387953251128675613f * (e3 * s1 + e4 * c2);
-  G = invk * (A6 * n6 + A8 * n8);
-  dG = invk * (R * (A6 * dn6 + A8 * dn8) - G);
+// ---------------------------------------------------------------- Green's function table
+// Mixed form: G_XY(|k|) and dG/d|k| from a per-call table on kGreenKnots intervals of
+// [0, kmax], kmax = sum_a (n_a / 2) |b_a| >= every mesh |k|. Knot j of pair p holds, in float,
+// {G, h G', h^2 G''} (h = kmax / kGreenKnots) computed in float64 from the closed form
+//   G = F(kR) / k, G' = (R F'(kR) - G) / k, G'' = (R^2 F''(kR) - 2 G') / k,
+//   F = s6 c6pre n6 + 3 s8 qq c8pre n8,
+// (the Taylor limit at k = 0); G and G' between knots are cubic Hermite interpolants (of G with
+// slopes G', and of G' with slopes G''), relative error ~ (h R)^4 / 384, below float rounding.
+constexpr int kGreenKnots = 2048;
+
+__host__ __device__ inline double green_kmax(const double (&recip)[9], const int (&n)[3]) {
+  double k = 0.0;
+  for (int a = 0; a < 3; ++a)
+    k += 0.5 * n[a] * sqrt(recip[3 * a] * recip[3 * a] + recip[3 * a + 1] * recip[3 * a + 1] +
+                           recip[3 * a + 2] * recip[3 * a + 2]);
+  return k;
+}
+
+// n6, n8 and their first two u-derivatives (float64)
+__device__ inline void green_n(double u, double* n6, double* d6, double* e6, double* n8, double* d8, double* e8) {
+  const double sq3 = 1.7320508075688772935, sin8 = 0.38268343236508977173, cos8 = 0.92387953251128675613;
+  const double e2 = exp(-0.5 * u), e1 = e2 * e2;
+  double sa, ca;
+  sincospi(1.0 / 3.0 + u * 0.27566444771089604, &sa, &ca);
+  *n6 = e1 - 2.0 * e2 * ca;
+  *d6 = -e1 + e2 * ca + sq3 * e2 * sa;
+  *e6 = e1 + e2 * ca - sq3 * e2 * sa;
+  const double e3 = exp(-u * sin8), e4 = exp(-u * cos8);
+  double s1, c1, s2, c2;
+  sincospi(0.25 + u * 0.29407998884120140, &s1, &c1);
+  sincospi(0.75 + u * 0.12181191980055409, &s2, &c2);
+  *n8 = e3 * c1 + e4 * c2;
+  *d8 = -sin8 * e3 * c1 - cos8 * e3 * s1 - cos8 * e4 * c2 - sin8 * e4 * s2;
+  *e8 = 0.70710678118654752440 * (-e3 * c1 + e3 * s1 + e4 * c2 + e4 * s2);
+}
+
+// Hermite basis of the fractional position f in a table interval.
+struct HermiteF {
+  float h00, h10, h01, h11;
+};
+__device__ __forceinline__ HermiteF hermite_basis(float f) {
+  const float g = 1.0f - f;
+  return HermiteF{(1.0f + 2.0f * f) * g * g, f * g * g, f * f * (3.0f - 2.0f * f), f * f * (f - 1.0f)};
+}
+
+// G and dG/dk of one pair from its table row at interval j (basis hb, 1/h = inv_h).
+__device__ __forceinline__ void green_lookup(const float4* __restrict__ row, int j, const HermiteF& hb, float inv_h,
+                                             float& G, float& dG) {
+  const float4 a = row[j], b = row[j + 1];
+  G = hb.h00 * a.x + hb.h10 * a.y + hb.h01 * b.x + hb.h11 * b.y;
+  dG = (hb.h00 * a.y + hb.h10 * a.z + hb.h01 * b.y + hb.h11 * b.z) * inv_h;
 }
 
 // Division of 32-bit unsigned values by a runtime-invariant divisor (round-up multiplier method):

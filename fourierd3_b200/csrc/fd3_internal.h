@@ -131,8 +131,12 @@ int launch_spread(const MeshGeom& mg, int n, const double* pos, double pos_scale
                   const MeshRecords& rec, T* rho, cudaStream_t s);
 template <typename T>
 int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const GreenPairF* gpf,
-                  const float4* g4, const Tables* tab, const float* deconv, int spme, void* spec, double* part,
+                  const float4* gtab, const Tables* tab, const float* deconv, int spme, void* spec, double* part,
                   int* n_blocks, cudaStream_t s);
+// mixed form: per-call table of G and its k-derivatives per species pair (gtab of the filter)
+int launch_green_table(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab, void* table,
+                       cudaStream_t s);
+size_t green_table_bytes(int S);
 int filter_max_blocks();
 int filter_default_kt(int S, int R, size_t tsize);
 int spread_chunk_in_effect(const MeshGeom& mg, size_t tsize);

@@ -70,6 +70,71 @@ int launch_mesh_keys(const MeshGeom& mg, int n, const double* pos, double pos_sc
   return FD3_OK;
 }
 
+// ------------------------------------------------------------------ Green table (mixed form)
+// Thread per (pair X <= Y, knot j); pair index X S - X (X - 1) / 2 + (Y - X).
+__global__ void __launch_bounds__(256) k_green_table(MeshDev g, const CellInfo* __restrict__ ci,
+                                                     const GreenPair* __restrict__ gp,
+                                                     const Tables* __restrict__ tab, float4* __restrict__ out) {
+  const int S = g.S, NP = S * (S + 1) / 2;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= NP * (kGreenKnots + 1)) return;
+  const int pi = e / (kGreenKnots + 1), j = e - pi * (kGreenKnots + 1);
+  int X = 0;
+  while ((X + 1) * S - (X + 1) * X / 2 <= pi) ++X;
+  const int Y = X + (pi - (X * S - X * (X - 1) / 2));
+  const GreenPair& q = gp[X * S + Y];
+  double rec[9];
+  for (int c = 0; c < 9; ++c) rec[c] = ci->recip[c];
+  const int n[3] = {g.n[0], g.n[1], g.n[2]};
+  const double h = green_kmax(rec, n) / kGreenKnots;
+  const double k = j * h;
+  const double s6 = tab->s6, s8 = tab->s8;
+  const double A6 = s6 * q.c6pre, A8 = 3.0 * s8 * q.qq * q.c8pre;
+  double G, G1, G2;
+  if (k * q.R < 1e-15) {
+    // Taylor limit (pair_pot.py: the kR < thresh branch): G = a - b k^2
+    const double a = s6 * q.c6s1 + 3.0 * s8 * q.qq * q.c8s1, b = s6 * q.c6s2 + 3.0 * s8 * q.qq * q.c8s2;
+    G = a - b * k * k;
+    G1 = -2.0 * b * k;
+    G2 = -2.0 * b;
+  } else {
+    double n6, d6, e6, n8, d8, e8;
+    green_n(k * q.R, &n6, &d6, &e6, &n8, &d8, &e8);
+    const double F = A6 * n6 + A8 * n8, F1 = A6 * d6 + A8 * d8, F2 = A6 * e6 + A8 * e8;
+    G = F / k;
+    G1 = (q.R * F1 - G) / k;
+    G2 = (q.R * q.R * F2 - 2.0 * G1) / k;
+  }
+  out[e] = make_float4((float)G, (float)(h * G1), (float)(h * h * G2), 0.f);
+}
+
+int launch_green_table(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab,
+                       void* table, cudaStream_t s) {
+  const int NP = mg.S * (mg.S + 1) / 2;
+  const int total = NP * (kGreenKnots + 1);
+  k_green_table<<<(total + 255) / 256, 256, 0, s>>>(to_dev(mg), ci, gp, tab, reinterpret_cast<float4*>(table));
+  FD3_LAUNCHED();
+  return FD3_OK;
+}
+
+size_t green_table_bytes(int S) { return (size_t)S * (S + 1) / 2 * (kGreenKnots + 1) * sizeof(float4); }
+
+// 1 / h of the table for this cell and mesh, in float, the same in every kernel that reads it
+__device__ __forceinline__ float green_inv_h(const MeshDev& g, const CellInfo* __restrict__ ci) {
+  double rec[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) rec[c] = ci->recip[c];
+  const int n[3] = {g.n[0], g.n[1], g.n[2]};
+  return (float)(kGreenKnots / green_kmax(rec, n));
+}
+
+__device__ __forceinline__ void table_pos(float k, float inv_h, int& j, HermiteF& hb) {
+  const float t = k * inv_h;
+  j = (int)t;
+  if (j > kGreenKnots - 1) j = kGreenKnots - 1;
+  hb = hermite_basis(t - (float)j);
+}
+
 // ------------------------------------------------------------------ filter
 template <typename T> struct Cplx;
 template <> struct Cplx<double> { using type = double2; };
@@ -175,7 +240,7 @@ template <typename T, int MAXS, int MAXR>
 __global__ void __launch_bounds__(kFilterThreads, sizeof(T) == 8 ? 2 : (MAXS <= 2 ? 3 : 1)) k_filter(MeshDev g, int P, int spme,
                                                            const CellInfo* __restrict__ ci,
                                                            const typename GreenPairOf<T>::type* __restrict__ gp,
-                                                           const float4* __restrict__ g4,
+                                                           const float4* __restrict__ gtab,
                                                            const Tables* __restrict__ tab,
                                                            const float* __restrict__ deconv,
                                                            typename Cplx<T>::type* __restrict__ spec,
@@ -187,9 +252,13 @@ __global__ void __launch_bounds__(kFilterThreads, sizeof(T) == 8 ? 2 : (MAXS <= 
   const T s6 = (T)tab->s6, s8 = (T)tab->s8;
   T rc[9];
   load_recip<T>(ci, rc);
+  float inv_h = 0.f;
+  if constexpr (sizeof(T) == 4) inv_h = green_inv_h(g, ci);
   for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < Mh; k += (size_t)gridDim.x * blockDim.x) {
     const KPoint<T> q = kpoint<T>(g, k, rc, deconv, spme, P);
-    const T invk = q.knorm > T(0) ? T(1) / q.knorm : T(0);
+    int tj = 0;
+    HermiteF hb{};
+    if constexpr (sizeof(T) == 4) table_pos(q.knorm, inv_h, tj, hb);
     T G[MAXS][MAXS], dG[MAXS][MAXS], Gh[MAXS][MAXS];
 #pragma unroll
     for (int X = 0; X < MAXS; ++X)
@@ -198,11 +267,8 @@ __global__ void __launch_bounds__(kFilterThreads, sizeof(T) == 8 ? 2 : (MAXS <= 
         T gv = T(0), dv = T(0);
         if (X < S && Y < S) {
           if constexpr (sizeof(T) == 4) {
-            const float4 c4 = g4[X * S + Y];
-            if (q.knorm * c4.x < 1e-15f)
-              green_eval<T>(gp[X * S + Y], q.knorm, s6, s8, gv, dv);
-            else
-              green_eval_folded(c4, q.knorm, invk, gv, dv);
+            const int pi = X * S - X * (X - 1) / 2 + (Y - X);
+            green_lookup(gtab + (size_t)pi * (kGreenKnots + 1), tj, hb, inv_h, gv, dv);
           } else {
             green_eval<T>(gp[X * S + Y], q.knorm, s6, s8, gv, dv);
           }
@@ -214,13 +280,21 @@ __global__ void __launch_bounds__(kFilterThreads, sizeof(T) == 8 ? 2 : (MAXS <= 
         Gh[X][Y] = Gh[Y][X] = gv;
       }
     if (q.partner) {
+      int pj = 0;
+      HermiteF pb{};
+      if constexpr (sizeof(T) == 4) table_pos(q.kpart, inv_h, pj, pb);
 #pragma unroll
       for (int X = 0; X < MAXS; ++X)
 #pragma unroll
         for (int Y = X; Y < MAXS; ++Y)
           if (X < S && Y < S) {
             T gv, dv;
-            green_eval<T>(gp[X * S + Y], q.kpart, s6, s8, gv, dv);
+            if constexpr (sizeof(T) == 4) {
+              const int pi = X * S - X * (X - 1) / 2 + (Y - X);
+              green_lookup(gtab + (size_t)pi * (kGreenKnots + 1), pj, pb, inv_h, gv, dv);
+            } else {
+              green_eval<T>(gp[X * S + Y], q.kpart, s6, s8, gv, dv);
+            }
             Gh[X][Y] = Gh[Y][X] = T(0.5) * (G[X][Y] + gv * q.inv_sc);
           }
     }
@@ -296,7 +370,7 @@ template <typename T, int KT>
 __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int P, int spme, int n_units,
                                                                  const CellInfo* __restrict__ ci,
                                                                  const typename GreenPairOf<T>::type* __restrict__ gp,
-                                                                 const float4* __restrict__ g4,
+                                                                 const float4* __restrict__ gtab,
                                                                  const Tables* __restrict__ tab,
                                                                  const float* __restrict__ deconv,
                                                                  typename Cplx<T>::type* __restrict__ spec,
@@ -326,6 +400,8 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
   const T s6 = (T)tab->s6, s8 = (T)tab->s8;
   T rc[9];
   load_recip<T>(ci, rc);
+  float inv_h = 0.f;
+  if constexpr (sizeof(T) == 4) inv_h = green_inv_h(g, ci);
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   for (size_t tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
     const size_t k0 = tile * KT;
@@ -338,8 +414,12 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
     const size_t k = k0 + kk;
     const bool valid = k < Mh;
     const KPoint<T> q = kpoint<T>(g, valid ? k : 0, rc, deconv, spme, P);
-    const T invk = q.knorm > T(0) ? T(1) / q.knorm : T(0);
-    const T invkp = q.kpart > T(0) ? T(1) / q.kpart : T(0);
+    int tj = 0, pj = 0;
+    HermiteF hb{}, pb{};
+    if constexpr (sizeof(T) == 4) {
+      table_pos(q.knorm, inv_h, tj, hb);
+      table_pos(q.kpart, inv_h, pj, pb);
+    }
     __syncthreads();
     T qq = T(0), dq = T(0);
     for (int u = slot; u < n_units; u += NSLOT) {
@@ -347,12 +427,6 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
       const int X = (int)(xy >> 16), Y0 = (int)(xy & 0xffffu);
       const int ya = X > Y0 ? X : Y0;
       const int yb = Y0 + kUnitY < S ? Y0 + kUnitY : S;
-      // mixed form: the unit's folded pair constants are requested before the rank loop
-      float4 gq[kUnitY];
-      if constexpr (sizeof(T) == 4) {
-#pragma unroll
-        for (int y = 0; y < kUnitY; ++y) gq[y] = Y0 + y < yb ? g4[X * S + Y0 + y] : make_float4(0.f, 0.f, 0.f, 0.f);
-      }
       T pr[kUnitY];
 #pragma unroll
       for (int y = 0; y < kUnitY; ++y) pr[y] = T(0);
@@ -387,33 +461,26 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
         const int Y = Y0 + y;
         if (Y >= ya && Y < yb) {
           T gv, dv;
-          if constexpr (sizeof(T) == 4) {
-            if (q.knorm * gq[y].x < 1e-15f)
-              green_eval<T>(gp[X * S + Y], q.knorm, s6, s8, gv, dv);
-            else
-              green_eval_folded(gq[y], q.knorm, invk, gv, dv);
-          } else {
+          const int pi = row0[X] + (Y - X);
+          if constexpr (sizeof(T) == 4)
+            green_lookup(gtab + (size_t)pi * (kGreenKnots + 1), tj, hb, inv_h, gv, dv);
+          else
             green_eval<T>(gp[X * S + Y], q.knorm, s6, s8, gv, dv);
-          }
           gv *= q.inv_sc;
           dv *= q.inv_sc;
           T gh = gv;
           if (q.partner) {
             T gpv, dpv;
-            if constexpr (sizeof(T) == 4) {
-              if (q.kpart * gq[y].x < 1e-15f)
-                green_eval<T>(gp[X * S + Y], q.kpart, s6, s8, gpv, dpv);
-              else
-                green_eval_folded(gq[y], q.kpart, invkp, gpv, dpv);
-            } else {
+            if constexpr (sizeof(T) == 4)
+              green_lookup(gtab + (size_t)pi * (kGreenKnots + 1), pj, pb, inv_h, gpv, dpv);
+            else
               green_eval<T>(gp[X * S + Y], q.kpart, s6, s8, gpv, dpv);
-            }
             gh = T(0.5) * (gv + gpv * q.inv_sc);
           }
           const T w = X == Y ? T(1) : T(2);
           qq += w * gv * pr[y];
           dq += w * dv * pr[y];
-          gs[(row0[X] + (Y - X)) * KT + kk] = gh;
+          gs[pi * KT + kk] = gh;
         }
       }
     }
@@ -490,7 +557,7 @@ bool filter_kt_valid(int kt, int S, int R, size_t tsize) {
 
 template <typename T, int KT>
 static int launch_tiled(const MeshDev& g, const MeshGeom& mg, const CellInfo* ci,
-                        const typename GreenPairOf<T>::type* gp, const float4* g4, const Tables* tab,
+                        const typename GreenPairOf<T>::type* gp, const float4* gtab, const Tables* tab,
                         const float* deconv, int spme, typename Cplx<T>::type* sp, double* part, int* n_blocks,
                         cudaStream_t s) {
   const size_t smem = FilterTileSmem::bytes(mg.S, mg.R, KT, sizeof(T));
@@ -525,14 +592,14 @@ static int launch_tiled(const MeshDev& g, const MeshGeom& mg, const CellInfo* ci
   if (blocks > (size_t)filter_max_blocks()) blocks = filter_max_blocks();
   *n_blocks = (int)blocks;
   k_filter_tiled<T, KT><<<(int)blocks, kFilterThreads, smem, s>>>(g, mg.order, spme, filter_units(mg.S), ci, gp,
-                                                                  g4, tab, deconv, sp, part);
+                                                                  gtab, tab, deconv, sp, part);
   FD3_LAUNCHED();
   return FD3_OK;
 }
 
 template <typename T>
 int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const GreenPairF* gpf,
-                  const float4* g4, const Tables* tab, const float* deconv, int spme, void* spec, double* part,
+                  const float4* gtab, const Tables* tab, const float* deconv, int spme, void* spec, double* part,
                   int* n_blocks, cudaStream_t s) {
   using C2 = typename Cplx<T>::type;
   using GP = typename GreenPairOf<T>::type;
@@ -545,7 +612,7 @@ int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, c
     const int blocks = filter_grid(Mh);
     *n_blocks = blocks;
 #define FD3_FILTER(SS, RR) \
-  k_filter<T, SS, RR><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gpt, g4, tab, deconv, sp, part)
+  k_filter<T, SS, RR><<<blocks, kFilterThreads, 0, s>>>(g, mg.order, spme, ci, gpt, gtab, tab, deconv, sp, part)
     if (mg.S <= 1)
       FD3_FILTER(1, 4);
     else if (mg.S <= 2 && mg.R <= 4)
@@ -563,11 +630,11 @@ int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, c
     return FD3_OK;
   }
   switch (kt) {
-    case 16: return launch_tiled<T, 16>(g, mg, ci, gpt, g4, tab, deconv, spme, sp, part, n_blocks, s);
-    case 8: return launch_tiled<T, 8>(g, mg, ci, gpt, g4, tab, deconv, spme, sp, part, n_blocks, s);
-    case 4: return launch_tiled<T, 4>(g, mg, ci, gpt, g4, tab, deconv, spme, sp, part, n_blocks, s);
-    case 2: return launch_tiled<T, 2>(g, mg, ci, gpt, g4, tab, deconv, spme, sp, part, n_blocks, s);
-    default: return launch_tiled<T, 1>(g, mg, ci, gpt, g4, tab, deconv, spme, sp, part, n_blocks, s);
+    case 16: return launch_tiled<T, 16>(g, mg, ci, gpt, gtab, tab, deconv, spme, sp, part, n_blocks, s);
+    case 8: return launch_tiled<T, 8>(g, mg, ci, gpt, gtab, tab, deconv, spme, sp, part, n_blocks, s);
+    case 4: return launch_tiled<T, 4>(g, mg, ci, gpt, gtab, tab, deconv, spme, sp, part, n_blocks, s);
+    case 2: return launch_tiled<T, 2>(g, mg, ci, gpt, gtab, tab, deconv, spme, sp, part, n_blocks, s);
+    default: return launch_tiled<T, 1>(g, mg, ci, gpt, gtab, tab, deconv, spme, sp, part, n_blocks, s);
   }
 }
 template int launch_filter<double>(const MeshGeom&, const CellInfo*, const GreenPair*, const GreenPairF*,

@@ -44,7 +44,7 @@ def parse():
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
                     help="'both' times plain fp64 and mixed (headline); one value restricts the run")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="sio2", choices=["sio2", "batch"],
+    ap.add_argument("--workload", default="sio2", choices=["sio2", "batch", "accuracy"],
                     help="'sio2': the 139,968-atom box (headline); 'batch': 256 structures, 32-4,096 atoms, "
                          "Z 1-54, graph-captured lanes vs per-structure launches")
     ap.add_argument("--batch-size", type=int, default=256)
@@ -223,6 +223,49 @@ def run_reference(args, ws, rank):
 BATCH_WORKLOAD = "batch256_N32-4096_Z1-54_spme_p5_h1.2_E+F+stress"
 
 
+def run_accuracy(args, ws, rank, local):
+    """Precision scaling: the seeded SiO2 box replicated 1^3..6^3 (648..139,968 atoms, jitter
+    N(0, 0.05 A)); plain float64 SPME and the mixed form against the float64 direct pairwise D3
+    lattice sum (committed fixtures, up to 5,184 atoms) and the mixed form against float64 SPME
+    at every size. One JSON line per size; energies in eV, forces eV/A, stress eV/A^3."""
+    if rank != 0:
+        return
+    from fourierd3_b200 import structures as st
+    from fourierd3_b200.functional import D3Model
+
+    device = torch.device("cuda", local)
+    kw = dict(method="spme", mesh_spacing=1.2, interpolation_nodes=5, c6tol=1.0, r_cut=6.0)
+    golden = os.path.join(REPO, "tests", "golden")
+    for reps in range(1, 7):
+        pos, cell, nums = st.sio2_scaled(reps)
+        path = os.path.join(golden, f"direct_sio2_{len(nums)}.npz")
+        d = np.load(path) if os.path.exists(path) else None
+        if d is not None:   # the direct-sum fixture's own structure (648: the box before jitter)
+            pos, cell, nums = d["positions"], d["cell"], d["numbers"]
+        res = {}
+        for prec in ("fp64", "mixed"):
+            m = D3Model(nums, cell, precision=prec, device=device, **kw)
+            e, f, s = m(pos, cell)
+            res[prec] = (float(e), f.cpu().numpy(), s.cpu().numpy())
+            del m
+            torch.cuda.empty_cache()
+        e64, f64, s64 = res["fp64"]
+        e32, f32, s32 = res["mixed"]
+        line = {"workload": "accuracy_sio2_scaling", "n_atoms": len(nums), "reps": reps,
+                "energy_ev_fp64": e64,
+                "mixed_vs_fp64": {"energy_rel": abs(e32 - e64) / abs(e64),
+                                  "force_max_ev_a": float(np.abs(f32 - f64).max()),
+                                  "stress_max_ev_a3": float(np.abs(s32 - s64).max())}}
+        if d is not None:
+            for prec in ("fp64", "mixed"):
+                e, f, s = res[prec]
+                line[f"{prec}_vs_direct_sum"] = {
+                    "energy_rel": abs(e - float(d["energy_ev"])) / abs(float(d["energy_ev"])),
+                    "force_max_ev_a": float(np.abs(f - d["forces"]).max()),
+                    "stress_max_ev_a3": float(np.abs(s - d["stress"]).max())}
+        print(json.dumps(line), flush=True)
+
+
 def run_batch(args, ws, rank, local):
     """Batch workload: structures sharded over ranks (LPT on N + M*S*r), one graph per rank."""
     from fourierd3_b200 import _native, structures as st
@@ -339,6 +382,13 @@ def main():
     ws, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, ws, rank)
+        if ws > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+    if args.workload == "accuracy":
+        run_accuracy(args, ws, rank, local)
         if ws > 1:
             import torch.distributed as dist
 

@@ -427,6 +427,21 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
       const int X = (int)(xy >> 16), Y0 = (int)(xy & 0xffffu);
       const int ya = X > Y0 ? X : Y0;
       const int yb = Y0 + kUnitY < S ? Y0 + kUnitY : S;
+      // mixed form: the unit's Green-table rows are requested before the rank loop
+      float4 ta[kUnitY], tb[kUnitY];
+      if constexpr (sizeof(T) == 4) {
+#pragma unroll
+        for (int y = 0; y < kUnitY; ++y) {
+          const int Y = Y0 + y;
+          if (Y >= ya && Y < yb) {
+            const float4* row = gtab + (size_t)(row0[X] + (Y - X)) * (kGreenKnots + 1);
+            ta[y] = row[tj];
+            tb[y] = row[tj + 1];
+          } else {
+            ta[y] = tb[y] = make_float4(0.f, 0.f, 0.f, 0.f);
+          }
+        }
+      }
       T pr[kUnitY];
 #pragma unroll
       for (int y = 0; y < kUnitY; ++y) pr[y] = T(0);
@@ -462,10 +477,12 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
         if (Y >= ya && Y < yb) {
           T gv, dv;
           const int pi = row0[X] + (Y - X);
-          if constexpr (sizeof(T) == 4)
-            green_lookup(gtab + (size_t)pi * (kGreenKnots + 1), tj, hb, inv_h, gv, dv);
-          else
+          if constexpr (sizeof(T) == 4) {
+            gv = hb.h00 * ta[y].x + hb.h10 * ta[y].y + hb.h01 * tb[y].x + hb.h11 * tb[y].y;
+            dv = (hb.h00 * ta[y].y + hb.h10 * ta[y].z + hb.h01 * tb[y].y + hb.h11 * tb[y].z) * inv_h;
+          } else {
             green_eval<T>(gp[X * S + Y], q.knorm, s6, s8, gv, dv);
+          }
           gv *= q.inv_sc;
           dv *= q.inv_sc;
           T gh = gv;

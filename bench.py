@@ -476,8 +476,15 @@ def main():
     peak, peak_kind = measured_peaks()
     dom_bytes = stage_bytes(dom, n, mesh, C, R, b)
     achieved = dom_bytes / (ours[dom] * 1e-3) / 1e9
+    # DRAM bytes (read + write) per launch from one ncu capture of the same 256^3 x 8-channel
+    # mixed mesh (profiles/kernels_sio2_41472_mixed.md); mesh-side traffic does not depend on N
+    traffic_by_stage = {"filter": (575.1e6 + 484.0e6), "spread": (11.1e6 + 486.3e6)}
+    mesh_match = tuple(mesh) == (256, 256, 256) and C == 8 and head == "mixed"
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
-            "unit": "GB/s", "frac": achieved / peak, "traffic": None,
+            "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic_by_stage.get(dom) if mesh_match else None,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, 256^3 x 8 channels, mixed"
+                              if mesh_match and dom in traffic_by_stage else None,
             "bytes_per_launch": dom_bytes, "ms_per_launch": ours[dom]}
 
     cpu = None

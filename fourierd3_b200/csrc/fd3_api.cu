@@ -22,6 +22,8 @@ struct fd3_plan {
   float* d_deconv = nullptr;
   cufftHandle fwd = 0, inv = 0;
   bool has_fft = false;
+  cufftHandle fwd2 = 0, inv2 = 0;   // (y, z) 2D transforms of the fused x-pass path
+  bool has_fft2 = false;
   size_t fft_ws = 0;
   // optional per-stage CUDA-event timing (fd3_profile_enable / fd3_profile_read)
   static constexpr int kMaxMarks = 24;
@@ -195,6 +197,7 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
       m.filter_kt = -1;
       m.spread_zc = -1;
       m.spread_cap = 0;
+      m.fft_x = -1;   // default: off (3D cuFFT around the separate filter measured faster on B200)
       const size_t Mh = (size_t)m.n[0] * m.n[1] * m.nzh;
       if (d->method == FD3_METHOD_SPME && d->deconv) {
         if (cudaMalloc(&p->d_deconv, sizeof(float) * Mh) != cudaSuccess ||
@@ -228,6 +231,28 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
       }
       p->has_fft = true;
       p->fft_ws = ws1 > ws2 ? ws1 : ws2;
+      // (y, z) planes for the fused x-pass: batch over the C channels and nx planes
+      if (xfilter_pencil(m, dp ? 1 : 0) > 0) {
+        long long n2d[2] = {m.n[1], m.n[2]};
+        const long long pr = (long long)m.n[1] * m.n[2], pc = (long long)m.n[1] * m.nzh;
+        size_t ws3 = 0, ws4 = 0;
+        if ((fr = cufftCreate(&p->fwd2)) != CUFFT_SUCCESS || (fr = cufftCreate(&p->inv2)) != CUFFT_SUCCESS ||
+            (fr = cufftSetAutoAllocation(p->fwd2, 0)) != CUFFT_SUCCESS ||
+            (fr = cufftSetAutoAllocation(p->inv2, 0)) != CUFFT_SUCCESS ||
+            (fr = cufftMakePlanMany64(p->fwd2, 2, n2d, nullptr, 1, pr, nullptr, 1, pc, dp ? CUFFT_D2Z : CUFFT_R2C,
+                                      C * m.n[0], &ws3)) != CUFFT_SUCCESS ||
+            (fr = cufftMakePlanMany64(p->inv2, 2, n2d, nullptr, 1, pc, nullptr, 1, pr, dp ? CUFFT_Z2D : CUFFT_C2R,
+                                      C * m.n[0], &ws4)) != CUFFT_SUCCESS) {
+          char b[64];
+          snprintf(b, sizeof(b), "cufft status %d", (int)fr);
+          set_error("fd3_plan_create: cufft 2D plan", b);
+          rc = FD3_ECUFFT;
+          break;
+        }
+        p->has_fft2 = true;
+        if (ws3 > p->fft_ws) p->fft_ws = ws3;
+        if (ws4 > p->fft_ws) p->fft_ws = ws4;
+      }
     }
   } while (0);
   delete[] gp;
@@ -260,6 +285,14 @@ extern "C" int fd3_plan_set_tuning(fd3_plan* p, int32_t knob, int32_t value) {
     p->mg.spread_zc = value;
     return FD3_OK;
   }
+  if (knob == FD3_TUNE_FFT_X) {
+    if (value < -1 || value > 1) {
+      set_error("fd3_plan_set_tuning", "fused x-pass must be -1 (default), 0 (3D FFT + filter) or 1");
+      return FD3_EINVAL;
+    }
+    p->mg.fft_x = value;
+    return FD3_OK;
+  }
   if (knob == FD3_TUNE_SPREAD_CAP) {
     if (value != 0 && value < 256) {
       set_error("fd3_plan_set_tuning", "spread staging cap must be 0 (shared-memory bound) or >= 256");
@@ -290,6 +323,10 @@ extern "C" int fd3_plan_get_tuning(const fd3_plan* p, int32_t knob, int32_t* val
     *value = p->mg.spread_cap;
     return FD3_OK;
   }
+  if (knob == FD3_TUNE_FFT_X) {
+    *value = (p->has_fft2 && p->mg.fft_x == 1) ? 1 : 0;
+    return FD3_OK;
+  }
   set_error("fd3_plan_get_tuning", "unknown knob");
   return FD3_EINVAL;
 }
@@ -300,6 +337,8 @@ extern "C" int fd3_plan_destroy(fd3_plan* p) {
     if (p->ev[k]) cudaEventDestroy(p->ev[k]);
   if (p->fwd) cufftDestroy(p->fwd);
   if (p->inv) cufftDestroy(p->inv);
+  if (p->fwd2) cufftDestroy(p->fwd2);
+  if (p->inv2) cufftDestroy(p->inv2);
   cudaFree(p->d_tab);
   cudaFree(p->d_eigvecs);
   cudaFree(p->d_green);
@@ -457,6 +496,33 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
   prof_mark(p, s, "mesh_sort");
   FD3_TRY(launch_spread<T>(mg, N, pos, ps, species, w.c6, w.ci, w.mstart, w.morder, w.rec, (T*)w.rho, s));
   prof_mark(p, s, "spread");
+  if (p->has_fft2 && mg.fft_x == 1) {
+    // (y, z) transforms by cuFFT; x transform, filter and inverse x transform in one kernel
+    FD3_CUFFT(cufftSetStream(p->fwd2, s));
+    FD3_CUFFT(cufftSetWorkArea(p->fwd2, w.fftw));
+    if (sizeof(T) == 8)
+      FD3_CUFFT(cufftExecD2Z(p->fwd2, (cufftDoubleReal*)w.rho, (cufftDoubleComplex*)w.spec));
+    else
+      FD3_CUFFT(cufftExecR2C(p->fwd2, (cufftReal*)w.rho, (cufftComplex*)w.spec));
+    prof_mark(p, s, "fft_r2c");
+    if (sizeof(T) == 4) FD3_TRY(launch_green_table(mg, w.ci, p->d_green, p->d_tab, w.gtab, s));
+    FD3_TRY(launch_xfilter<T>(mg, w.ci, p->d_green, p->d_green_f, (const float4*)w.gtab, p->d_tab, p->d_deconv,
+                              p->method == FD3_METHOD_SPME, w.spec, w.kspc_part, n_kspc, s));
+    prof_mark(p, s, "filter");
+    *n_mcell = 0;
+    if (!need_grad) return FD3_OK;
+    FD3_CUFFT(cufftSetStream(p->inv2, s));
+    FD3_CUFFT(cufftSetWorkArea(p->inv2, w.fftw));
+    if (sizeof(T) == 8)
+      FD3_CUFFT(cufftExecZ2D(p->inv2, (cufftDoubleComplex*)w.spec, (cufftDoubleReal*)w.rho));
+    else
+      FD3_CUFFT(cufftExecC2R(p->inv2, (cufftComplex*)w.spec, (cufftReal*)w.rho));
+    prof_mark(p, s, "fft_c2r");
+    FD3_TRY(launch_gather<T>(mg, N, pos, ps, species, w.c6, w.dc6, w.ci, p->d_tab, w.morder, w.mstart, w.rec,
+                             (const T*)w.rho, w.gcn, gpos, mcell, n_mcell, s));
+    prof_mark(p, s, "gather");
+    return FD3_OK;
+  }
   FD3_CUFFT(cufftSetStream(p->fwd, s));
   FD3_CUFFT(cufftSetWorkArea(p->fwd, w.fftw));
   if (sizeof(T) == 8)

@@ -113,6 +113,7 @@ struct MeshGeom {
   int filter_kt;  // filter k-tile width (0: register kernel), -1: default for (S, R)
   int spread_zc;  // z-tiles per column chunk of the spread (0: per-tile kernel), -1: default
   int spread_cap; // staged atoms per column chunk at most (0: as many as shared memory holds)
+  int fft_x;      // fused x-pass (2D cuFFT + x FFT/filter kernel): 1 on, 0 off, -1 default
 };
 int launch_cellinfo(const double* cell, double scale, CellInfo* ci, cudaStream_t s);
 int launch_mesh_keys(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
@@ -133,6 +134,13 @@ template <typename T>
 int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const GreenPairF* gpf,
                   const float4* gtab, const Tables* tab, const float* deconv, int spme, void* spec, double* part,
                   int* n_blocks, cudaStream_t s);
+// fused x-pass: forward x FFT + filter + inverse x FFT on the (y, z)-transformed spectrum
+template <typename T>
+int launch_xfilter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const GreenPairF* gpf,
+                   const float4* gtab, const Tables* tab, const float* deconv, int spme, void* spec, double* part,
+                   int* n_blocks, cudaStream_t s);
+// kz width of the fused x-pass pencils for this mesh (0: the fused path does not apply)
+int xfilter_pencil(const MeshGeom& mg, int is_double);
 // mixed form: per-call table of G and its k-derivatives per species pair (gtab of the filter)
 int launch_green_table(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab, void* table,
                        cudaStream_t s);

@@ -90,10 +90,15 @@ FD3_API int fd3_plan_destroy(fd3_plan* plan);
  *   FD3_TUNE_SPREAD_CAP staged atoms per column chunk at most: 0 = what shared memory
  *                       holds, >= 256 = a lower bound (denser chunks take the per-tile
  *                       staging path inside the same CTA).
+ *   FD3_TUNE_FFT_X      1 = cuFFT transforms the (y, z) planes and one kernel does the x
+ *                       transform, the filter and the inverse x transform per pencil; 0 =
+ *                       3D cuFFT around a separate filter; -1 = the default (1 where it
+ *                       applies: at most 4 species and 8 ranks, nx = 64, 128 or 256).
  * fd3_plan_get_tuning returns the value in effect (the default resolved). */
 #define FD3_TUNE_FILTER_KT 0
 #define FD3_TUNE_SPREAD_ZC 1
 #define FD3_TUNE_SPREAD_CAP 2
+#define FD3_TUNE_FFT_X 3
 FD3_API int fd3_plan_set_tuning(fd3_plan* plan, int32_t knob, int32_t value);
 FD3_API int fd3_plan_get_tuning(const fd3_plan* plan, int32_t knob, int32_t* value);
 

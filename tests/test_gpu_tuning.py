@@ -87,3 +87,31 @@ def test_spread_column_chunks_agree(precision, cuda_device):
                 assert (s - s0).abs().max().item() <= tol_f, (zc, cap)
     with pytest.raises(ValueError):
         m.engine.set_tuning(spread_cap=100)
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_fused_x_pass_agrees_with_3d_fft(precision, cuda_device):
+    """cuFFT (y, z) planes + the fused x-FFT / filter / inverse x-FFT kernel against 3D cuFFT
+    around the separate filter, for SPME and PME, one to four species, nx = 64 and 128."""
+    import golden_cases as gc
+    from fourierd3_b200 import D3Model
+
+    tol_e = 1e-12 if precision == "fp64" else 2e-6
+    tol_f = 1e-10 if precision == "fp64" else 1e-5
+    ran = 0
+    for name in ("sio2_648_spme_p5", "sio2_648_pme_p5", "hcno_240_spme_p6", "hcno_240_spme_p4_tol1e-4"):
+        rec = gc.load(name)
+        m = D3Model(rec["numbers"], rec["cell"], precision=precision, device=cuda_device,
+                    **gc.model_kwargs(rec["config"]))
+        m.engine.set_tuning(fft_x=0)
+        assert m.engine.tuning()["fft_x"] == 0
+        e0, f0, s0 = (t.clone() for t in m(rec["positions"], rec["cell"]))
+        m.engine.set_tuning(fft_x=1)
+        if m.engine.tuning()["fft_x"] != 1:
+            continue   # more than 4 species or 8 ranks, or an nx outside 64/128/256
+        ran += 1
+        e, f, s = m(rec["positions"], rec["cell"])
+        assert abs(float(e) - float(e0)) <= tol_e * abs(float(e0)), (name, float(e), float(e0))
+        assert (f - f0).abs().max().item() <= tol_f, name
+        assert (s - s0).abs().max().item() <= tol_f, name
+    assert ran >= 2

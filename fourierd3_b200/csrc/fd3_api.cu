@@ -424,8 +424,7 @@ void carve(const fd3_plan* p, int64_t N, int64_t K_in, Carver& c, Work& w) {
   w.hits.cap = kHitCap;
   w.hits.is_double = p->precision == FD3_PREC_FP64;
   w.hits.j = c.take<int>(hn * kHitCap);
-  w.hits.a = c.take<char>(hn * kHitCap * es);
-  w.hits.d = c.take<char>(hn * kHitCap * 3 * es);
+  w.hits.ad = c.take<char>(hn * kHitCap * 4 * es);
   w.hits.n = c.take<int>(N);
   w.hits.ovf = c.take<int>(1);
   const size_t C = (size_t)p->S * p->R;

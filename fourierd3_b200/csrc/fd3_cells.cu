@@ -430,16 +430,19 @@ __device__ __forceinline__ void wrapped_pos(const GridDev& g, double4 x, int4 m,
   w2 = x.z - (m.x * g.cell[2] + m.y * g.cell[5] + m.z * g.cell[8]);
 }
 
-// The forward CN kernel also records, per atom, every pair with a non-zero CN derivative:
-// neighbour id, f'(r)/r and the Bohr vector d (HitList, TE = double for the plain form, float for
-// the mixed form). The adjoint then streams those records instead of searching the cell list a
-// second time. An atom with more than `cap` such pairs (or one handled by the global-memory path)
-// is marked n = -1 and the adjoint recomputes it.
+// The forward CN kernel also records, per atom, every in-cutoff pair: the neighbour id and one
+// 4-wide record {f'(r)/r, Bohr vector d} (HitList, TE = double for the plain form, float for the
+// mixed form), so the adjoint reads a pair with one vector load instead of searching the cell list
+// a second time. An atom with more than `cap` such pairs (or one handled by the global-memory
+// path) is marked n = -1 and the adjoint recomputes it.
+template <typename TE> struct Vec4;
+template <> struct Vec4<float> { using type = float4; };
+template <> struct Vec4<double> { using type = double4; };
+
 template <typename TE>
 struct HitList {
   int* j;
-  TE* a;
-  TE* d;
+  typename Vec4<TE>::type* ad;
   int* n;
   int cap;
 };
@@ -470,10 +473,7 @@ __device__ __forceinline__ void cn_hit(const BinStage& st, int c, double w0, dou
   }
   if (h < hl.cap) {
     hl.j[hb + h] = st.j[c];
-    hl.a[hb + h] = (TE)a;
-    hl.d[3 * (hb + h)] = (TE)v0;
-    hl.d[3 * (hb + h) + 1] = (TE)v1;
-    hl.d[3 * (hb + h) + 2] = (TE)v2;
+    hl.ad[hb + h] = typename Vec4<TE>::type{(TE)a, (TE)v0, (TE)v1, (TE)v2};
   }
 }
 
@@ -569,11 +569,11 @@ int launch_cn_c6_cells(const CellGrid& g, int n, const CellList& cl, const doubl
   if (hs.is_double)
     k_cn_bins<double, double><<<K, 32 * kWarpsPerBlock, 0, s>>>(
         to_dev(g), cl.bin_start, cl.xs, cl.meta, tab, cn,
-        HitList<double>{hs.j, (double*)hs.a, (double*)hs.d, hs.n, hs.cap}, hs.ovf);
+        HitList<double>{hs.j, (double4*)hs.ad, hs.n, hs.cap}, hs.ovf);
   else
     k_cn_bins<float, float><<<K, 32 * kWarpsPerBlock, 0, s>>>(
         to_dev(g), cl.bin_start, cl.xs, cl.meta, tab, cn,
-        HitList<float>{hs.j, (float*)hs.a, (float*)hs.d, hs.n, hs.cap}, hs.ovf);
+        HitList<float>{hs.j, (float4*)hs.ad, hs.n, hs.cap}, hs.ovf);
   FD3_LAUNCHED();
   const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
   if (blocks > 0) {
@@ -604,9 +604,8 @@ __global__ void __launch_bounds__(256) k_cn_adjoint_hits(int n, const int4* __re
     const double gi = gcn[i];
     const size_t hb = (size_t)t * hl.cap;
     for (int e = lane; e < nh; e += 32) {
-      const double a = (double)hl.a[hb + e];
-      const double v0 = (double)hl.d[3 * (hb + e)], v1 = (double)hl.d[3 * (hb + e) + 1],
-                   v2 = (double)hl.d[3 * (hb + e) + 2];
+      const typename Vec4<TE>::type r4 = hl.ad[hb + e];
+      const double a = (double)r4.x, v0 = (double)r4.y, v1 = (double)r4.z, v2 = (double)r4.w;
       const double w = (gi + gcn[hl.j[hb + e]]) * a;
       f0 -= w * v0;
       f1 -= w * v1;
@@ -673,10 +672,10 @@ int launch_cn_adjoint_cells(const CellGrid& g, int n, const CellList& cl, const 
   if (hs.is_double)
     k_cn_adjoint_hits<double><<<blocks, 32 * kWarpsPerBlock, 0, s>>>(
         n, cl.meta, gcn, grad, out_scale, vir_part,
-        HitList<double>{hs.j, (double*)hs.a, (double*)hs.d, hs.n, hs.cap});
+        HitList<double>{hs.j, (double4*)hs.ad, hs.n, hs.cap});
   else
     k_cn_adjoint_hits<float><<<blocks, 32 * kWarpsPerBlock, 0, s>>>(
-        n, cl.meta, gcn, grad, out_scale, vir_part, HitList<float>{hs.j, (float*)hs.a, (float*)hs.d, hs.n, hs.cap});
+        n, cl.meta, gcn, grad, out_scale, vir_part, HitList<float>{hs.j, (float4*)hs.ad, hs.n, hs.cap});
   FD3_LAUNCHED();
   k_cn_adjoint_global<<<fb, 32 * kWarpsPerBlock, 0, s>>>(to_dev(g), n, cl.bin_start, cl.xs, cl.meta, cl.off, tab,
                                                           gcn, grad, out_scale, vir_part + 9 * (size_t)blocks, hs.n,

@@ -60,12 +60,12 @@ int scan_exclusive(const int* in, int n, int* out, cudaStream_t s);   // out[n] 
 int build_cell_list(const CellGrid& g, int n, const double* pos_ang, const int32_t* species, CellList& cl,
                     cudaStream_t s);
 
-// Per-atom records of the CN pairs (neighbour, f'(r)/r, Bohr vector), written by the CN kernel
-// and streamed by its adjoint; a/d are double (plain form) or float (mixed form).
+// Per-atom records of the CN pairs (neighbour, and {f'(r)/r, Bohr vector} as one 4-wide record),
+// written by the CN kernel and streamed by its adjoint; ad is double4 (plain form) or float4
+// (mixed form).
 struct HitStore {
   int* j;
-  void* a;
-  void* d;
+  void* ad;
   int* n;
   int* ovf;     // count of bins / atoms that need the global-memory fallback (zeroed per call)
   int cap;

@@ -23,8 +23,9 @@ Layout on the device:
 over the lane streams), after which a call is a single graph replay. The cells are fixed
 for the life of a capture (they set the cell-list grid and the mesh).
 
-``autotune_lanes`` times candidate lane counts under graph replay and caches the winner in
-a JSON file keyed by the batch's shape signature.
+``autotune_filter`` and ``autotune_spread`` time the filter k-tile and the spread z-chunk on
+the heaviest structures; ``autotune_lanes`` times candidate lane counts under graph replay and
+caches the winner in a JSON file keyed by the batch's shape signature.
 """
 from __future__ import annotations
 
@@ -325,6 +326,30 @@ def autotune_filter(batch: "D3Batch", candidates: Sequence[int] = (0, 1, 2, 4, 8
                 except ValueError:
                     e.set_tuning(filter_kt=-1)
         out[c] = (best, times)
+    return out
+
+
+def autotune_spread(batch: "D3Batch", candidates: Sequence[int] = (0, 2, 4, 8, 15), reps: int = 2) -> dict:
+    """Pick the spread's z-chunk length (0 = per-tile kernel) from the heaviest structure of each
+    plan: every candidate is timed (profiled eager calls) and the fastest is set on that plan.
+    Returns {plan index: (chunk, {chunk: ms})}. Drops a captured graph."""
+    batch._graph = None
+    heaviest: dict = {}
+    for i, key in enumerate(batch._keys):
+        if key not in heaviest or batch.costs[i] > batch.costs[heaviest[key]]:
+            heaviest[key] = i
+    out = {}
+    for n, (key, i) in enumerate(heaviest.items()):
+        eng = batch._engines[key]
+        times = {}
+        for zc in candidates:
+            eng.set_tuning(spread_zc=zc)
+            if eng.tuning()["spread_zc"] != zc and zc != 0:
+                continue   # capped by the mesh: the same as a smaller chunk
+            times[zc] = _profiled_stage(batch, i, "spread", reps)
+        best = min(times, key=times.get)
+        eng.set_tuning(spread_zc=best)
+        out[n] = (best, times)
     return out
 
 

@@ -449,8 +449,17 @@ __device__ __forceinline__ void col_atom(const ColSmem<T>& m, const T* zrows, in
                                          T (&acc)[kSpTZ][kSpRC]) {
   if (CHECK && (m.zi[a] & ~kZiSpill) != zsrc) return;
   T cr[kSpRC];
+  if (sizeof(T) == 4 && kSpRC == 4 && (R & 3) == 0) {
+    // a whole 4-rank group in one 16-byte load (rows of R floats start on 16-byte boundaries)
+    const float4 c4 = *reinterpret_cast<const float4*>(m.cc + (size_t)a * R + r0);
+    cr[0] = wxy * (T)c4.x;
+    cr[1] = wxy * (T)c4.y;
+    cr[2] = wxy * (T)c4.z;
+    cr[3] = wxy * (T)c4.w;
+  } else {
 #pragma unroll
-  for (int r = 0; r < kSpRC; ++r) cr[r] = r0 + r < R ? wxy * m.cc[(size_t)a * R + r0 + r] : T(0);
+    for (int r = 0; r < kSpRC; ++r) cr[r] = r0 + r < R ? wxy * m.cc[(size_t)a * R + r0 + r] : T(0);
+  }
   T zr[kSpTZ];
   if (sizeof(T) == 4) {
     const float4* v = reinterpret_cast<const float4*>(zrows + (size_t)a * kSpTZ);

@@ -259,7 +259,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
           if (r0 + r < R) {
-            const C2 a = ss[((size_t)X * R + r0 + r) * KT + kk];
+            const C2 a = ss[(X * R + r0 + r) * KT + kk];
             const T l = lam[r0 + r];
             xl[r] = C2{l * a.x, l * a.y};
           } else {
@@ -270,7 +270,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
         for (int y = 0; y < kUnitY; ++y) {
           const int Y = Y0 + y;
           if (Y >= ya && Y < yb) {
-            const C2* sy = ss + ((size_t)Y * R + r0) * KT + kk;
+            const C2* sy = ss + (Y * R + r0) * KT + kk;
 #pragma unroll
             for (int r = 0; r < 8; ++r)
               if (r0 + r < R) {
@@ -315,28 +315,38 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
       virial_acc<T>(q, dq, acc);
     }
     __syncthreads();
-    for (int X = slot; X < S; X += NSLOT) {
+    // two species per thread (X and X + NSLOT): every staged S_Yr value serves both
+    for (int X = slot; X < S; X += 2 * NSLOT) {
+      const int X2 = X + NSLOT;
+      const bool two = X2 < S;
       for (int r0 = 0; r0 < R; r0 += 8) {
-        C2 h[8];
+        C2 h[8], h2[8];
 #pragma unroll
-        for (int r = 0; r < 8; ++r) h[r] = C2{T(0), T(0)};
+        for (int r = 0; r < 8; ++r) h[r] = h2[r] = C2{T(0), T(0)};
         // Y < X: pair index row0[Y] + (X - Y); Y >= X: row0[X] + (Y - X), contiguous
         for (int Y = 0; Y < S; ++Y) {
           const int pi = Y < X ? row0[Y] + (X - Y) : row0[X] + (Y - X);
           const T gh = gs[pi * KT + kk];
-          const C2* sy = ss + ((size_t)Y * R + r0) * KT + kk;
+          T gh2 = T(0);
+          if (two) gh2 = gs[(Y < X2 ? row0[Y] + (X2 - Y) : row0[X2] + (Y - X2)) * KT + kk];
+          const C2* sy = ss + (Y * R + r0) * KT + kk;
 #pragma unroll
           for (int r = 0; r < 8; ++r)
             if (r0 + r < R) {
               const C2 b = sy[r * KT];
               h[r].x += gh * b.x;
               h[r].y += gh * b.y;
+              h2[r].x += gh2 * b.x;
+              h2[r].y += gh2 * b.y;
             }
         }
         if (valid) {
 #pragma unroll
           for (int r = 0; r < 8; ++r)
-            if (r0 + r < R) spec[((size_t)X * R + r0 + r) * Mh + k] = h[r];
+            if (r0 + r < R) {
+              spec[((size_t)X * R + r0 + r) * Mh + k] = h[r];
+              if (two) spec[((size_t)X2 * R + r0 + r) * Mh + k] = h2[r];
+            }
         }
       }
     }

@@ -386,10 +386,10 @@ __device__ int col_stage(const MeshDev& g, const int* s_a0, const int* s_pref, i
     const int slot = staged + block_compact(keep, s_wcnt, &tot);
     if (keep && slot < cap) {
       // tile-local x and y rows (stencil nodes that wrap onto the same point are summed)
-      T* wxr = m.wx + (size_t)slot * 16;
-      T* wyr = m.wy + (size_t)slot * 16;
-      T* zo = m.wzo + (size_t)slot * kSpTZ;
-      T* zn = m.wzn + (size_t)slot * kSpTZ;
+      T* wxr = m.wx + slot * 16;
+      T* wyr = m.wy + slot * 16;
+      T* zo = m.wzo + slot * kSpTZ;
+      T* zn = m.wzn + slot * kSpTZ;
 #pragma unroll
       for (int z = 0; z < 16; ++z) {
         wxr[z] = T(0);
@@ -422,7 +422,7 @@ __device__ int col_stage(const MeshDev& g, const int* s_a0, const int* s_pref, i
         }
       }
       m.zi[slot] = seg / seg_per_z + (spill ? kZiSpill : 0);
-      for (int r = 0; r < R; ++r) m.cc[(size_t)slot * R + r] = rc[(size_t)u * R + r];
+      for (int r = 0; r < R; ++r) m.cc[slot * R + r] = rc[(size_t)u * R + r];
     }
     if (keep && slot >= cap) atomicMin(s_next, ca);
     staged += tot;
@@ -451,25 +451,25 @@ __device__ __forceinline__ void col_atom(const ColSmem<T>& m, const T* zrows, in
   T cr[kSpRC];
   if (sizeof(T) == 4 && kSpRC == 4 && (R & 3) == 0) {
     // a whole 4-rank group in one 16-byte load (rows of R floats start on 16-byte boundaries)
-    const float4 c4 = *reinterpret_cast<const float4*>(m.cc + (size_t)a * R + r0);
+    const float4 c4 = *reinterpret_cast<const float4*>(m.cc + a * R + r0);
     cr[0] = wxy * (T)c4.x;
     cr[1] = wxy * (T)c4.y;
     cr[2] = wxy * (T)c4.z;
     cr[3] = wxy * (T)c4.w;
   } else {
 #pragma unroll
-    for (int r = 0; r < kSpRC; ++r) cr[r] = r0 + r < R ? wxy * m.cc[(size_t)a * R + r0 + r] : T(0);
+    for (int r = 0; r < kSpRC; ++r) cr[r] = r0 + r < R ? wxy * m.cc[a * R + r0 + r] : T(0);
   }
   T zr[kSpTZ];
   if (sizeof(T) == 4) {
-    const float4* v = reinterpret_cast<const float4*>(zrows + (size_t)a * kSpTZ);
+    const float4* v = reinterpret_cast<const float4*>(zrows + a * kSpTZ);
     const float4 p0 = v[0], p1 = v[1];
     const float t8[8] = {p0.x, p0.y, p0.z, p0.w, p1.x, p1.y, p1.z, p1.w};
 #pragma unroll
     for (int z = 0; z < kSpTZ; ++z) zr[z] = (T)t8[z];
   } else {
 #pragma unroll
-    for (int z = 0; z < kSpTZ; ++z) zr[z] = zrows[(size_t)a * kSpTZ + z];
+    for (int z = 0; z < kSpTZ; ++z) zr[z] = zrows[a * kSpTZ + z];
   }
 #pragma unroll
   for (int z = 0; z < kSpTZ; ++z)
@@ -485,13 +485,13 @@ __device__ __forceinline__ void col_accumulate(const ColSmem<T>& m, int a0, int 
   for (; a + 4 <= a1; a += 4) {
     T wxy[4];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) wxy[u] = m.wx[(size_t)(a + u) * 16 + lx] * m.wy[(size_t)(a + u) * 16 + ly];
+    for (int u = 0; u < 4; ++u) wxy[u] = m.wx[(a + u) * 16 + lx] * m.wy[(a + u) * 16 + ly];
 #pragma unroll
     for (int u = 0; u < 4; ++u)
       if (wxy[u] != T(0)) col_atom<T, CHECK>(m, zrows, a + u, wxy[u], zsrc, R, r0, acc);
   }
   for (; a < a1; ++a) {
-    const T wxy = m.wx[(size_t)a * 16 + lx] * m.wy[(size_t)a * 16 + ly];
+    const T wxy = m.wx[a * 16 + lx] * m.wy[a * 16 + ly];
     if (wxy != T(0)) col_atom<T, CHECK>(m, zrows, a, wxy, zsrc, R, r0, acc);
   }
 }

@@ -299,9 +299,7 @@ def run_batch(args, ws, rank, local):
     if not b.captured:
         b.capture()
     with ClockSampler(torch.cuda.current_device()) as cs:
-        l0 = _native.launch_count()
         ms = max_over_ranks(time_steps(lambda: b(), steps, warm, ws, device), ws, device)
-        launches = _native.launch_count() - l0   # graph replays launch no host-counted kernels
     clocks = cs.summary()
     res["mixed_graph"] = ms
     # the kernel count per replay: count one eager pass over the same lanes

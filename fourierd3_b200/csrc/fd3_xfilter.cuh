@@ -257,7 +257,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_xfilter(MeshDev g, int P, in
 template <typename T>
 inline int xfilter_kz(const MeshGeom& mg) {
   const int C = mg.S * mg.R;
-  if (mg.S > 4 || mg.R > 8 || mg.lagrange < 0) return 0;
+  if (mg.S > 4 || mg.R > 8) return 0;
   int n1 = 0, n2 = 0;
   if (mg.n[0] == 64) n1 = 8, n2 = 8;
   else if (mg.n[0] == 128) n1 = 8, n2 = 16;

@@ -10,7 +10,6 @@ src/fourierd3/calculator.py:146-188, i.e. torch.autograd calling the hand-writte
 """
 from __future__ import annotations
 
-import math
 from dataclasses import dataclass
 from typing import Optional
 

@@ -1,7 +1,6 @@
 """Hand-written adjoints against central finite differences (h = 1e-4 A) on the GPU."""
 import numpy as np
 import pytest
-import torch
 
 import golden_cases as gc
 

@@ -11,7 +11,6 @@ import os
 
 import numpy as np
 import pytest
-import torch
 
 pytestmark = pytest.mark.gpu
 

@@ -16,7 +16,7 @@ KW = dict(method="spme", mesh_spacing=1.2, interpolation_nodes=5, c6tol=1.0)
 
 def test_md_nve_with_adjoint_checks(cuda_device):
     from fourierd3_b200 import FourierD3, structures
-    from fourierd3_b200.geometry import ANGSTROM_TO_BOHR, HARTREE_TO_EV
+    from fourierd3_b200.geometry import HARTREE_TO_EV
     from fourierd3_b200.md import VelocityVerlet
 
     p0, c0, z0 = structures.sio2_box(0)

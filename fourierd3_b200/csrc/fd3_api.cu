@@ -20,6 +20,7 @@ struct fd3_plan {
   GreenPair* d_green = nullptr;
   GreenPairF* d_green_f = nullptr;
   float* d_deconv = nullptr;
+  float* d_win_axes = nullptr;
   cufftHandle fwd = 0, inv = 0;
   bool has_fft = false;
   cufftHandle fwd2 = 0, inv2 = 0;   // (y, z) 2D transforms of the fused x-pass path
@@ -199,6 +200,31 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
       m.spread_cap = 0;
       m.fft_x = -1;   // default: off (3D cuFFT around the separate filter measured faster on B200)
       const size_t Mh = (size_t)m.n[0] * m.n[1] * m.nzh;
+      m.win_axes = nullptr;
+      if (d->method == FD3_METHOD_SPME && d->precision == FD3_PREC_MIXED) {
+        // sinc(m/n)^(2p) per axis (fftfreq order on x and y, rfftfreq on z), float64 rounded to float
+        const int na = m.n[0] + m.n[1] + m.nzh;
+        float* hw = new float[na];
+        for (int a = 0, o = 0; a < 3; ++a) {
+          const int cnt = a < 2 ? m.n[a] : m.nzh;
+          for (int i = 0; i < cnt; ++i) {
+            const int mm = (a < 2 && i > (m.n[a] - 1) / 2) ? i - m.n[a] : i;
+            const double x = (double)mm / m.n[a];
+            const double sc = x == 0.0 ? 1.0 : sin(kPi * x) / (kPi * x);
+            hw[o + i] = (float)pow(sc, 2.0 * d->order);
+          }
+          o += cnt;
+        }
+        const bool ok = cudaMalloc(&p->d_win_axes, sizeof(float) * na) == cudaSuccess &&
+                        cudaMemcpy(p->d_win_axes, hw, sizeof(float) * na, cudaMemcpyHostToDevice) == cudaSuccess;
+        delete[] hw;
+        if (!ok) {
+          set_error("fd3_plan_create", "upload of the per-axis window failed");
+          rc = FD3_ECUDA;
+          break;
+        }
+        m.win_axes = p->d_win_axes;
+      }
       if (d->method == FD3_METHOD_SPME && d->deconv) {
         if (cudaMalloc(&p->d_deconv, sizeof(float) * Mh) != cudaSuccess ||
             cudaMemcpy(p->d_deconv, d->deconv, sizeof(float) * Mh, cudaMemcpyHostToDevice) != cudaSuccess) {
@@ -344,6 +370,7 @@ extern "C" int fd3_plan_destroy(fd3_plan* p) {
   cudaFree(p->d_green);
   cudaFree(p->d_green_f);
   cudaFree(p->d_deconv);
+  cudaFree(p->d_win_axes);
   delete p;
   return FD3_OK;
 }

@@ -55,7 +55,13 @@ __device__ __forceinline__ KPoint<T> kpoint_idx(const MeshDev& g, int ix, int iy
 #pragma unroll
   for (int c = 0; c < 3; ++c) q.kv[c] = T(mx) * rc[c] + T(my) * rc[3 + c] + T(mz) * rc[6 + c];
   q.knorm = sqrt(q.kv[0] * q.kv[0] + q.kv[1] * q.kv[1] + q.kv[2] * q.kv[2]);
-  if (sizeof(T) == 4 && spme && deconv) {
+  if (sizeof(T) == 4 && spme && g.win_axes) {
+    // mixed form: the window is separable, sinc(mx/nx)^2p sinc(my/ny)^2p sinc(mz/nz)^2p (clamped
+    // at 1e-10 like the table); three per-axis values that stay in L1 instead of one table read
+    const float* wa = g.win_axes;
+    const float w = wa[ix] * wa[g.n[0] + iy] * wa[g.n[0] + g.n[1] + iz];
+    q.inv_sc = T(__frcp_rn(w < 1e-10f ? 1e-10f : w));
+  } else if (sizeof(T) == 4 && spme && deconv) {
     q.inv_sc = T(__frcp_rn(deconv[k]));   // mixed form: the float32 window inverted (correctly rounded)
   } else {
     double sc = 1.0;
@@ -182,13 +188,23 @@ __device__ __forceinline__ void filter_point(const KPoint<T>& q, int S, int R,
         }
   }
   T qq = T(0), dq = T(0);
+  const bool full = S == MAXS && R % MAXR == 0;   // every slot holds a channel: no predication
+  const size_t xs = (size_t)R * cs;               // channel stride between species
   for (int r0 = 0; r0 < R; r0 += MAXR) {
     C2 sv[MAXR][MAXS];
+    typename Cplx<T>::type* vr = v + (size_t)r0 * cs;
+    if (full) {
 #pragma unroll
-    for (int r = 0; r < MAXR; ++r)
+      for (int r = 0; r < MAXR; ++r)
 #pragma unroll
-      for (int X = 0; X < MAXS; ++X)
-        sv[r][X] = (X < S && r0 + r < R) ? v[((size_t)X * R + r0 + r) * cs] : C2{T(0), T(0)};
+        for (int X = 0; X < MAXS; ++X) sv[r][X] = vr[X * xs + r * cs];
+    } else {
+#pragma unroll
+      for (int r = 0; r < MAXR; ++r)
+#pragma unroll
+        for (int X = 0; X < MAXS; ++X)
+          sv[r][X] = (X < S && r0 + r < R) ? v[((size_t)X * R + r0 + r) * cs] : C2{T(0), T(0)};
+    }
 #pragma unroll
     for (int r = 0; r < MAXR; ++r) {
       T qr = T(0), dqr = T(0);
@@ -203,7 +219,10 @@ __device__ __forceinline__ void filter_point(const KPoint<T>& q, int S, int R,
           qr += G[X][Y] * re;
           dqr += dG[X][Y] * re;
         }
-        if (X < S && r0 + r < R) v[((size_t)X * R + r0 + r) * cs] = C2{hre, him};
+        if (full)
+          vr[X * xs + r * cs] = C2{hre, him};
+        else if (X < S && r0 + r < R)
+          v[((size_t)X * R + r0 + r) * cs] = C2{hre, him};
       }
       if (r0 + r < R) {
         const T lam = (T)tab->eigs[r0 + r];

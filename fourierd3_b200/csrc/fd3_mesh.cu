@@ -137,9 +137,29 @@ __global__ void __launch_bounds__(kFilterThreads, sizeof(T) == 8 ? 2 : (MAXS <= 
   load_recip<T>(ci, rc);
   float inv_h = 0.f;
   if constexpr (sizeof(T) == 4) inv_h = green_inv_h(g, ci);
-  for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < Mh; k += (size_t)gridDim.x * blockDim.x) {
-    const KPoint<T> q = kpoint<T>(g, k, rc, deconv, spme, P);
+  // the grid stride and the start point decomposed once into (rows of ix, rows of iy, iz);
+  // each step then advances (ix, iy, iz) by additions with at most one carry per axis
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t st_row = fdiv((uint32_t)stride, g.div_nzh);
+  const int st_z = (int)((uint32_t)stride - st_row * (uint32_t)g.nzh);
+  const uint32_t st_x = fdiv(st_row, g.div_ny);
+  const int st_y = (int)(st_row - st_x * (uint32_t)g.n[1]);
+  const uint32_t k_row = fdiv((uint32_t)k, g.div_nzh);
+  int iz = (int)((uint32_t)k - k_row * (uint32_t)g.nzh);
+  const uint32_t k_x = fdiv(k_row, g.div_ny);
+  int iy = (int)(k_row - k_x * (uint32_t)g.n[1]);
+  int ix = (int)k_x;
+  for (; k < Mh; k += stride) {
+    const KPoint<T> q = kpoint_idx<T>(g, ix, iy, iz, k, rc, deconv, spme, P);
     filter_point<T, MAXS, MAXR>(q, g.S, g.R, gp, gtab, inv_h, s6, s8, tab, spec + k, Mh, acc);
+    iz += st_z;
+    int c = iz >= g.nzh;
+    if (c) iz -= g.nzh;
+    iy += st_y + c;
+    c = iy >= g.n[1];
+    if (c) iy -= g.n[1];
+    ix += (int)st_x + c;
   }
   block_sum_store<7>(acc, part + 7 * blockIdx.x);
 }

@@ -22,6 +22,7 @@ namespace fd3 {
 struct MeshDev {
   int n[3], nzh, t[3], nt[3], ns[3], S, R;
   FastDiv div_nzh, div_ny;
+  const float* win_axes;
 };
 static inline MeshDev to_dev(const MeshGeom& g) {
   MeshDev d;
@@ -36,6 +37,7 @@ static inline MeshDev to_dev(const MeshGeom& g) {
   d.R = g.R;
   d.div_nzh = make_fastdiv((uint32_t)g.nzh);
   d.div_ny = make_fastdiv((uint32_t)g.n[1]);
+  d.win_axes = g.win_axes;
   return d;
 }
 

@@ -876,7 +876,7 @@ __device__ __forceinline__ void zrun_sums(const T (&v)[MAXR][NE], int R, const T
 }
 
 template <typename T, int P, int MAXR>
-__global__ void __launch_bounds__(32 * kGatherWarps) k_gather_z(MeshDev g, int n, const double* __restrict__ c6,
+__global__ void __launch_bounds__(32 * kGatherWarps, (sizeof(T) == 4 && MAXR <= 4 && P <= 5) ? 4 : 1) k_gather_z(MeshDev g, int n, const double* __restrict__ c6,
                                                                 const double* __restrict__ dc6,
                                                                 const CellInfo* __restrict__ ci,
                                                                 const Tables* __restrict__ tab,

@@ -527,7 +527,7 @@ __device__ __forceinline__ void col_store(const MeshDev& g, int X, int r0, const
 }
 
 template <typename T, int P>
-__global__ void __launch_bounds__(kSpThreads, sizeof(T) == 8 ? 2 : 3) k_spread_col(
+__global__ void __launch_bounds__(kSpThreads, sizeof(T) == 8 ? 2 : 4) k_spread_col(
     MeshDev g, int zc, int cap, const int4* __restrict__ rb, const T* __restrict__ rw, const T* __restrict__ rc,
     const int* __restrict__ key_start, T* __restrict__ rho) {
   extern __shared__ __align__(16) unsigned char col_raw[];
@@ -635,10 +635,10 @@ __global__ void __launch_bounds__(kSpThreads, sizeof(T) == 8 ? 2 : 3) k_spread_c
   }
 }
 
-// Staged atoms per column chunk: as many as let 3 (float) or 2 (double) CTAs share an SM.
+// Staged atoms per column chunk: as many as let 4 (float) or 2 (double) CTAs share an SM.
 template <typename T>
 inline int spread_col_cap(const MeshGeom& mg) {
-  constexpr int per_sm = sizeof(T) == 8 ? 2 : 3;
+  constexpr int per_sm = sizeof(T) == 8 ? 2 : 4;
   const size_t fixed = col_smem_bytes<T>(0, mg.R);
   const size_t per_atom = col_smem_bytes<T>(64, mg.R) / 64;
   int cap = (int)((size_t)(220 * 1024 / per_sm - 2048 - fixed) / per_atom);

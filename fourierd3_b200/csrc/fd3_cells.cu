@@ -367,22 +367,34 @@ __device__ __forceinline__ void cn_adjoint_atom_global(const GridDev& g, const i
 constexpr int kBinCap = 768;
 constexpr int kMaxNbrBins = 343;
 
+// P4 = double4: absolute image positions (the plain form, and the exact pair predicate);
+// P4 = float4 (mixed form): positions relative to the bin's own corner, so that float keeps
+// ~1e-6 A over the few bins a stage spans.
+template <typename P4>
 struct BinStage {
-  double4 p[kBinCap];   // image position (A), species in .w
+  P4 p[kBinCap];   // image position (A), species in .w
   int j[kBinCap];
   int a0[kMaxNbrBins];
   int pref[kMaxNbrBins + 1];
   int img[kMaxNbrBins][3];
 };
 
-// Returns the number of staged candidates, or -1 when the neighbourhood does not fit.
+// Returns the number of staged candidates, or -1 when the neighbourhood does not fit; org is the
+// origin subtracted from the staged positions (zero for double4).
+template <typename P4>
 __device__ int stage_bin(const GridDev& g, int b, const int* __restrict__ bin_start,
-                         const double4* __restrict__ xs, const int4* __restrict__ meta, BinStage& st,
-                         double* __restrict__ s_g, const double* __restrict__ gcn) {
+                         const double4* __restrict__ xs, const int4* __restrict__ meta, BinStage<P4>& st,
+                         double* __restrict__ s_g, const double* __restrict__ gcn, double (&org)[3]) {
   const int nx = 2 * g.reach[0] + 1, ny = 2 * g.reach[1] + 1, nz = 2 * g.reach[2] + 1;
   const int nnb = nx * ny * nz;
   if (nnb > kMaxNbrBins) return -1;
   const int bz = b % g.nb[2], by = (b / g.nb[2]) % g.nb[1], bx = b / (g.nb[2] * g.nb[1]);
+#pragma unroll
+  for (int c = 0; c < 3; ++c)
+    org[c] = sizeof(P4) == sizeof(double4)
+                 ? 0.0
+                 : ((double)bx / g.nb[0]) * g.cell[c] + ((double)by / g.nb[1]) * g.cell[3 + c] +
+                       ((double)bz / g.nb[2]) * g.cell[6 + c];
   for (int e = threadIdx.x; e < nnb; e += blockDim.x) {
     const int dz = e % nz - g.reach[2], dy = (e / nz) % ny - g.reach[1], dx = e / (nz * ny) - g.reach[0];
     const int cx = bx + dx, cy = by + dy, cz = bz + dz;
@@ -413,9 +425,13 @@ __device__ int stage_bin(const GridDev& g, int b, const int* __restrict__ bin_st
     const double4 xj = xs[u];
     const int4 mj = meta[u];
     const double S0 = st.img[lo][0] - mj.x, S1 = st.img[lo][1] - mj.y, S2 = st.img[lo][2] - mj.z;
-    st.p[c] = make_double4(xj.x + S0 * g.cell[0] + S1 * g.cell[3] + S2 * g.cell[6],
-                           xj.y + S0 * g.cell[1] + S1 * g.cell[4] + S2 * g.cell[7],
-                           xj.z + S0 * g.cell[2] + S1 * g.cell[5] + S2 * g.cell[8], xj.w);
+    const double px = xj.x + S0 * g.cell[0] + S1 * g.cell[3] + S2 * g.cell[6];
+    const double py = xj.y + S0 * g.cell[1] + S1 * g.cell[4] + S2 * g.cell[7];
+    const double pz = xj.z + S0 * g.cell[2] + S1 * g.cell[5] + S2 * g.cell[8];
+    if constexpr (sizeof(P4) == sizeof(double4))
+      st.p[c] = make_double4(px, py, pz, xj.w);
+    else
+      st.p[c] = make_float4((float)(px - org[0]), (float)(py - org[1]), (float)(pz - org[2]), (float)xj.w);
     st.j[c] = mj.w;
     if (s_g) s_g[c] = gcn[mj.w];
   }
@@ -451,20 +467,23 @@ struct HitList {
 // pair records. Bins whose neighbourhood does not fit the stage mark their atoms n = -2 and
 // leave them to k_cn_global.
 // Per atom (one warp) the staged candidates are first tested against the cutoff 32 at a time
-// (float64 distances); the indices of the pairs inside are compacted in order into a per-warp
-// ring of 64, and whenever 32 are waiting all lanes evaluate the CN function for them and write
-// their records contiguously. The CN function and the record stores thus run on full warps
+// (float64 distances in the plain form, float relative to the bin corner in the mixed form); the
+// indices of the pairs inside are compacted in order into a per-warp ring of 64, and whenever 32
+// are waiting all lanes evaluate the CN function for them and write their records contiguously. The CN function and the record stores thus run on full warps
 // instead of on the ~15 % of lanes that hit in a given candidate batch.
 constexpr int kCnRing = 64;
 
+template <typename TC> struct StagePos { using type = double4; };
+template <> struct StagePos<float> { using type = float4; };
+
 template <typename TE, typename TC>
-__device__ __forceinline__ void cn_hit(const BinStage& st, int c, double w0, double w1, double w2, TC rci, TC rc,
-                                       const Tables* __restrict__ tab, HitList<TE>& hl, size_t hb, int h,
-                                       TC& acc) {
-  const double4 pj = st.p[c];
-  const TC v0 = (TC)((pj.x - w0) * kAngToBohr);
-  const TC v1 = (TC)((pj.y - w1) * kAngToBohr);
-  const TC v2 = (TC)((pj.z - w2) * kAngToBohr);
+__device__ __forceinline__ void cn_hit(const BinStage<typename StagePos<TC>::type>& st, int c, TC w0, TC w1, TC w2,
+                                       TC rci, TC rc, const Tables* __restrict__ tab, HitList<TE>& hl, size_t hb,
+                                       int h, TC& acc) {
+  const auto pj = st.p[c];
+  const TC v0 = (TC)((pj.x - w0) * (TC)kAngToBohr);
+  const TC v1 = (TC)((pj.y - w1) * (TC)kAngToBohr);
+  const TC v2 = (TC)((pj.z - w2) * (TC)kAngToBohr);
   const TC r2 = v0 * v0 + v1 * v1 + v2 * v2;
   TC f = TC(0), a = TC(0);
   if (r2 > TC(1e-12)) {
@@ -482,11 +501,13 @@ __global__ void __launch_bounds__(256) k_cn_bins(GridDev g, const int* __restric
                                                 const double4* __restrict__ xs, const int4* __restrict__ meta,
                                                 const Tables* __restrict__ tab, double* __restrict__ cn,
                                                 HitList<TE> hl, int* __restrict__ ovf) {
-  __shared__ BinStage st;
+  using P4 = typename StagePos<TC>::type;
+  __shared__ BinStage<P4> st;
   __shared__ int ring[kWarpsPerBlock][kCnRing];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int b = blockIdx.x;
-  const int total = stage_bin(g, b, bin_start, xs, meta, st, nullptr, nullptr);
+  double org[3];
+  const int total = stage_bin<P4>(g, b, bin_start, xs, meta, st, nullptr, nullptr, org);
   const int s0 = bin_start[b], s1 = bin_start[b + 1];
   if (total < 0) {
     for (int t = s0 + threadIdx.x; t < s1; t += blockDim.x) hl.n[t] = -2;
@@ -495,12 +516,14 @@ __global__ void __launch_bounds__(256) k_cn_bins(GridDev g, const int* __restric
   }
   const unsigned lt = (1u << lane) - 1u;
   const TC rc = (TC)tab->r_cut;
+  const TC rc2 = (TC)g.rc2;
   int* rg = ring[wid];
   for (int t = s0 + wid; t < s1; t += kWarpsPerBlock) {
     const double4 xi = xs[t];
     const int4 mi = meta[t];
-    double w0, w1, w2;
-    wrapped_pos(g, xi, mi, w0, w1, w2);
+    double wd0, wd1, wd2;
+    wrapped_pos(g, xi, mi, wd0, wd1, wd2);
+    const TC w0 = (TC)(wd0 - org[0]), w1 = (TC)(wd1 - org[1]), w2 = (TC)(wd2 - org[2]);
     const TC rci = (TC)tab->rcov[(int)xi.w];
     TC acc = TC(0);
     int produced = 0, consumed = 0;
@@ -509,9 +532,9 @@ __global__ void __launch_bounds__(256) k_cn_bins(GridDev g, const int* __restric
       const int c = c0 + lane;
       bool hit = false;
       if (c < total) {
-        const double4 pj = st.p[c];
-        const double d0 = pj.x - w0, d1 = pj.y - w1, d2 = pj.z - w2;
-        hit = d0 * d0 + d1 * d1 + d2 * d2 < g.rc2;
+        const P4 pj = st.p[c];
+        const TC d0 = pj.x - w0, d1 = pj.y - w1, d2 = pj.z - w2;
+        hit = d0 * d0 + d1 * d1 + d2 * d2 < rc2;
       }
       const unsigned m = __ballot_sync(0xffffffffu, hit);
       if (hit) rg[(produced + __popc(m & lt)) & (kCnRing - 1)] = c;

@@ -618,32 +618,34 @@ __global__ void __launch_bounds__(256) k_cn_adjoint_hits(int n, const int4* __re
                                                         double out_scale, double* __restrict__ vir_part,
                                                         HitList<TE> hl) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  const int t = blockIdx.x * kWarpsPerBlock + wid;
   double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  const int nh = t < n ? hl.n[t] : -1;
-  if (nh >= 0) {
-    const int i = meta[t].w;
-    double f0 = 0, f1 = 0, f2 = 0;
-    const double gi = gcn[i];
-    const size_t hb = (size_t)t * hl.cap;
-    for (int e = lane; e < nh; e += 32) {
-      const typename Vec4<TE>::type r4 = hl.ad[hb + e];
-      const double a = (double)r4.x, v0 = (double)r4.y, v1 = (double)r4.z, v2 = (double)r4.w;
-      const double w = (gi + gcn[hl.j[hb + e]]) * a;
-      f0 -= w * v0;
-      f1 -= w * v1;
-      f2 -= w * v2;
-      const double bb = gi * a;
-      v[0] += bb * v0 * v0; v[1] += bb * v0 * v1; v[2] += bb * v0 * v2;
-      v[4] += bb * v1 * v1; v[5] += bb * v1 * v2; v[8] += bb * v2 * v2;
-    }
-    f0 = warp_sum(f0);
-    f1 = warp_sum(f1);
-    f2 = warp_sum(f2);
-    if (lane == 0) {
-      grad[3 * i] = out_scale * (grad[3 * i] + f0);
-      grad[3 * i + 1] = out_scale * (grad[3 * i + 1] + f1);
-      grad[3 * i + 2] = out_scale * (grad[3 * i + 2] + f2);
+  // grid-stride over atoms: the block's virial is reduced once, after all its atoms
+  for (int t = blockIdx.x * kWarpsPerBlock + wid; t < n; t += gridDim.x * kWarpsPerBlock) {
+    const int nh = hl.n[t];
+    if (nh >= 0) {
+      const int i = meta[t].w;
+      double f0 = 0, f1 = 0, f2 = 0;
+      const double gi = gcn[i];
+      const size_t hb = (size_t)t * hl.cap;
+      for (int e = lane; e < nh; e += 32) {
+        const typename Vec4<TE>::type r4 = hl.ad[hb + e];
+        const double a = (double)r4.x, v0 = (double)r4.y, v1 = (double)r4.z, v2 = (double)r4.w;
+        const double w = (gi + gcn[hl.j[hb + e]]) * a;
+        f0 -= w * v0;
+        f1 -= w * v1;
+        f2 -= w * v2;
+        const double bb = gi * a;
+        v[0] += bb * v0 * v0; v[1] += bb * v0 * v1; v[2] += bb * v0 * v2;
+        v[4] += bb * v1 * v1; v[5] += bb * v1 * v2; v[8] += bb * v2 * v2;
+      }
+      f0 = warp_sum(f0);
+      f1 = warp_sum(f1);
+      f2 = warp_sum(f2);
+      if (lane == 0) {
+        grad[3 * i] = out_scale * (grad[3 * i] + f0);
+        grad[3 * i + 1] = out_scale * (grad[3 * i + 1] + f1);
+        grad[3 * i + 2] = out_scale * (grad[3 * i + 2] + f2);
+      }
     }
   }
   v[3] = v[1];
@@ -688,8 +690,9 @@ int launch_cn_adjoint_cells(const CellGrid& g, int n, const CellList& cl, const 
                             cudaStream_t s) {
   (void)pos_ang;
   (void)species;
-  const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
-  const int fb = blocks < kFallbackBlocks ? blocks : kFallbackBlocks;
+  const int need = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  const int blocks = need < 148 * 8 ? need : 148 * 8;   // resident grid, grid-stride over atoms
+  const int fb = need < kFallbackBlocks ? need : kFallbackBlocks;
   *n_blocks = blocks + fb;
   if (blocks == 0) return FD3_OK;
   if (hs.is_double)

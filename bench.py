@@ -501,7 +501,7 @@ def main():
     achieved = dom_bytes / (ours[dom] * 1e-3) / 1e9
     # DRAM bytes (read + write) per launch from one ncu capture of the same 256^3 x 8-channel
     # mixed mesh (profiles/kernels_sio2_41472_mixed.md); mesh-side traffic does not depend on N
-    traffic_by_stage = {"filter": (575.1e6 + 484.0e6), "spread": (11.1e6 + 486.3e6)}
+    traffic_by_stage = {"filter": (541.3e6 + 481.7e6), "spread": (11.1e6 + 486.3e6)}
     mesh_match = tuple(mesh) == (256, 256, 256) and C == 8 and head == "mixed"
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": achieved / peak,

@@ -156,7 +156,8 @@ def measured_peaks():
 
 
 def stage_bytes(stage: str, n: int, mesh, C: int, R: int, b: int) -> float:
-    """Algorithmic HBM bytes of one launch of a pipeline stage (Roofline)."""
+    """Algorithmic HBM bytes of one launch of a pipeline stage: mesh terms per mesh point and
+    channel (b bytes real, 2b complex), atom terms per atom."""
     M = mesh[0] * mesh[1] * mesh[2]
     Mh = mesh[0] * mesh[1] * (mesh[2] // 2 + 1)
     if stage == "spread":

@@ -427,7 +427,7 @@ def main():
     # replay relaunches every kernel and cuFFT pass, so nothing is cached between steps
     from fourierd3_b200.batch import D3Batch
 
-    from fourierd3_b200.batch import autotune_spread
+    from fourierd3_b200.batch import autotune_fft_x, autotune_spread
 
     graphs, tuned = {}, {}
     for prec in precs:
@@ -436,10 +436,13 @@ def main():
         # launch shapes chosen by timing (results agree to rounding); the same plan settings
         # are copied to the eager model so both forms run the same kernels
         sp = autotune_spread(b, reps=2)
+        fx = autotune_fft_x(b, reps=2)
         eng = next(iter(b._engines.values()))
         tuned[prec] = eng.tuning()
         tuned[prec]["spread_ms"] = {str(k): round(v, 4) for k, v in sp[0][1].items()}
-        models[prec].engine.set_tuning(spread_zc=tuned[prec]["spread_zc"])
+        tuned[prec]["fft_filter_ms"] = {str(k): round(v, 4) for k, v in fx[0][1].items()}
+        models[prec].engine.set_tuning(spread_zc=tuned[prec]["spread_zc"], fft_x=tuned[prec]["fft_x"],
+                                       xpencil=tuned[prec]["xpencil"] if tuned[prec]["fft_x"] == 1 else -1)
         b.capture()
         graphs[prec] = b
 

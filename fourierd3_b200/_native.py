@@ -19,6 +19,7 @@ TUNE_FILTER_KT = 0
 TUNE_SPREAD_ZC = 1
 TUNE_SPREAD_CAP = 2
 TUNE_FFT_X = 3
+TUNE_XPENCIL = 4
 
 _c_int32 = ctypes.c_int32
 _c_int64 = ctypes.c_int64

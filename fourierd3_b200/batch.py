@@ -277,8 +277,10 @@ class D3Batch:
         return float(np.median(times))
 
 
-def _profiled_stage(batch: "D3Batch", i: int, stage: str, reps: int = 2) -> float:
-    """Milliseconds of one pipeline stage of structure ``i`` (eager, profiled calls)."""
+def _profiled_stage(batch: "D3Batch", i: int, stage, reps: int = 2) -> float:
+    """Milliseconds of one pipeline stage of structure ``i``, or the summed milliseconds of a
+    tuple of stages (eager, profiled calls; the fastest of ``reps`` after one warm-up call)."""
+    stages = (stage,) if isinstance(stage, str) else tuple(stage)
     q = int(batch.lane_of[i])
     for call in batch._lane_calls[q]:
         eng, pos, cell_h, cell_d, out, spc, wsl = call
@@ -287,7 +289,8 @@ def _profiled_stage(batch: "D3Batch", i: int, stage: str, reps: int = 2) -> floa
             best = float("inf")
             for _ in range(reps + 1):
                 eng.energy_forces_stress(pos, cell_h, batch.r_cut, cell_dev=cell_d, out=out, species=spc, work=wsl)
-                best = min(best, eng.stage_times().get(stage, float("inf")))
+                t = eng.stage_times()
+                best = min(best, sum(t.get(s, float("inf")) for s in stages))
             eng.profile(False)
             return best
     raise KeyError(i)
@@ -349,6 +352,39 @@ def autotune_spread(batch: "D3Batch", candidates: Sequence[int] = (0, 2, 4, 8, 1
             times[zc] = _profiled_stage(batch, i, "spread", reps)
         best = min(times, key=times.get)
         eng.set_tuning(spread_zc=best)
+        out[n] = (best, times)
+    return out
+
+
+def autotune_fft_x(batch: "D3Batch", pencils: Sequence[int] = (1, 2, 4), reps: int = 2) -> dict:
+    """Choose per plan between the 3D cuFFT transforms around the separate filter ("0") and the
+    (y, z) 2D cuFFT transforms around the fused x-FFT / filter / inverse x-FFT kernel with
+    pencils of ``pencils`` kz values ("1/<kz>"), by the summed time of the forward transform,
+    filter and inverse transform stages of the plan's heaviest structure. Plans where the fused
+    path does not apply keep "0". Returns {plan index: (choice, {choice: ms})}. Drops a
+    captured graph."""
+    batch._graph = None
+    heaviest: dict = {}
+    for i, key in enumerate(batch._keys):
+        if key not in heaviest or batch.costs[i] > batch.costs[heaviest[key]]:
+            heaviest[key] = i
+    out = {}
+    stages = ("fft_r2c", "filter", "fft_c2r")
+    for n, (key, i) in enumerate(heaviest.items()):
+        eng = batch._engines[key]
+        eng.set_tuning(fft_x=0, xpencil=-1)
+        times = {"0": _profiled_stage(batch, i, stages, reps)}
+        for kz in pencils:
+            eng.set_tuning(fft_x=1, xpencil=kz)
+            t = eng.tuning()
+            if t["fft_x"] != 1 or t["xpencil"] != kz:
+                continue   # no fused kernel for this mesh, species or rank count, or too wide
+            times[f"1/{kz}"] = _profiled_stage(batch, i, stages, reps)
+        best = min(times, key=times.get)
+        if best == "0":
+            eng.set_tuning(fft_x=0, xpencil=-1)
+        else:
+            eng.set_tuning(fft_x=1, xpencil=int(best.split("/")[1]))
         out[n] = (best, times)
     return out
 

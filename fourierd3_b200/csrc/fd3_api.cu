@@ -198,6 +198,7 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
       m.filter_kt = -1;
       m.spread_zc = -1;
       m.spread_cap = 0;
+      m.xpencil = -1;
       m.fft_x = -1;   // default: off (3D cuFFT around the separate filter measured faster on B200)
       const size_t Mh = (size_t)m.n[0] * m.n[1] * m.nzh;
       m.win_axes = nullptr;
@@ -319,6 +320,14 @@ extern "C" int fd3_plan_set_tuning(fd3_plan* p, int32_t knob, int32_t value) {
     p->mg.fft_x = value;
     return FD3_OK;
   }
+  if (knob == FD3_TUNE_XPENCIL) {
+    if (value != -1 && value != 1 && value != 2 && value != 4) {
+      set_error("fd3_plan_set_tuning", "fused x-pass pencil must be -1 (default), 1, 2 or 4 kz values");
+      return FD3_EINVAL;
+    }
+    p->mg.xpencil = value;
+    return FD3_OK;
+  }
   if (knob == FD3_TUNE_SPREAD_CAP) {
     if (value != 0 && value < 256) {
       set_error("fd3_plan_set_tuning", "spread staging cap must be 0 (shared-memory bound) or >= 256");
@@ -351,6 +360,10 @@ extern "C" int fd3_plan_get_tuning(const fd3_plan* p, int32_t knob, int32_t* val
   }
   if (knob == FD3_TUNE_FFT_X) {
     *value = (p->has_fft2 && p->mg.fft_x == 1) ? 1 : 0;
+    return FD3_OK;
+  }
+  if (knob == FD3_TUNE_XPENCIL) {
+    *value = p->has_fft2 ? xfilter_pencil(p->mg, p->precision == FD3_PREC_FP64 ? 1 : 0) : 0;
     return FD3_OK;
   }
   set_error("fd3_plan_get_tuning", "unknown knob");

@@ -114,6 +114,7 @@ struct MeshGeom {
   int spread_zc;  // z-tiles per column chunk of the spread (0: per-tile kernel), -1: default
   int spread_cap; // staged atoms per column chunk at most (0: as many as shared memory holds)
   int fft_x;      // fused x-pass (2D cuFFT + x FFT/filter kernel): 1 on, 0 off, -1 default
+  int xpencil;    // kz values per pencil of the fused x-pass (1, 2, 4), -1 default
   const float* win_axes;  // SPME, mixed form: sinc(m/n)^(2p) per axis, [nx | ny | nz/2+1] (null: none)
 };
 int launch_cellinfo(const double* cell, double scale, CellInfo* ci, cudaStream_t s);

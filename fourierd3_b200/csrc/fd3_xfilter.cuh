@@ -5,7 +5,10 @@
 // consecutive kz, every x, every channel -- into shared memory, transforms it along x,
 // filters every k-point of the pencil (the same per-k-point code as k_filter), transforms it
 // back and writes it in place. The spectrum crosses HBM once between the two 2D transforms
-// instead of three times (x pass, filter, x pass) on the 3D-FFT path.
+// instead of three times (x pass, filter, x pass) on the 3D-FFT path. (cuFFT's 2D transforms
+// with x innermost in the spectrum -- which would make each pencil one contiguous block --
+// measured 3x slower than with the natural layout, so the pencil reads KZ-value pieces of
+// the spectrum rows.)
 //
 // The x transform of length NX = N1 * N2 (N1, N2 in {8, 16}) is done in two register passes:
 //   X[k1 + N1 k2] = sum_n2 w_N2^(n2 k2) w_NX^(n2 k1) [ sum_n1 x[N2 n1 + n2] w_N1^(n1 k1) ],
@@ -63,6 +66,9 @@ __device__ __forceinline__ void cmul16(int m16, T br, T bi, T& tr, T& ti) {
 }
 
 // In-register DFT of N <= 16 points, X[k] = sum_n x[n] exp(SIGN 2 pi i n k / N).
+// Radix-2 decimation in time; every loop has a constant trip count, so after unrolling each
+// index is a compile-time constant and the arrays stay in registers (a loop stepping by the
+// stage length is not unrolled by nvcc and leaves the arrays in local memory).
 template <typename T, int N, int SIGN>
 __device__ __forceinline__ void dft_reg(T (&re)[N], T (&im)[N]) {
   T ar[N], ai[N];
@@ -71,20 +77,20 @@ __device__ __forceinline__ void dft_reg(T (&re)[N], T (&im)[N]) {
     ar[brev_n<N>(i)] = re[i];
     ai[brev_n<N>(i)] = im[i];
   }
+  constexpr int kLog = log2_n<N>();
 #pragma unroll
-  for (int st = 1; st <= log2_n<N>(); ++st) {
-    const int len = 1 << st, half = len >> 1;
+  for (int st = 0; st < kLog; ++st) {   // butterflies of span 2^st, twiddle exp(SIGN 2 pi i j / 2^(st+1))
 #pragma unroll
-    for (int i = 0; i < N; i += len)
-#pragma unroll
-      for (int j = 0; j < half; ++j) {
-        T tr, ti;
-        cmul16<T, SIGN>(j * (16 / len), ar[i + j + half], ai[i + j + half], tr, ti);
-        ar[i + j + half] = ar[i + j] - tr;
-        ai[i + j + half] = ai[i + j] - ti;
-        ar[i + j] = ar[i + j] + tr;
-        ai[i + j] = ai[i + j] + ti;
-      }
+    for (int b = 0; b < N / 2; ++b) {
+      const int j = b & ((1 << st) - 1);
+      const int lo = ((b >> st) << (st + 1)) + j, hi = lo + (1 << st);
+      T tr, ti;
+      cmul16<T, SIGN>(j * (8 >> st), ar[hi], ai[hi], tr, ti);
+      ar[hi] = ar[lo] - tr;
+      ai[hi] = ai[lo] - ti;
+      ar[lo] = ar[lo] + tr;
+      ai[lo] = ai[lo] + ti;
+    }
   }
 #pragma unroll
   for (int i = 0; i < N; ++i) {
@@ -93,33 +99,58 @@ __device__ __forceinline__ void dft_reg(T (&re)[N], T (&im)[N]) {
   }
 }
 
+// Asynchronous copies global -> shared; copy_async_wait_all waits for this thread's copies.
+// One complex value (8 bytes through L1 for float, 16 bytes through L2 only for double):
+template <typename C2>
+__device__ __forceinline__ void copy_async(C2* dst, const C2* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  if constexpr (sizeof(C2) == 16)
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+// 16 bytes (two float complex values), both addresses 16-byte aligned, through L2 only:
+__device__ __forceinline__ void copy_async16(void* dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void copy_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
+}
+
 template <int N1, int N2>
 struct XLayout {
   static constexpr int NX = N1 * N2;
-  static constexpr int ROW = N2 + 1;           // padded row
-  static constexpr int CS = N1 * ROW + 1;      // column stride (complex values)
+  static constexpr int ROW = N2 + 1;           // padded row (positions)
+  static constexpr int PC = N1 * ROW;          // positions per column
   static constexpr int TW = N2 * (N1 + 1);     // twiddle table exp(-2 pi i n2 k1 / NX) at n2 (N1 + 1) + k1
+  static constexpr int LN1 = log2_n<N1>(), LN2 = log2_n<N2>(), LNX = log2_n<NX>();
 };
 
-// shared memory: twiddle table + C * KZ columns
+// Pencil layout in shared memory: for channel c, position p of the padded N1 x (N2 + 1) column
+// and kz offset j, the value sits at c * (PC << LKZ) + (p << LKZ) + j -- the KZ values of one
+// (c, x) are adjacent, as they are in the spectrum, so a pencil row moves in 16-byte copies.
 template <typename T, int N1, int N2>
 __host__ __device__ inline size_t xfilter_smem(int C, int KZ) {
   using L = XLayout<N1, N2>;
-  return ((size_t)L::TW + (size_t)C * KZ * L::CS) * 2 * sizeof(T);
+  return ((size_t)L::TW + (size_t)C * KZ * L::PC) * 2 * sizeof(T);
 }
 
-// Forward x transform of the columns [0, ncol): natural order in, (k1, k2) order out.
+// Forward x transform of every column (c, j): natural order in, (k1, k2) order out.
 template <typename T, int N1, int N2>
-__device__ __forceinline__ void xfft_forward(typename Cplx<T>::type* buf, const typename Cplx<T>::type* tw, int ncol) {
+__device__ __forceinline__ void xfft_forward(typename Cplx<T>::type* buf, const typename Cplx<T>::type* tw, int C,
+                                             int LKZ) {
   using C2 = typename Cplx<T>::type;
   using L = XLayout<N1, N2>;
-  for (int it = threadIdx.x; it < ncol * N2; it += blockDim.x) {
-    C2* b = buf + (size_t)(it / N2) * L::CS;
-    const int n2 = it % N2;
+  const int KZ = 1 << LKZ, CSC = L::PC << LKZ;
+  // pass 1: lanes over (j, n2) -- a half-warp reads 16 adjacent values
+  for (int it = threadIdx.x; it < (C * N2) << LKZ; it += blockDim.x) {
+    const int j = it & (KZ - 1), n2 = (it >> LKZ) & (N2 - 1), c = it >> (LKZ + L::LN2);
+    C2* b = buf + c * CSC + (n2 << LKZ) + j;
     T re[N1], im[N1];
 #pragma unroll
     for (int n1 = 0; n1 < N1; ++n1) {
-      const C2 v = b[n1 * L::ROW + n2];
+      const C2 v = b[(n1 * L::ROW) << LKZ];
       re[n1] = v.x;
       im[n1] = v.y;
     }
@@ -127,91 +158,106 @@ __device__ __forceinline__ void xfft_forward(typename Cplx<T>::type* buf, const 
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) {
       const C2 w = tw[n2 * (N1 + 1) + k1];   // exp(-2 pi i n2 k1 / NX)
-      b[k1 * L::ROW + n2] = C2{re[k1] * w.x - im[k1] * w.y, re[k1] * w.y + im[k1] * w.x};
+      b[(k1 * L::ROW) << LKZ] = C2{re[k1] * w.x - im[k1] * w.y, re[k1] * w.y + im[k1] * w.x};
     }
   }
   __syncthreads();
-  for (int it = threadIdx.x; it < ncol * N1; it += blockDim.x) {
-    C2* b = buf + (size_t)(it / N1) * L::CS + (it % N1) * L::ROW;
+  // pass 2: lanes over (j, k1) -- rows (N2 + 1) << LKZ apart, free of bank conflicts
+  for (int it = threadIdx.x; it < (C * N1) << LKZ; it += blockDim.x) {
+    const int j = it & (KZ - 1), k1 = (it >> LKZ) & (N1 - 1), c = it >> (LKZ + L::LN1);
+    C2* b = buf + c * CSC + ((k1 * L::ROW) << LKZ) + j;
     T re[N2], im[N2];
 #pragma unroll
     for (int n2 = 0; n2 < N2; ++n2) {
-      const C2 v = b[n2];
+      const C2 v = b[n2 << LKZ];
       re[n2] = v.x;
       im[n2] = v.y;
     }
     dft_reg<T, N2, -1>(re, im);
 #pragma unroll
-    for (int k2 = 0; k2 < N2; ++k2) b[k2] = C2{re[k2], im[k2]};
+    for (int k2 = 0; k2 < N2; ++k2) b[k2 << LKZ] = C2{re[k2], im[k2]};
   }
   __syncthreads();
 }
 
 // Inverse x transform: (k1, k2) order in, natural order out.
 template <typename T, int N1, int N2>
-__device__ __forceinline__ void xfft_inverse(typename Cplx<T>::type* buf, const typename Cplx<T>::type* tw, int ncol) {
+__device__ __forceinline__ void xfft_inverse(typename Cplx<T>::type* buf, const typename Cplx<T>::type* tw, int C,
+                                             int LKZ) {
   using C2 = typename Cplx<T>::type;
   using L = XLayout<N1, N2>;
-  for (int it = threadIdx.x; it < ncol * N1; it += blockDim.x) {
-    C2* b = buf + (size_t)(it / N1) * L::CS + (it % N1) * L::ROW;
+  const int KZ = 1 << LKZ, CSC = L::PC << LKZ;
+  for (int it = threadIdx.x; it < (C * N1) << LKZ; it += blockDim.x) {
+    const int j = it & (KZ - 1), k1 = (it >> LKZ) & (N1 - 1), c = it >> (LKZ + L::LN1);
+    C2* b = buf + c * CSC + ((k1 * L::ROW) << LKZ) + j;
     T re[N2], im[N2];
 #pragma unroll
     for (int k2 = 0; k2 < N2; ++k2) {
-      const C2 v = b[k2];
+      const C2 v = b[k2 << LKZ];
       re[k2] = v.x;
       im[k2] = v.y;
     }
     dft_reg<T, N2, 1>(re, im);
 #pragma unroll
-    for (int n2 = 0; n2 < N2; ++n2) b[n2] = C2{re[n2], im[n2]};
+    for (int n2 = 0; n2 < N2; ++n2) b[n2 << LKZ] = C2{re[n2], im[n2]};
   }
   __syncthreads();
-  for (int it = threadIdx.x; it < ncol * N2; it += blockDim.x) {
-    C2* b = buf + (size_t)(it / N2) * L::CS;
-    const int n2 = it % N2;
+  for (int it = threadIdx.x; it < (C * N2) << LKZ; it += blockDim.x) {
+    const int j = it & (KZ - 1), n2 = (it >> LKZ) & (N2 - 1), c = it >> (LKZ + L::LN2);
+    C2* b = buf + c * CSC + (n2 << LKZ) + j;
     T re[N1], im[N1];
 #pragma unroll
     for (int k1 = 0; k1 < N1; ++k1) {
-      const C2 v = b[k1 * L::ROW + n2];
+      const C2 v = b[(k1 * L::ROW) << LKZ];
       const C2 w = tw[n2 * (N1 + 1) + k1];   // conj: exp(+2 pi i n2 k1 / NX)
       re[k1] = v.x * w.x + v.y * w.y;
       im[k1] = v.y * w.x - v.x * w.y;
     }
     dft_reg<T, N1, 1>(re, im);
 #pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) b[n1 * L::ROW + n2] = C2{re[n1], im[n1]};
+    for (int n1 = 0; n1 < N1; ++n1) b[(n1 * L::ROW) << LKZ] = C2{re[n1], im[n1]};
   }
   __syncthreads();
 }
 
-// One CTA per pencil (y, kz0..kz0+KZ-1) at a time (grid-stride over pencils); the spectrum
-// must hold the (y, z) 2D transforms of the C channels (layout (C, nx, ny, nz/2+1)).
-template <typename T, int MAXS, int MAXR, int N1, int N2>
-__global__ void __launch_bounds__(kFilterThreads) k_xfilter(MeshDev g, int P, int spme, int LKZ,
-                                                            const CellInfo* __restrict__ ci,
-                                                            const typename GreenPairOf<T>::type* __restrict__ gp,
-                                                            const float4* __restrict__ gtab,
-                                                            const Tables* __restrict__ tab,
-                                                            const float* __restrict__ deconv,
-                                                            typename Cplx<T>::type* __restrict__ spec,
-                                                            double* __restrict__ part) {
+// Pencil start along kz. With float values and an even number of values per spectrum x-row
+// block (ny * (nz/2 + 1) even), every row of the pencil of one y starts at the same parity;
+// shifting the pencil by that parity makes each pair of kz values one aligned 16-byte piece.
+// Returns the first kz of pencil gz (-1 for the first pencil of a shifted y).
+__device__ __forceinline__ int xpencil_start(int gz, int y, int nzh, int LKZ, bool pairs) {
+  const int par = pairs ? ((y * nzh) & 1) : 0;
+  return (gz << LKZ) - par;
+}
+
+// One CTA per pencil (y, kz0..kz0+KZ-1), KZ = 2^LKZ, at a time (grid-stride over pencils); the
+// spectrum must hold the (y, z) 2D transforms of the C channels (layout (C, nx, ny, nz/2+1)).
+// LKZ is a template parameter: constant shifts keep the float kernel within 80 registers.
+template <typename T, int MAXS, int MAXR, int N1, int N2, int LKZ>
+__global__ void __launch_bounds__(kFilterThreads, sizeof(T) == 4 && MAXS * MAXR <= 8 ? 3 : 1)
+    k_xfilter(MeshDev g, int P, int spme, const CellInfo* __restrict__ ci,
+              const typename GreenPairOf<T>::type* __restrict__ gp, const float4* __restrict__ gtab,
+              const Tables* __restrict__ tab, const float* __restrict__ deconv,
+              typename Cplx<T>::type* __restrict__ spec, double* __restrict__ part) {
   using C2 = typename Cplx<T>::type;
   using L = XLayout<N1, N2>;
   constexpr int NX = L::NX;
   extern __shared__ __align__(16) unsigned char xs_raw[];
   C2* tw = reinterpret_cast<C2*>(xs_raw);   // [n2][k1] exp(-2 pi i n2 k1 / NX), rows of N1 + 1
-  C2* buf = tw + L::TW;
+  C2* buf = tw + L::TW;                     // TW * sizeof(C2) is a multiple of 16 bytes
   const int KZ = 1 << LKZ;
   const int C = g.S * g.R;
-  const int ncol = C * KZ;
+  const int CSC = L::PC << LKZ;
   const int n1 = g.n[1], nzh = g.nzh;
+  const size_t xrow = (size_t)n1 * nzh;   // values between consecutive x of one channel
+  // float pencils of KZ >= 2 move as 16-byte pairs when every row of a pencil has one parity
+  const bool pairs = sizeof(T) == 4 && LKZ >= 1 && (xrow & 1) == 0;
   for (int m = threadIdx.x; m < L::TW; m += blockDim.x) {
     const int a = m / (N1 + 1), b = m % (N1 + 1);
     double sn, cs;
     sincospi(-2.0 * ((a * b) % NX) / NX, &sn, &cs);
     tw[m] = C2{(T)cs, (T)sn};
   }
-  const int ngz = (nzh + KZ - 1) / KZ;
+  const int ngz = (nzh + (pairs ? 1 : 0) + KZ - 1) >> LKZ;
   const int ngroups = n1 * ngz;
   double acc[7] = {0, 0, 0, 0, 0, 0, 0};
   const T s6 = (T)tab->s6, s8 = (T)tab->s8;
@@ -220,40 +266,83 @@ __global__ void __launch_bounds__(kFilterThreads) k_xfilter(MeshDev g, int P, in
   float inv_h = 0.f;
   if constexpr (sizeof(T) == 4) inv_h = green_inv_h(g, ci);
   for (int grp = blockIdx.x; grp < ngroups; grp += gridDim.x) {
-    const int y = grp / ngz, kz0 = (grp % ngz) * KZ;
+    const int y = grp / ngz;
+    const int kz0 = xpencil_start(grp - y * ngz, y, nzh, LKZ, pairs);
+    const C2* src = spec + (size_t)y * nzh + kz0;   // + (c NX + x) xrow + j, valid for 0 <= kz0 + j < nzh
     __syncthreads();   // twiddles written; the previous pencil has been stored
-    for (int e = threadIdx.x; e < (C * NX) << LKZ; e += blockDim.x) {
-      const int j = e & (KZ - 1), cx = e >> LKZ, x = cx % NX, c = cx / NX;
-      const int iz = kz0 + j;
-      buf[(size_t)(c * KZ + j) * L::CS + (x / N2) * L::ROW + (x % N2)] =
-          iz < nzh ? spec[((size_t)cx * n1 + y) * nzh + iz] : C2{T(0), T(0)};
+    // every copy of the pencil is in flight at once (asynchronous global -> shared copies)
+    if (pairs) {
+      constexpr int LNV = LKZ >= 1 ? LKZ - 1 : 0;   // pairs per (c, x) = 2^LNV
+      for (int i = threadIdx.x; i < (C * NX) << LNV; i += blockDim.x) {
+        const int v = i & ((1 << LNV) - 1), cx = i >> LNV, c = cx >> L::LNX, x = cx & (NX - 1);
+        const int kz = kz0 + 2 * v;
+        C2* d = buf + c * CSC + (((x >> L::LN2) * L::ROW + (x & (N2 - 1))) << LKZ) + 2 * v;
+        const C2* s = src + (size_t)cx * xrow + 2 * v;
+        if (kz >= 0 && kz + 1 < nzh) {
+          copy_async16(d, s);
+        } else {   // ragged pencil ends
+          d[0] = (kz >= 0 && kz < nzh) ? s[0] : C2{T(0), T(0)};
+          d[1] = (kz + 1 < nzh) ? s[1] : C2{T(0), T(0)};
+        }
+      }
+    } else {
+      for (int i = threadIdx.x; i < (C * NX) << LKZ; i += blockDim.x) {
+        const int j = i & (KZ - 1), cx = i >> LKZ, c = cx >> L::LNX, x = cx & (NX - 1);
+        const int kz = kz0 + j;
+        C2* d = buf + c * CSC + (((x >> L::LN2) * L::ROW + (x & (N2 - 1))) << LKZ) + j;
+        if (kz < nzh)
+          copy_async(d, src + (size_t)cx * xrow + j);
+        else
+          *d = C2{T(0), T(0)};
+      }
     }
+    copy_async_wait_all();
     __syncthreads();
-    xfft_forward<T, N1, N2>(buf, tw, ncol);
+    xfft_forward<T, N1, N2>(buf, tw, C, LKZ);
     for (int pt = threadIdx.x; pt < NX << LKZ; pt += blockDim.x) {
-      const int j = pt / NX, pos = pt % NX;   // consecutive lanes: consecutive positions of one column
+      const int j = pt & (KZ - 1), pos = pt >> LKZ;   // consecutive lanes: adjacent values
       const int iz = kz0 + j;
-      if (iz >= nzh) continue;
-      const int k1 = pos / N2, k2 = pos % N2;
+      if (iz < 0 || iz >= nzh) continue;
+      const int k1 = pos >> L::LN2, k2 = pos & (N2 - 1);
       const int ix = k1 + N1 * k2;
       const size_t k = ((size_t)ix * n1 + y) * nzh + iz;
       const KPoint<T> q = kpoint_idx<T>(g, ix, y, iz, k, rc, deconv, spme, P);
       filter_point<T, MAXS, MAXR>(q, g.S, g.R, gp, gtab, inv_h, s6, s8, tab,
-                                  buf + (size_t)j * L::CS + k1 * L::ROW + k2, (size_t)KZ * L::CS, acc);
+                                  buf + ((k1 * L::ROW + k2) << LKZ) + j, (size_t)CSC, acc);
     }
     __syncthreads();
-    xfft_inverse<T, N1, N2>(buf, tw, ncol);
-    for (int e = threadIdx.x; e < (C * NX) << LKZ; e += blockDim.x) {
-      const int j = e & (KZ - 1), cx = e >> LKZ, x = cx % NX, c = cx / NX;
-      const int iz = kz0 + j;
-      if (iz < nzh)
-        spec[((size_t)cx * n1 + y) * nzh + iz] = buf[(size_t)(c * KZ + j) * L::CS + (x / N2) * L::ROW + (x % N2)];
+    xfft_inverse<T, N1, N2>(buf, tw, C, LKZ);
+    C2* dst = spec + (size_t)y * nzh + kz0;
+    if (pairs) {
+      constexpr int LNV = LKZ >= 1 ? LKZ - 1 : 0;
+      for (int i = threadIdx.x; i < (C * NX) << LNV; i += blockDim.x) {
+        const int v = i & ((1 << LNV) - 1), cx = i >> LNV, c = cx >> L::LNX, x = cx & (NX - 1);
+        const int kz = kz0 + 2 * v;
+        const C2* d = buf + c * CSC + (((x >> L::LN2) * L::ROW + (x & (N2 - 1))) << LKZ) + 2 * v;
+        C2* s = dst + (size_t)cx * xrow + 2 * v;
+        if (kz >= 0 && kz + 1 < nzh) {
+          *reinterpret_cast<float4*>(s) = *reinterpret_cast<const float4*>(d);
+        } else {
+          if (kz >= 0 && kz < nzh) s[0] = d[0];
+          if (kz + 1 < nzh) s[1] = d[1];
+        }
+      }
+    } else {
+      for (int i = threadIdx.x; i < (C * NX) << LKZ; i += blockDim.x) {
+        const int j = i & (KZ - 1), cx = i >> LKZ, c = cx >> L::LNX, x = cx & (NX - 1);
+        if (kz0 + j < nzh)
+          dst[(size_t)cx * xrow + j] = buf[c * CSC + (((x >> L::LN2) * L::ROW + (x & (N2 - 1))) << LKZ) + j];
+      }
     }
   }
   block_sum_store<7>(acc, part + 7 * blockIdx.x);
 }
 
-// pencil width along kz for this plan (0: the fused path does not apply)
+// kz values per pencil for this plan (0: the fused path does not apply). A requested width
+// (mg.xpencil = 1, 2 or 4) is used when it fits in 200 KB of shared memory; otherwise, and by
+// default, the widest pencil that leaves three CTAs per SM (float) or fits in 100 KB (double).
+// Wider pencils move longer pieces of each spectrum row (measured on the 256^3 x 8-channel
+// float mesh without the L2 prefetch hint: 1.28, 0.675 and 0.568 ms for 1, 2 and 4 kz values).
 template <typename T>
 inline int xfilter_kz(const MeshGeom& mg) {
   const int C = mg.S * mg.R;
@@ -263,11 +352,12 @@ inline int xfilter_kz(const MeshGeom& mg) {
   else if (mg.n[0] == 128) n1 = 8, n2 = 16;
   else if (mg.n[0] == 256) n1 = 16, n2 = 16;
   else return 0;
-  for (int kz = 4; kz >= 1; kz >>= 1) {
-    const size_t b = (((size_t)n2 * (n1 + 1)) + (size_t)C * kz * (n1 * (n2 + 1) + 1)) * 2 * sizeof(T);
-    if (b <= 100 * 1024) return kz;
-  }
-  return 0;
+  auto bytes = [&](int kz) { return (((size_t)n2 * (n1 + 1)) + (size_t)C * kz * n1 * (n2 + 1)) * 2 * sizeof(T); };
+  if ((mg.xpencil == 1 || mg.xpencil == 2 || mg.xpencil == 4) && bytes(mg.xpencil) <= 200 * 1024) return mg.xpencil;
+  const size_t cap = sizeof(T) == 4 ? 74 * 1024 : 100 * 1024;
+  for (int kz = 4; kz >= 2; kz >>= 1)
+    if (bytes(kz) <= cap) return kz;
+  return bytes(1) <= 200 * 1024 ? 1 : 0;
 }
 
 }  // namespace fd3

@@ -4,14 +4,15 @@
 
 namespace fd3 {
 
-template <typename T, int MAXS, int MAXR, int N1, int N2>
-static int launch_x(const MeshGeom& mg, int KZ, const CellInfo* ci, const typename GreenPairOf<T>::type* gp,
-                    const float4* gtab, const Tables* tab, const float* deconv, int spme,
-                    typename Cplx<T>::type* sp, double* part, int* n_blocks, cudaStream_t s) {
+template <typename T, int MAXS, int MAXR, int N1, int N2, int LKZ>
+static int launch_xk(const MeshGeom& mg, const CellInfo* ci, const typename GreenPairOf<T>::type* gp,
+                     const float4* gtab, const Tables* tab, const float* deconv, int spme,
+                     typename Cplx<T>::type* sp, double* part, int* n_blocks, cudaStream_t s) {
+  constexpr int KZ = 1 << LKZ;
   const size_t smem = xfilter_smem<T, N1, N2>(mg.S * mg.R, KZ);
   static bool attr = false;
   if (!attr) {
-    if (cudaFuncSetAttribute(k_xfilter<T, MAXS, MAXR, N1, N2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(k_xfilter<T, MAXS, MAXR, N1, N2, LKZ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              200 * 1024) != cudaSuccess) {
       set_error("filter", "could not raise the shared-memory limit of the fused x-pass filter");
       return FD3_ECUDA;
@@ -19,22 +20,34 @@ static int launch_x(const MeshGeom& mg, int KZ, const CellInfo* ci, const typena
     attr = true;
   }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_xfilter<T, MAXS, MAXR, N1, N2>, kFilterThreads,
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_xfilter<T, MAXS, MAXR, N1, N2, LKZ>, kFilterThreads,
                                                     smem) != cudaSuccess || per_sm < 1)
     per_sm = 1;
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
-  const long long ngroups = (long long)mg.n[1] * ((mg.nzh + KZ - 1) / KZ);
+  // pencils per y: one more when float pairs shift odd-parity rows (kernel: ngz)
+  const bool pairs = sizeof(T) == 4 && LKZ >= 1 && (((size_t)mg.n[1] * mg.nzh) & 1) == 0;
+  const long long ngroups = (long long)mg.n[1] * ((mg.nzh + (pairs ? 1 : 0) + KZ - 1) / KZ);
   long long blocks = (long long)sms * per_sm;
   if (blocks > ngroups) blocks = ngroups;
   if (blocks > filter_max_blocks()) blocks = filter_max_blocks();
   *n_blocks = (int)blocks;
-  const int lkz = KZ >= 4 ? 2 : KZ >= 2 ? 1 : 0;
-  k_xfilter<T, MAXS, MAXR, N1, N2><<<(int)blocks, kFilterThreads, smem, s>>>(to_dev(mg), mg.order, spme, lkz, ci, gp,
-                                                                            gtab, tab, deconv, sp, part);
+  k_xfilter<T, MAXS, MAXR, N1, N2, LKZ><<<(int)blocks, kFilterThreads, smem, s>>>(to_dev(mg), mg.order, spme, ci, gp,
+                                                                                 gtab, tab, deconv, sp, part);
   FD3_LAUNCHED();
   return FD3_OK;
+}
+
+template <typename T, int MAXS, int MAXR, int N1, int N2>
+static int launch_x(const MeshGeom& mg, int KZ, const CellInfo* ci, const typename GreenPairOf<T>::type* gp,
+                    const float4* gtab, const Tables* tab, const float* deconv, int spme,
+                    typename Cplx<T>::type* sp, double* part, int* n_blocks, cudaStream_t s) {
+  if (KZ == 4)
+    return launch_xk<T, MAXS, MAXR, N1, N2, 2>(mg, ci, gp, gtab, tab, deconv, spme, sp, part, n_blocks, s);
+  if (KZ == 2)
+    return launch_xk<T, MAXS, MAXR, N1, N2, 1>(mg, ci, gp, gtab, tab, deconv, spme, sp, part, n_blocks, s);
+  return launch_xk<T, MAXS, MAXR, N1, N2, 0>(mg, ci, gp, gtab, tab, deconv, spme, sp, part, n_blocks, s);
 }
 
 template <typename T, int N1, int N2>

@@ -162,16 +162,19 @@ class Engine:
         return tuple(nb), tuple(rr)
 
     _KNOBS = {"filter_kt": _native.TUNE_FILTER_KT, "spread_zc": _native.TUNE_SPREAD_ZC,
-              "spread_cap": _native.TUNE_SPREAD_CAP, "fft_x": _native.TUNE_FFT_X}
+              "spread_cap": _native.TUNE_SPREAD_CAP, "fft_x": _native.TUNE_FFT_X,
+              "xpencil": _native.TUNE_XPENCIL}
 
     def set_tuning(self, filter_kt: Optional[int] = None, spread_zc: Optional[int] = None,
-                   spread_cap: Optional[int] = None, fft_x: Optional[int] = None) -> None:
+                   spread_cap: Optional[int] = None, fft_x: Optional[int] = None,
+                   xpencil: Optional[int] = None) -> None:
         """Launch-shape knobs (results agree to rounding): ``filter_kt`` = k-points per filter
         tile, ``spread_zc`` = z-tiles per column chunk of the spread, ``spread_cap`` = staged
         atoms per chunk at most, ``fft_x`` = fused x-pass (2D cuFFT + x FFT/filter kernel) on
-        or off; -1 (0 for the cap) restores a default."""
+        or off, ``xpencil`` = kz values per pencil of the fused x-pass (1, 2, 4); -1 (0 for the
+        cap) restores a default."""
         for name, val in (("filter_kt", filter_kt), ("spread_zc", spread_zc), ("spread_cap", spread_cap),
-                          ("fft_x", fft_x)):
+                          ("fft_x", fft_x), ("xpencil", xpencil)):
             if val is not None:
                 _native.check(_native.lib().fd3_plan_set_tuning(self._plan, self._KNOBS[name], int(val)),
                               "fd3_plan_set_tuning")

@@ -91,14 +91,20 @@ FD3_API int fd3_plan_destroy(fd3_plan* plan);
  *                       holds, >= 256 = a lower bound (denser chunks take the per-tile
  *                       staging path inside the same CTA).
  *   FD3_TUNE_FFT_X      1 = cuFFT transforms the (y, z) planes and one kernel does the x
- *                       transform, the filter and the inverse x transform per pencil; 0 =
- *                       3D cuFFT around a separate filter; -1 = the default (1 where it
- *                       applies: at most 4 species and 8 ranks, nx = 64, 128 or 256).
+ *                       transform, the filter and the inverse x transform per pencil (where
+ *                       it applies: at most 4 species and 8 ranks, nx = 64, 128 or 256); 0 =
+ *                       3D cuFFT around a separate filter; -1 = the default (0). Which is
+ *                       faster depends on the mesh and precision: time both.
+ *   FD3_TUNE_XPENCIL    kz values per pencil of the fused x-pass: 1, 2 or 4 (used when the
+ *                       pencil fits in shared memory), -1 = the default (the widest that
+ *                       leaves three CTAs per SM for float, within 100 KB for double);
+ *                       the value in effect is 0 where the fused x-pass does not apply.
  * fd3_plan_get_tuning returns the value in effect (the default resolved). */
 #define FD3_TUNE_FILTER_KT 0
 #define FD3_TUNE_SPREAD_ZC 1
 #define FD3_TUNE_SPREAD_CAP 2
 #define FD3_TUNE_FFT_X 3
+#define FD3_TUNE_XPENCIL 4
 FD3_API int fd3_plan_set_tuning(fd3_plan* plan, int32_t knob, int32_t value);
 FD3_API int fd3_plan_get_tuning(const fd3_plan* plan, int32_t knob, int32_t* value);
 

@@ -92,7 +92,9 @@ def test_spread_column_chunks_agree(precision, cuda_device):
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
 def test_fused_x_pass_agrees_with_3d_fft(precision, cuda_device):
     """cuFFT (y, z) planes + the fused x-FFT / filter / inverse x-FFT kernel against 3D cuFFT
-    around the separate filter, for SPME and PME, one to four species, nx = 64 and 128."""
+    around the separate filter, for SPME and PME, one to four species, nx = 64 and 128, and
+    pencils of 1, 2 and 4 kz values (float pencils of 2 and 4 move as 16-byte pairs, shifted by
+    one kz on the rows of odd parity; the case meshes have odd nz/2 + 1)."""
     import golden_cases as gc
     from fourierd3_b200 import D3Model
 
@@ -110,8 +112,14 @@ def test_fused_x_pass_agrees_with_3d_fft(precision, cuda_device):
         if m.engine.tuning()["fft_x"] != 1:
             continue   # more than 4 species or 8 ranks, or an nx outside 64/128/256
         ran += 1
-        e, f, s = m(rec["positions"], rec["cell"])
-        assert abs(float(e) - float(e0)) <= tol_e * abs(float(e0)), (name, float(e), float(e0))
-        assert (f - f0).abs().max().item() <= tol_f, name
-        assert (s - s0).abs().max().item() <= tol_f, name
+        for kz in (-1, 1, 2, 4):
+            m.engine.set_tuning(xpencil=kz)
+            got = m.engine.tuning()["xpencil"]
+            assert got in (1, 2, 4) and (kz == -1 or got <= kz), (name, kz, got)   # wider than shared memory: default
+            e, f, s = m(rec["positions"], rec["cell"])
+            assert abs(float(e) - float(e0)) <= tol_e * abs(float(e0)), (name, kz, float(e), float(e0))
+            assert (f - f0).abs().max().item() <= tol_f, (name, kz)
+            assert (s - s0).abs().max().item() <= tol_f, (name, kz)
     assert ran >= 2
+    with pytest.raises(ValueError):
+        m.engine.set_tuning(xpencil=3)

@@ -26,6 +26,10 @@ struct fd3_plan {
   cufftHandle fwd2 = 0, inv2 = 0;   // (y, z) 2D transforms of the fused x-pass path
   bool has_fft2 = false;
   size_t fft_ws = 0;
+  // side stream of the fused entry: the mesh sort (positions only) runs beside the cell list and
+  // the CN stage, forked from and joined back to the caller's stream by events (also under capture)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // optional per-stage CUDA-event timing (fd3_profile_enable / fd3_profile_read)
   static constexpr int kMaxMarks = 24;
   bool prof = false;
@@ -280,6 +284,16 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
         if (ws3 > p->fft_ws) p->fft_ws = ws3;
         if (ws4 > p->fft_ws) p->fft_ws = ws4;
       }
+      // side stream and fork/join events of the fused entry (without them it runs on one stream)
+      if (cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) != cudaSuccess ||
+          cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+          cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+        if (p->side) cudaStreamDestroy(p->side);
+        p->side = nullptr;
+        p->ev_fork = p->ev_join = nullptr;
+      }
     }
   } while (0);
   delete[] gp;
@@ -378,6 +392,9 @@ extern "C" int fd3_plan_destroy(fd3_plan* p) {
   if (p->inv) cufftDestroy(p->inv);
   if (p->fwd2) cufftDestroy(p->fwd2);
   if (p->inv2) cufftDestroy(p->inv2);
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+  if (p->ev_join) cudaEventDestroy(p->ev_join);
+  if (p->side) cudaStreamDestroy(p->side);
   cudaFree(p->d_tab);
   cudaFree(p->d_eigvecs);
   cudaFree(p->d_green);
@@ -525,13 +542,21 @@ static int check_work(const fd3_plan* p, int64_t N, int64_t K, void* work, size_
 
 // ------------------------------------------------------------------ shared mesh pipeline
 // spread -> forward FFT -> filter (energy, virial, H = G S) -> [inverse FFT -> gather]
-template <typename T>
-static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const int32_t* species, Work& w,
-                         bool need_grad, double* gpos, double* mcell, int* n_kspc, int* n_mcell, cudaStream_t s) {
+// atoms counting-sorted by (mesh tile, species): needs only the positions and the cell info
+static int mesh_sort(fd3_plan* p, int N, const double* pos, double ps, const int32_t* species, Work& w,
+                     cudaStream_t s) {
   const MeshGeom& mg = p->mg;
   const int Kmesh = mg.nt[0] * mg.nt[1] * mg.nt[2] * p->S;
   FD3_TRY(launch_mesh_keys(mg, N, pos, ps, species, w.ci, w.mkeys, s));
-  FD3_TRY(counting_sort(w.mkeys, N, Kmesh, w.mcount, w.mstart, w.morder, s));
+  return counting_sort(w.mkeys, N, Kmesh, w.mcount, w.mstart, w.morder, s);
+}
+
+template <typename T>
+static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const int32_t* species, Work& w,
+                         bool need_grad, double* gpos, double* mcell, int* n_kspc, int* n_mcell, bool presorted,
+                         cudaStream_t s) {
+  const MeshGeom& mg = p->mg;
+  if (!presorted) FD3_TRY(mesh_sort(p, N, pos, ps, species, w, s));
   prof_mark(p, s, "mesh_sort");
   FD3_TRY(launch_spread<T>(mg, N, pos, ps, species, w.c6, w.ci, w.mstart, w.morder, w.rec, (T*)w.rho, s));
   prof_mark(p, s, "spread");
@@ -590,7 +615,8 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
 }
 
 static int run_mesh(fd3_plan* p, int N, const double* pos, double ps, const int32_t* species, Work& w,
-                    bool need_grad, double* gpos, double* mcell, int* n_kspc, int* n_mcell, cudaStream_t s) {
+                    bool need_grad, double* gpos, double* mcell, int* n_kspc, int* n_mcell, cudaStream_t s,
+                    bool presorted = false) {
   if (p->method == FD3_METHOD_EWALD) {
     EwaldGeom eg{{p->ens[0], p->ens[1], p->ens[2]}, p->S, p->R};
     int rc;
@@ -604,8 +630,8 @@ static int run_mesh(fd3_plan* p, int N, const double* pos, double ps, const int3
     return rc;
   }
   if (p->precision == FD3_PREC_FP64)
-    return mesh_pipeline<double>(p, N, pos, ps, species, w, need_grad, gpos, mcell, n_kspc, n_mcell, s);
-  return mesh_pipeline<float>(p, N, pos, ps, species, w, need_grad, gpos, mcell, n_kspc, n_mcell, s);
+    return mesh_pipeline<double>(p, N, pos, ps, species, w, need_grad, gpos, mcell, n_kspc, n_mcell, presorted, s);
+  return mesh_pipeline<float>(p, N, pos, ps, species, w, need_grad, gpos, mcell, n_kspc, n_mcell, presorted, s);
 }
 
 // ------------------------------------------------------------------ edge-list entry
@@ -657,14 +683,23 @@ extern "C" int fd3_energy_forces_stress(fd3_plan* p, int64_t n_atoms, const doub
   FD3_TRY(check_work(p, N, K, d_work, work_bytes, w));
   prof_begin(p, s);
   FD3_TRY(launch_cellinfo(d_cell_ang, kAngToBohr, w.ci, s));
+  const bool fork = p->side != nullptr && p->method != FD3_METHOD_EWALD;
+  if (fork) {   // mesh sort on the side stream, beside the cell list and the CN stage
+    FD3_CUDA(cudaEventRecord(p->ev_fork, s));
+    FD3_CUDA(cudaStreamWaitEvent(p->side, p->ev_fork, 0));
+    FD3_TRY(mesh_sort(p, N, d_pos_ang, kAngToBohr, d_species, w, p->side));
+    FD3_CUDA(cudaEventRecord(p->ev_join, p->side));
+  }
   FD3_TRY(build_cell_list(g, N, d_pos_ang, d_species, w.cl, s));
   prof_mark(p, s, "cell_list");
   int n_self = 0, n_kspc = 0, n_mcell = 0, n_cnv = 0;
   FD3_TRY(launch_cn_c6_cells(g, N, w.cl, d_pos_ang, d_species, p->d_tab, p->d_eigvecs, p->R, w.cn, w.c6, w.dc6,
                              w.self_part, &n_self, w.hits, s));
   prof_mark(p, s, "cn_c6");
+  if (fork) FD3_CUDA(cudaStreamWaitEvent(s, p->ev_join, 0));
   // the mesh gradient (Hartree/Bohr) is staged in d_forces, then finished by the CN adjoint
-  FD3_TRY(run_mesh(p, N, d_pos_ang, kAngToBohr, d_species, w, true, d_forces, nullptr, &n_kspc, &n_mcell, s));
+  FD3_TRY(run_mesh(p, N, d_pos_ang, kAngToBohr, d_species, w, true, d_forces, nullptr, &n_kspc, &n_mcell, s,
+                   fork));
   FD3_TRY(launch_cn_adjoint_cells(g, N, w.cl, d_pos_ang, d_species, p->d_tab, w.gcn, d_forces,
                                   -kHartreeToEv * kAngToBohr, w.cnv_part, &n_cnv, w.hits, s));
   prof_mark(p, s, "cn_adjoint");

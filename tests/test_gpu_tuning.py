@@ -123,3 +123,29 @@ def test_fused_x_pass_agrees_with_3d_fft(precision, cuda_device):
     assert ran >= 2
     with pytest.raises(ValueError):
         m.engine.set_tuning(xpencil=3)
+
+
+def test_autotune_fft_x_picks_a_timed_path(cuda_device):
+    """batch.autotune_fft_x times the 3D path and the fused x-pass at each pencil width on the
+    plan's heaviest structure, leaves the fastest set on the plan, and the batch results agree
+    with the 3D path (few species: the fused path applies; many species: it does not)."""
+    from fourierd3_b200 import structures as st
+    from fourierd3_b200.batch import D3Batch, autotune_fft_x
+
+    structs = [st.sio2_box(0), st.random_box(61, 90, z_max=54)]
+    b = D3Batch(structs, precision="mixed", device=cuda_device, **KW)
+    e0 = b()[0].clone()
+    res = autotune_fft_x(b, reps=1)
+    assert len(res) == 2
+    for n, (best, times) in res.items():
+        assert best == min(times, key=times.get) and "0" in times
+        eng = list(b._engines.values())[n]
+        t = eng.tuning()
+        if best == "0":
+            assert t["fft_x"] == 0
+        else:
+            assert t["fft_x"] == 1 and t["xpencil"] == int(best.split("/")[1])
+    fused = [times for _, times in res.values() if len(times) > 1]
+    assert len(fused) == 1 and set(fused[0]) == {"0", "1/1", "1/2", "1/4"}   # SiO2: 64^3, 2 species
+    e = b()[0]
+    assert torch.allclose(e, e0, rtol=2e-6, atol=0.0)

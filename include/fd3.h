@@ -144,6 +144,9 @@ FD3_API int fd3_energy_edges(fd3_plan* plan, int64_t n_atoms, const double* d_po
  *   d_cell_ang [9]   the same cell on the device
  *   r_cut_ang        neighbour cutoff (the pair predicate uses Angstrom, as matscipy)
  * outputs: d_energy [1] eV, d_forces [N*3] eV/A, d_stress [9] eV/A^3 (ASE sign)
+ * All work is ordered on `stream`; the mesh sort runs on the plan's own side stream, forked
+ * from and joined back to `stream` by events (so one plan serialises the sorts of calls made
+ * on different streams, and the call may be captured into a CUDA graph).
  */
 FD3_API int fd3_energy_forces_stress(fd3_plan* plan, int64_t n_atoms, const double* d_pos_ang,
                              const int32_t* d_species, const double* h_cell_ang, const double* d_cell_ang,

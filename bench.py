@@ -586,6 +586,27 @@ def main():
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, 256^3 x 8 channels, mixed"
                               if mesh_match and dom in traffic_by_stage else None,
             "bytes_per_launch": dom_bytes, "ms_per_launch": ours[dom]}
+    if fused and dom == "filter" and head == "mixed":
+        # bandwidth ceiling of the fused x-pass kernel's access pattern: every spectrum value read
+        # and written once in that kernel's pencil order and piece size, nothing computed
+        Mh = mesh[0] * mesh[1] * (mesh[2] // 2 + 1)
+        buf = torch.zeros(C * Mh * 2, dtype=torch.float32, device=device)
+        eng = models[head].engine
+        for _ in range(2):
+            eng.probe_pencil_traffic(buf)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(device)
+        ev0.record()
+        for _ in range(5):
+            eng.probe_pencil_traffic(buf)
+        ev1.record()
+        torch.cuda.synchronize(device)
+        pms = ev0.elapsed_time(ev1) / 5
+        ceiling = 2.0 * C * Mh * 8 / (pms * 1e-3) / 1e9
+        roof["pattern_ceiling"] = {"value": ceiling, "unit": "GB/s", "ms": pms, "frac": achieved / ceiling,
+                                   "what": "the same spectrum bytes moved in the kernel's pencil order and piece "
+                                           "size with no arithmetic (fd3_probe_pencil_traffic)"}
+        del buf
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:

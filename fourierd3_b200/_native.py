@@ -58,6 +58,7 @@ _SIGS = {
     "fd3_neighbor_fill_static": (ctypes.c_int, [_c_int64, _vp, _dp, _c_double, _c_int64, _vp, _vp, _vp,
                                                 ctypes.POINTER(_c_int64), _vp]),
     "fd3_profile_enable": (ctypes.c_int, [_vp, _c_int32]),
+    "fd3_probe_pencil_traffic": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t, _vp]),
     "fd3_profile_read": (ctypes.c_int, [_vp, _dp, _c_int32, ctypes.c_char_p, _c_int32, ctypes.POINTER(_c_int32)]),
     "fd3_last_error": (ctypes.c_char_p, []),
     "fd3_launch_count": (_c_int64, []),

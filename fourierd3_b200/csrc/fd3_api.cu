@@ -787,6 +787,19 @@ extern "C" int fd3_neighbor_fill(int64_t n, const double* d_pos, const double* h
   return FD3_OK;
 }
 
+// ------------------------------------------------------------------ access-pattern probe
+extern "C" int fd3_probe_pencil_traffic(const fd3_plan* p, void* d_buf, size_t bytes, void* stream) {
+  if (!p || !d_buf || p->method == FD3_METHOD_EWALD) return FD3_EINVAL;
+  const size_t need = (size_t)p->S * p->R * p->mg.n[0] * p->mg.n[1] * p->mg.nzh * 2 * sizeof(float);
+  if (bytes < need) {
+    set_error("fd3_probe_pencil_traffic", "buffer smaller than the float spectrum of the plan");
+    return FD3_EINVAL;
+  }
+  int kz = xfilter_pencil(p->mg, 0);
+  if (kz < 1) kz = 4;
+  return launch_probe_pencil(p->mg, kz, d_buf, (cudaStream_t)stream);
+}
+
 // ------------------------------------------------------------------ profiling
 extern "C" int fd3_profile_enable(fd3_plan* p, int32_t on) {
   if (!p) return FD3_EINVAL;

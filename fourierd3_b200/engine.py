@@ -187,6 +187,17 @@ class Engine:
             out[name] = int(v.value)
         return out
 
+    def probe_pencil_traffic(self, buf: torch.Tensor) -> None:
+        """Measurement helper: read and write back unchanged every value of ``buf`` (a device
+        buffer of at least S*R*nx*ny*(nz/2+1) complex floats) in the fused x-pass kernel's
+        pencil order and piece size, on the current stream. Timing it gives that access
+        pattern's bandwidth ceiling; it computes nothing."""
+        nbytes = buf.numel() * buf.element_size()
+        if not (buf.is_cuda and buf.is_contiguous()):
+            raise ValueError("probe_pencil_traffic needs a contiguous CUDA buffer")
+        _native.check(_native.lib().fd3_probe_pencil_traffic(self._plan, buf.data_ptr(), nbytes,
+                                                             _stream_ptr(buf.device)), "fd3_probe_pencil_traffic")
+
     def profile(self, on: bool = True) -> None:
         """Record CUDA events between pipeline stages of the following calls."""
         _native.check(_native.lib().fd3_profile_enable(self._plan, 1 if on else 0), "fd3_profile_enable")

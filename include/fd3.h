@@ -193,6 +193,13 @@ FD3_API int fd3_profile_enable(fd3_plan* plan, int32_t on);
 FD3_API int fd3_profile_read(fd3_plan* plan, double* ms, int32_t max_stages, char* names, int32_t names_len,
                              int32_t* n_stages);
 
+/* Measurement helper (no reference counterpart; no compute path calls it): reads and writes
+ * back unchanged every value of d_buf, a buffer shaped like the plan's float half spectrum
+ * (S*R channels, (nx, ny, nz/2+1) complex float; bytes >= S*R*nx*ny*(nz/2+1)*8), pencil by
+ * pencil in the order and piece size of the fused x-pass kernel (FD3_TUNE_XPENCIL width in
+ * effect, else 4). Timing it gives the bandwidth ceiling of that kernel's access pattern. */
+FD3_API int fd3_probe_pencil_traffic(const fd3_plan* plan, void* d_buf, size_t bytes, void* stream);
+
 /* Last CUDA / cuFFT error text of the calling thread (static storage). */
 FD3_API const char* fd3_last_error(void);
 /* Number of kernel launches this library issued since load (for launch accounting). */

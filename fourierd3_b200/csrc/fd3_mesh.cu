@@ -183,10 +183,14 @@ static int filter_units(int S) {
   for (int y0 = 0; y0 < S; y0 += kUnitY) n += (y0 + kUnitY < S ? y0 + kUnitY : S);
   return n;
 }
+// The spectrum tile keeps species X's R rows of KT values at X (R KT + kTilePad) + r KT: the pad
+// puts the rows of consecutive species, read together by the slots of one warp in phase B, on
+// different shared-memory banks (R KT is a multiple of the 32 banks for the usual R and KT).
+constexpr int kTilePad = 4;
 struct FilterTileSmem {
   static size_t bytes(int S, int R, int kt, size_t tsize) {
     const size_t C = (size_t)S * R, np = (size_t)S * (S + 1) / 2;
-    size_t b = C * kt * 2 * tsize;                  // spectrum tile
+    size_t b = (C * kt + (size_t)S * kTilePad) * 2 * tsize;   // spectrum tile
     b += 32 * tsize;                                // lambda_r
     b += np * kt * tsize;                           // Gh tile
     b += (size_t)filter_units(S) * sizeof(uint32_t); // units (X, Y0)
@@ -195,7 +199,9 @@ struct FilterTileSmem {
   }
 };
 
-template <typename T, int KT>
+// RF > 0: the rank count is RF at compile time (the rank loops unroll without predicates);
+// RF = 0: any rank from the geometry.
+template <typename T, int KT, int RF>
 __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int P, int spme, int n_units,
                                                                  const CellInfo* __restrict__ ci,
                                                                  const typename GreenPairOf<T>::type* __restrict__ gp,
@@ -207,10 +213,11 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
   using C2 = typename Cplx<T>::type;
   constexpr int NSLOT = kFilterThreads / KT;
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int S = g.S, R = g.R, C = S * R, NP = S * (S + 1) / 2;
+  const int S = g.S, R = RF > 0 ? RF : g.R, C = S * R, NP = S * (S + 1) / 2;
   // sections in decreasing alignment: T-sized arrays first, then the 4-byte tables
-  C2* ss = reinterpret_cast<C2*>(smem_raw);                  // [C][KT]
-  T* lam = reinterpret_cast<T*>(ss + (size_t)C * KT);        // [32]
+  C2* ss = reinterpret_cast<C2*>(smem_raw);                  // [S][R KT + kTilePad]
+  const int XS = R * KT + kTilePad;                          // species stride of the tile
+  T* lam = reinterpret_cast<T*>(ss + (size_t)S * XS);        // [32]
   T* gs = lam + 32;                                          // [NP][KT]
   uint32_t* units = reinterpret_cast<uint32_t*>(gs + (size_t)NP * KT);
   int* row0 = reinterpret_cast<int*>(units + n_units);
@@ -238,7 +245,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
     for (int e = threadIdx.x; e < C * KT; e += kFilterThreads) {
       const int c = e / KT, j = e % KT;
       const size_t k = k0 + j;
-      ss[e] = k < Mh ? spec[(size_t)c * Mh + k] : C2{T(0), T(0)};
+      ss[e + (c / R) * kTilePad] = k < Mh ? spec[(size_t)c * Mh + k] : C2{T(0), T(0)};
     }
     const size_t k = k0 + kk;
     const bool valid = k < Mh;
@@ -279,7 +286,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
           if (r0 + r < R) {
-            const C2 a = ss[(X * R + r0 + r) * KT + kk];
+            const C2 a = ss[X * XS + (r0 + r) * KT + kk];
             const T l = lam[r0 + r];
             xl[r] = C2{l * a.x, l * a.y};
           } else {
@@ -290,7 +297,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
         for (int y = 0; y < kUnitY; ++y) {
           const int Y = Y0 + y;
           if (Y >= ya && Y < yb) {
-            const C2* sy = ss + (Y * R + r0) * KT + kk;
+            const C2* sy = ss + Y * XS + r0 * KT + kk;
 #pragma unroll
             for (int r = 0; r < 8; ++r)
               if (r0 + r < R) {
@@ -343,13 +350,15 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
         C2 h[8], h2[8];
 #pragma unroll
         for (int r = 0; r < 8; ++r) h[r] = h2[r] = C2{T(0), T(0)};
-        // Y < X: pair index row0[Y] + (X - Y); Y >= X: row0[X] + (Y - X), contiguous
-        for (int Y = 0; Y < S; ++Y) {
-          const int pi = Y < X ? row0[Y] + (X - Y) : row0[X] + (Y - X);
-          const T gh = gs[pi * KT + kk];
-          T gh2 = T(0);
-          if (two) gh2 = gs[(Y < X2 ? row0[Y] + (X2 - Y) : row0[X2] + (Y - X2)) * KT + kk];
-          const C2* sy = ss + (Y * R + r0) * KT + kk;
+        // pair index of (X, Y): row0[Y] + (X - Y) for Y < X, row0[X] + (Y - X) for Y >= X; both
+        // advance without a table read: +(S - Y - 1) per Y below the diagonal, +1 above it
+        int pa = X, pb2 = two ? X2 : 0;   // row0[0] + X, row0[0] + X2
+        const C2* sy = ss + r0 * KT + kk;
+        for (int Y = 0; Y < S; ++Y, sy += XS) {
+          const T gh = gs[pa * KT + kk];
+          const T gh2 = two ? gs[pb2 * KT + kk] : T(0);
+          pa += Y < X ? S - Y - 1 : 1;
+          pb2 += Y < X2 ? S - Y - 1 : 1;
 #pragma unroll
           for (int r = 0; r < 8; ++r)
             if (r0 + r < R) {
@@ -411,8 +420,8 @@ bool filter_kt_valid(int kt, int S, int R, size_t tsize) {
   return FilterTileSmem::bytes(S, R, kt, tsize) <= 220 * 1024;
 }
 
-template <typename T, int KT>
-static int launch_tiled(const MeshDev& g, const MeshGeom& mg, const CellInfo* ci,
+template <typename T, int KT, int RF>
+static int launch_tiled_r(const MeshDev& g, const MeshGeom& mg, const CellInfo* ci,
                         const typename GreenPairOf<T>::type* gp, const float4* gtab, const Tables* tab,
                         const float* deconv, int spme, typename Cplx<T>::type* sp, double* part, int* n_blocks,
                         cudaStream_t s) {
@@ -425,8 +434,8 @@ static int launch_tiled(const MeshDev& g, const MeshGeom& mg, const CellInfo* ci
     cudaFuncAttributes fa{};
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
-        cudaFuncGetAttributes(&fa, k_filter_tiled<T, KT>) != cudaSuccess ||
-        cudaFuncSetAttribute(k_filter_tiled<T, KT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncGetAttributes(&fa, k_filter_tiled<T, KT, RF>) != cudaSuccess ||
+        cudaFuncSetAttribute(k_filter_tiled<T, KT, RF>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              optin - (int)fa.sharedSizeBytes) != cudaSuccess) {
       set_error("filter", "could not raise the shared-memory limit of the tiled filter");
       return FD3_ECUDA;
@@ -438,7 +447,7 @@ static int launch_tiled(const MeshDev& g, const MeshGeom& mg, const CellInfo* ci
     return FD3_EINVAL;
   }
   int per_sm = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_filter_tiled<T, KT>, kFilterThreads, smem) !=
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_filter_tiled<T, KT, RF>, kFilterThreads, smem) !=
           cudaSuccess || per_sm < 1)
     per_sm = 1;
   const size_t Mh = (size_t)mg.n[0] * mg.n[1] * mg.nzh;
@@ -447,10 +456,20 @@ static int launch_tiled(const MeshDev& g, const MeshGeom& mg, const CellInfo* ci
   if (blocks > ntile) blocks = ntile;
   if (blocks > (size_t)filter_max_blocks()) blocks = filter_max_blocks();
   *n_blocks = (int)blocks;
-  k_filter_tiled<T, KT><<<(int)blocks, kFilterThreads, smem, s>>>(g, mg.order, spme, filter_units(mg.S), ci, gp,
+  k_filter_tiled<T, KT, RF><<<(int)blocks, kFilterThreads, smem, s>>>(g, mg.order, spme, filter_units(mg.S), ci, gp,
                                                                   gtab, tab, deconv, sp, part);
   FD3_LAUNCHED();
   return FD3_OK;
+}
+
+template <typename T, int KT>
+static int launch_tiled(const MeshDev& g, const MeshGeom& mg, const CellInfo* ci,
+                        const typename GreenPairOf<T>::type* gp, const float4* gtab, const Tables* tab,
+                        const float* deconv, int spme, typename Cplx<T>::type* sp, double* part, int* n_blocks,
+                        cudaStream_t s) {
+  if (mg.R == 8)
+    return launch_tiled_r<T, KT, 8>(g, mg, ci, gp, gtab, tab, deconv, spme, sp, part, n_blocks, s);
+  return launch_tiled_r<T, KT, 0>(g, mg, ci, gp, gtab, tab, deconv, spme, sp, part, n_blocks, s);
 }
 
 template <typename T>

@@ -183,14 +183,16 @@ static int filter_units(int S) {
   for (int y0 = 0; y0 < S; y0 += kUnitY) n += (y0 + kUnitY < S ? y0 + kUnitY : S);
   return n;
 }
-// The spectrum tile keeps species X's R rows of KT values at X (R KT + kTilePad) + r KT: the pad
-// puts the rows of consecutive species, read together by the slots of one warp in phase B, on
-// different shared-memory banks (R KT is a multiple of the 32 banks for the usual R and KT).
-constexpr int kTilePad = 4;
+// The spectrum tile keeps species X's R rows of KT values at X (R KT + pad) + r KT. In phase B the
+// slots of one warp read rows of consecutive species; a 64-bit shared load is served per
+// half-warp (16 lanes = 16 / KT slots of KT values each), so the species stride is padded to
+// KT modulo 16 complex values: consecutive species then start KT values (one slot's width)
+// apart in the banks and a half-warp's loads do not collide.
+__host__ __device__ inline int tile_pad(int R, int KT) { return (((KT - R * KT) % 16) + 16) % 16; }
 struct FilterTileSmem {
   static size_t bytes(int S, int R, int kt, size_t tsize) {
     const size_t C = (size_t)S * R, np = (size_t)S * (S + 1) / 2;
-    size_t b = (C * kt + (size_t)S * kTilePad) * 2 * tsize;   // spectrum tile
+    size_t b = (C * kt + (size_t)S * tile_pad(R, kt)) * 2 * tsize;   // spectrum tile
     b += 32 * tsize;                                // lambda_r
     b += np * kt * tsize;                           // Gh tile
     b += (size_t)filter_units(S) * sizeof(uint32_t); // units (X, Y0)
@@ -216,7 +218,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
   const int S = g.S, R = RF > 0 ? RF : g.R, C = S * R, NP = S * (S + 1) / 2;
   // sections in decreasing alignment: T-sized arrays first, then the 4-byte tables
   C2* ss = reinterpret_cast<C2*>(smem_raw);                  // [S][R KT + kTilePad]
-  const int XS = R * KT + kTilePad;                          // species stride of the tile
+  const int XS = R * KT + tile_pad(R, KT);                   // species stride of the tile
   T* lam = reinterpret_cast<T*>(ss + (size_t)S * XS);        // [32]
   T* gs = lam + 32;                                          // [NP][KT]
   uint32_t* units = reinterpret_cast<uint32_t*>(gs + (size_t)NP * KT);
@@ -245,7 +247,7 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
     for (int e = threadIdx.x; e < C * KT; e += kFilterThreads) {
       const int c = e / KT, j = e % KT;
       const size_t k = k0 + j;
-      ss[e + (c / R) * kTilePad] = k < Mh ? spec[(size_t)c * Mh + k] : C2{T(0), T(0)};
+      ss[e + (c / R) * (XS - R * KT)] = k < Mh ? spec[(size_t)c * Mh + k] : C2{T(0), T(0)};
     }
     const size_t k = k0 + kk;
     const bool valid = k < Mh;

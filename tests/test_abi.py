@@ -84,6 +84,8 @@ def test_invalid_arguments_return_status_codes():
     assert lib.fd3_plan_set_tuning(None, _native.TUNE_FILTER_KT, 4) == _native.FD3_EINVAL
     v = ctypes.c_int32()
     assert lib.fd3_plan_get_tuning(None, _native.TUNE_FILTER_KT, ctypes.byref(v)) == _native.FD3_EINVAL
+    assert lib.fd3_plan_set_tuning(None, _native.TUNE_XPENCIL, 4) == _native.FD3_EINVAL
+    assert lib.fd3_probe_pencil_traffic(None, None, 0, None) == _native.FD3_EINVAL
     # degenerate cell, non-positive cutoff
     nb = (ctypes.c_int32 * 3)()
     rr = (ctypes.c_int32 * 3)()

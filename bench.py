@@ -38,7 +38,10 @@ def parse():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--impl", default="fd3", choices=["fd3", "reference"])
+    ap.add_argument("--impl", default="fd3", choices=["fd3", "reference", "reference-gpu"],
+                    help="'reference-gpu': only the reference package's float64 torch path on this GPU "
+                         "(the headline run starts it as a child process for the plain_fp64_reference_gpu block)")
+    ap.add_argument("--no-reference-gpu", action="store_true")
     ap.add_argument("--reps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
@@ -235,22 +238,35 @@ def stage_bytes(stage: str, n: int, mesh, C: int, R: int, b: int) -> float:
     return 0.0
 
 
-def cpu_baseline_port(threads: int, reps: int = 2):
-    """The oracle (CPU float64 restatement of the reference) on a bounded sample."""
+def cpu_baseline_port(threads: int, reps_list=(1, 2, 3)):
+    """The oracle (CPU float64 restatement of the reference, neighbour search included) timed on
+    the host cores at the 1x1x1, 2x2x2 and 3x3x3 replicas of the SiO2 box (648, 5,184 and
+    17,496 atoms): one warm-up and one timed E+F+stress evaluation each."""
     from fourierd3_b200 import structures as st
     from oracle.reference_port import OracleFourierD3
 
     torch.set_num_threads(threads)
-    p, c, z = st.sio2_scaled(reps)
-    o = OracleFourierD3(z, c, method="spme", mesh_spacing=1.2, interpolation_nodes=5, c6tol=1.0, r_cut=6.0)
-    o.calculate(p, c)                      # warm-up (decomposition cache, allocator)
-    t0 = time.perf_counter()
-    o.calculate(p, c)
-    dt = time.perf_counter() - t0
-    return len(z) / dt, dt, len(z)
+    out = {}
+    for reps in reps_list:
+        p, c, z = st.sio2_scaled(reps)
+        o = OracleFourierD3(z, c, method="spme", mesh_spacing=1.2, interpolation_nodes=5, c6tol=1.0, r_cut=6.0)
+        o.calculate(p, c)                      # warm-up (decomposition cache, allocator)
+        t0 = time.perf_counter()
+        o.calculate(p, c)
+        dt = time.perf_counter() - t0
+        out[len(z)] = (len(z) / dt, dt)
+    return out
+
+
+REF_SAMPLE_WORKLOAD = "sio2_5184_spme_p5_h1.2_E+F+stress"
 
 
 def run_reference(args, ws, rank):
+    """Reference arm: the reference algorithm's CPU path on the host cores. The reference's own
+    dependencies (torch-pme, ase, matscipy) are not installable offline, so the arm times the
+    oracle -- the float64 CPU restatement of the reference, neighbour search included -- with
+    every host thread, on a bounded sample: the 5,184-atom 2x2x2 replica of the benchmarked
+    SiO2 box (the 139,968-atom box takes about a minute per evaluation on the host)."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
@@ -262,21 +278,109 @@ def run_reference(args, ws, rank):
     o = OracleFourierD3(z, c, method="spme", mesh_spacing=1.2, interpolation_nodes=5, c6tol=1.0, r_cut=6.0)
     for _ in range(args.warmup):
         o.calculate(p, c)
-    t0 = time.perf_counter()
+    per = []
     for _ in range(args.steps):
+        t0 = time.perf_counter()
         o.calculate(p, c)
-    dt = (time.perf_counter() - t0) / args.steps
+        per.append(time.perf_counter() - t0)
+    dt = float(np.median(per))
     val = len(z) / dt
-    sample = f"one E+F+stress evaluation per step of the 5,184-atom 2x2x2 replica of the same SiO2 box (128^3 mesh)"
+    sample = ("one E+F+stress evaluation per step of the 5,184-atom 2x2x2 replica of the benchmarked SiO2 box "
+              "(128^3 mesh), neighbour search included; median of the timed steps")
     line = {
         "metric": METRIC, "value": val, "unit": "atoms/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": WORKLOAD, "sample": sample, "method": "spme", "order": 5},
+        "config": {"workload": REF_SAMPLE_WORKLOAD, "sample_of": WORKLOAD, "n_atoms": len(z), "method": "spme",
+                   "order": 5},
         "cpu_baseline": {"value": val, "unit": "atoms/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": val, "unit": "atoms/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
+
+
+def run_reference_gpu(args, local):
+    """The metric's denominator, "plain FP64 on the same B200": the reference package's own
+    float64 torch path on this GPU. The package (installed unmodified in baseline/_ref) is driven
+    through its ASE calculator, FourierD3ASECalculator.calculate (calculator.py:125-192: strain,
+    _update_cell, forward, autograd backward, results copied to the host), in float64 at the
+    benchmarked box. Its third-party imports are satisfied by the committed stand-ins in
+    tests/golden/_shims (torch-pme's mesh size, k-vectors and spline weights restated in plain
+    torch; not installable offline), and its table loaders, which read data files the package
+    does not ship, return this repository's copies of the same tables (the C6^ref table being the
+    synthetic stand-in the kernels use). The neighbour list is built once, outside the timed
+    region, as the reference's own timing script does (papercode/get_scaling.py:69); it is the
+    same pair set matscipy returns. Prints one JSON line."""
+    device = torch.device("cuda", local)
+    torch.cuda.set_device(device)
+    ref_root = os.path.join(REPO, "baseline", "_ref")
+    out = {"impl": "reference-gpu-fp64"}
+    if not os.path.exists(os.path.join(ref_root, "fourierd3", "core.py")):
+        out["unavailable"] = "the reference package is not installed in baseline/_ref"
+        print(json.dumps(out), flush=True)
+        return
+    sys.path[:0] = [ref_root, os.path.join(REPO, "tests", "golden", "_shims")]
+    import fourierd3
+    import fourierd3.core as rcore
+    import fourierd3.pair_pot as rpp
+    import fourierd3.utils as rutils
+    from ase import Atoms
+
+    from fourierd3_b200 import structures as st
+    from fourierd3_b200 import tables
+    from fourierd3_b200.engine import neighbour_list
+
+    t = tables.load_tables()
+    rutils.load_c6ref = lambda types: tables.c6ref_matrix(list(types))
+    rcore.load_rcov = lambda: torch.from_numpy(t["rcov"].copy())
+    rcore.load_cnref = lambda: torch.from_numpy(t["cnref"].copy())
+    rpp.load_sqrtQz = lambda types, device, dtype=torch.float32: \
+        torch.from_numpy(t["sqrtQz"].copy())[types].to(device=device, dtype=dtype)
+    rpp.load_en = lambda: torch.from_numpy(t["en"].copy())
+    rpp.load_rcov_cn = lambda: torch.from_numpy(t["rcov_cn"].copy())
+
+    pos, cell, nums = st.sio2_scaled(args.reps)
+    t0 = time.perf_counter()
+    calc = fourierd3.FourierD3ASECalculator(dtype=torch.float64, device=device, method="spme", mesh_spacing=1.2,
+                                            interpolation_nodes=5, c6tol=1.0, r_cut=6.0)
+    atoms = Atoms(nums, pos, cell)
+    calc._build_model(atoms)
+    i, j, S = neighbour_list(torch.tensor(pos, dtype=torch.float64, device=device), cell, 6.0)
+    edges = (torch.stack([i, j]), S.to(torch.float64))
+    calc._build_graph = lambda atoms_, rcut=None: edges
+    setup_s = time.perf_counter() - t0
+    torch.cuda.reset_peak_memory_stats(device)
+    ms_med, ms_mean = time_steps_stats(lambda: calc.calculate(atoms), args.steps, args.warmup, 1, device)
+    out.update({
+        "value": len(nums) / (ms_med * 1e-3), "unit": "atoms/s", "ms_per_step": ms_med, "mean_ms": ms_mean,
+        "steps": args.steps, "warmup": args.warmup, "n_atoms": len(nums), "dtype": "f64",
+        "mesh": [int(v) for v in calc._model.ns_mesh], "c6_rank": int(calc._model.n_rank),
+        "energy_ev": float(calc.results["energy"]), "setup_s": setup_s,
+        "peak_mem_gb": torch.cuda.max_memory_allocated(device) / 1e9,
+        "step": "FourierD3ASECalculator.calculate with the neighbour list prebuilt (papercode/get_scaling.py:69)",
+        "third_party": "torch-pme / ase / matscipy stand-ins from tests/golden/_shims",
+        "c6_source": tables.c6_source()})
+    print(json.dumps(out), flush=True)
+
+
+def reference_gpu_subprocess(args, local, timeout_s=900):
+    """Runs run_reference_gpu in a child process (its memory is released when it exits, and a
+    failure there cannot end the headline run); returns its JSON record."""
+    cmd = [sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference-gpu", "--reps", str(args.reps),
+           "--steps", str(max(3, min(args.steps, 5))), "--warmup", "1"]
+    env = dict(os.environ, LOCAL_RANK=str(local), WORLD_SIZE="1", RANK="0")
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s, env=env)
+    except subprocess.TimeoutExpired:
+        return {"impl": "reference-gpu-fp64", "unavailable": f"did not finish within {timeout_s} s"}
+    for line in reversed(r.stdout.splitlines()):
+        if line.startswith("{"):
+            try:
+                return json.loads(line)
+            except ValueError:
+                break
+    tail = (r.stderr or r.stdout).strip().splitlines()[-3:]
+    return {"impl": "reference-gpu-fp64", "unavailable": f"exit {r.returncode}: " + " | ".join(tail)}
 
 
 BATCH_WORKLOAD = "batch256_N32-4096_Z1-54_spme_p5_h1.2_E+F+stress"
@@ -426,25 +530,35 @@ def run_batch(args, ws, rank, local):
         print(json.dumps(line), flush=True)
 
 
-def time_steps(fn, steps, warmup, ws, device):
+def time_steps_stats(fn, steps, warmup, ws, device):
+    """W untimed steps, then K steps bracketed by a barrier and a device synchronisation on both
+    sides, with a CUDA event on the launching stream before every step and after the last:
+    returns (median, mean) milliseconds per step."""
     for _ in range(warmup):
         fn()
     barrier(ws)
     torch.cuda.synchronize(device)
-    s = torch.cuda.Event(enable_timing=True)
-    e = torch.cuda.Event(enable_timing=True)
-    s.record()
-    for _ in range(steps):
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    evs[0].record()
+    for k in range(steps):
         fn()
-    e.record()
+        evs[k + 1].record()
     torch.cuda.synchronize(device)
     barrier(ws)
-    return s.elapsed_time(e) / steps
+    per = [evs[k].elapsed_time(evs[k + 1]) for k in range(steps)]
+    return float(np.median(per)), evs[0].elapsed_time(evs[-1]) / steps
+
+
+def time_steps(fn, steps, warmup, ws, device):
+    return time_steps_stats(fn, steps, warmup, ws, device)[0]
 
 
 def main():
     args = parse()
     ws, rank, local = dist_setup(args)
+    if args.impl == "reference-gpu":
+        run_reference_gpu(args, local)
+        return
     if args.impl == "reference":
         run_reference(args, ws, rank)
         if ws > 1:
@@ -526,8 +640,9 @@ def main():
         if prec == head:
             launches = per_step
             with ClockSampler(torch.cuda.current_device()) as cs:
-                ms = time_steps(lambda: graphs[prec](), args.steps, args.warmup, ws, device)
+                ms, ms_mean = time_steps_stats(lambda: graphs[prec](), args.steps, args.warmup, ws, device)
             clocks = cs.summary()
+            head_mean = max_over_ranks(ms_mean, ws, device)
         else:
             ms = time_steps(lambda: graphs[prec](), args.steps, args.warmup, ws, device)
         res[prec] = max_over_ranks(ms, ws, device)
@@ -586,35 +701,21 @@ def main():
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, 256^3 x 8 channels, mixed"
                               if mesh_match and dom in traffic_by_stage else None,
             "bytes_per_launch": dom_bytes, "ms_per_launch": ours[dom]}
-    if fused and dom == "filter" and head == "mixed":
-        # bandwidth ceiling of the fused x-pass kernel's access pattern: every spectrum value read
-        # and written once in that kernel's pencil order and piece size, nothing computed
-        Mh = mesh[0] * mesh[1] * (mesh[2] // 2 + 1)
-        buf = torch.zeros(C * Mh * 2, dtype=torch.float32, device=device)
-        eng = models[head].engine
-        for _ in range(2):
-            eng.probe_pencil_traffic(buf)
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        torch.cuda.synchronize(device)
-        ev0.record()
-        for _ in range(5):
-            eng.probe_pencil_traffic(buf)
-        ev1.record()
-        torch.cuda.synchronize(device)
-        pms = ev0.elapsed_time(ev1) / 5
-        ceiling = 2.0 * C * Mh * 8 / (pms * 1e-3) / 1e9
-        roof["pattern_ceiling"] = {"value": ceiling, "unit": "GB/s", "ms": pms, "frac": achieved / ceiling,
-                                   "what": "the same spectrum bytes moved in the kernel's pencil order and piece "
-                                           "size with no arithmetic (fd3_probe_pencil_traffic)"}
-        del buf
-
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        v, dt, natoms = cpu_baseline_port(threads)
-        cpu = {"value": v, "unit": "atoms/s", "cores": threads, "kind": "port",
-               "sample": f"oracle (CPU float64 restatement) one E+F+stress of the {natoms}-atom 2x2x2 replica, "
-                         f"{dt:.1f} s"}
+        sizes = cpu_baseline_port(threads)
+        big = max(sizes)
+        cpu = {"value": sizes[big][0], "unit": "atoms/s", "cores": threads, "kind": "port",
+               "sample": f"oracle (CPU float64 restatement, neighbour search included): one E+F+stress of the "
+                         f"{big}-atom 3x3x3 replica of the benchmarked box, {sizes[big][1]:.1f} s; "
+                         f"also 648 and 5,184 atoms (by_size)",
+               "by_size": {str(k): {"atoms_per_s": v, "s": t} for k, (v, t) in sorted(sizes.items())}}
+
+    # the metric's denominator: the reference package's float64 torch path on this GPU
+    ref_gpu = None
+    if rank == 0 and ws == 1 and not args.no_reference_gpu:
+        ref_gpu = reference_gpu_subprocess(args, local)
 
     ms = res[head]
     line = {
@@ -632,6 +733,13 @@ def main():
         "eager": {"value": ws * n / (eager[head] * 1e-3), "ms_per_step": eager[head],
                   "note": "the same step launched from the host without graph capture"},
         "mixed_over_fp64": res["fp64"] / ms if "fp64" in res and head == "mixed" else None,
+        "plain_fp64_reference_gpu": ref_gpu,
+        "mixed_over_reference_fp64_gpu": (ref_gpu["ms_per_step"] / ms
+                                          if ref_gpu and "ms_per_step" in ref_gpu else None),
+        "fp64_over_reference_fp64_gpu": (ref_gpu["ms_per_step"] / res["fp64"]
+                                         if ref_gpu and "ms_per_step" in ref_gpu and "fp64" in res else None),
+        "timing": {"statistic": "median of the timed steps (CUDA events per step on the launching stream)",
+                   "mean_ms_per_step": head_mean},
         "stages_ms": stages[head],
         "roofline": roof,
         "cpu_baseline": cpu,

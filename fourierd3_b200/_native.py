@@ -50,7 +50,8 @@ _SIGS = {
                                         ctypes.c_size_t, _vp, _vp, _vp, _vp, _vp]),
     "fd3_energy_forces_stress": (ctypes.c_int, [_vp, _c_int64, _vp, _vp, _dp, _vp, _c_double, _vp,
                                                 ctypes.c_size_t, _vp, _vp, _vp, _vp]),
-    "fd3_neighbor_workspace_size": (ctypes.c_int, [_c_int64, _dp, _c_double, ctypes.POINTER(ctypes.c_size_t)]),
+    "fd3_atom_terms": (ctypes.c_int, [_vp, _c_int64, _c_int64, _vp, ctypes.c_size_t, _vp, _vp, _vp]),
+    "fd3_neighbor_workspace_size":(ctypes.c_int, [_c_int64, _dp, _c_double, ctypes.POINTER(ctypes.c_size_t)]),
     "fd3_neighbor_count": (ctypes.c_int, [_c_int64, _vp, _dp, _c_double, _vp, ctypes.c_size_t,
                                           ctypes.POINTER(_c_int64), _vp]),
     "fd3_neighbor_fill": (ctypes.c_int, [_c_int64, _vp, _dp, _c_double, _vp, ctypes.c_size_t, _c_int64, _vp, _vp,
@@ -58,7 +59,6 @@ _SIGS = {
     "fd3_neighbor_fill_static": (ctypes.c_int, [_c_int64, _vp, _dp, _c_double, _c_int64, _vp, _vp, _vp,
                                                 ctypes.POINTER(_c_int64), _vp]),
     "fd3_profile_enable": (ctypes.c_int, [_vp, _c_int32]),
-    "fd3_probe_pencil_traffic": (ctypes.c_int, [_vp, _vp, ctypes.c_size_t, _vp]),
     "fd3_profile_read": (ctypes.c_int, [_vp, _dp, _c_int32, ctypes.c_char_p, _c_int32, ctypes.POINTER(_c_int32)]),
     "fd3_last_error": (ctypes.c_char_p, []),
     "fd3_launch_count": (_c_int64, []),

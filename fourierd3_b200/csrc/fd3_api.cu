@@ -709,6 +709,19 @@ extern "C" int fd3_energy_forces_stress(fd3_plan* p, int64_t n_atoms, const doub
   return FD3_OK;
 }
 
+// ------------------------------------------------------------------ per-atom read-back
+extern "C" int fd3_atom_terms(const fd3_plan* p, int64_t n_atoms, int64_t n_bins, const void* d_work,
+                              size_t work_bytes, double* d_cn, double* d_c6, void* stream) {
+  if (!p || n_atoms < 1 || n_atoms > (int64_t)1 << 30 || n_bins < 0 || (!d_cn && !d_c6)) return FD3_EINVAL;
+  Work w;
+  FD3_TRY(check_work(p, n_atoms, n_bins, const_cast<void*>(d_work), work_bytes, w));
+  cudaStream_t s = (cudaStream_t)stream;
+  if (d_cn) FD3_CUDA(cudaMemcpyAsync(d_cn, w.cn, sizeof(double) * n_atoms, cudaMemcpyDeviceToDevice, s));
+  if (d_c6)
+    FD3_CUDA(cudaMemcpyAsync(d_c6, w.c6, sizeof(double) * n_atoms * p->R, cudaMemcpyDeviceToDevice, s));
+  return FD3_OK;
+}
+
 // ------------------------------------------------------------------ neighbour export
 namespace {
 struct NbrWork {
@@ -747,7 +760,10 @@ int nbr_prepare(int64_t n, const double* d_pos, const double* h_cell, double r_c
 
 extern "C" int fd3_neighbor_workspace_size(int64_t n, const double* h_cell, double r_cut, size_t* bytes) {
   CellGrid g;
-  if (!bytes) return FD3_EINVAL;
+  if (!bytes || !h_cell || n < 1 || n > (int64_t)1 << 30) {
+    set_error("fd3_neighbor_workspace_size", "need a cell, an output pointer and 1 <= n_atoms <= 2^30");
+    return FD3_EINVAL;
+  }
   FD3_TRY(make_cell_grid(h_cell, r_cut, &g));
   Carver c;
   NbrWork w;
@@ -785,19 +801,6 @@ extern "C" int fd3_neighbor_fill(int64_t n, const double* d_pos, const double* h
   if (total > capacity) return FD3_ECAPACITY;
   FD3_TRY(launch_nbr_fill(g, (int)n, w.cl, d_pos, w.row_start, d_src, d_dst, d_shift, s));
   return FD3_OK;
-}
-
-// ------------------------------------------------------------------ access-pattern probe
-extern "C" int fd3_probe_pencil_traffic(const fd3_plan* p, void* d_buf, size_t bytes, void* stream) {
-  if (!p || !d_buf || p->method == FD3_METHOD_EWALD) return FD3_EINVAL;
-  const size_t need = (size_t)p->S * p->R * p->mg.n[0] * p->mg.n[1] * p->mg.nzh * 2 * sizeof(float);
-  if (bytes < need) {
-    set_error("fd3_probe_pencil_traffic", "buffer smaller than the float spectrum of the plan");
-    return FD3_EINVAL;
-  }
-  int kz = xfilter_pencil(p->mg, 0);
-  if (kz < 1) kz = 4;
-  return launch_probe_pencil(p->mg, kz, d_buf, (cudaStream_t)stream);
 }
 
 // ------------------------------------------------------------------ profiling

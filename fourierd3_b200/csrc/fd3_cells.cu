@@ -32,6 +32,10 @@ static void inv3_host(const double* m, double* inv, double* det_out) {
 }
 
 int make_cell_grid(const double* h_cell, double r_cut, CellGrid* g) {
+  if (!h_cell || !g) {
+    set_error("cell grid", "null cell");
+    return FD3_EINVAL;
+  }
   if (!(r_cut > 0)) return FD3_EINVAL;
   double det;
   inv3_host(h_cell, g->inv, &det);

@@ -143,8 +143,6 @@ int launch_xfilter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, 
                    int* n_blocks, cudaStream_t s);
 // kz width of the fused x-pass pencils for this mesh (0: the fused path does not apply)
 int xfilter_pencil(const MeshGeom& mg, int is_double);
-// bandwidth probe of the fused x-pass access pattern on a float spectrum-shaped buffer
-int launch_probe_pencil(const MeshGeom& mg, int KZ, void* buf, cudaStream_t s);
 // mixed form: per-call table of G and its k-derivatives per species pair (gtab of the filter)
 int launch_green_table(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab, void* table,
                        cudaStream_t s);

@@ -19,7 +19,10 @@
 //    threads, or two streams, running it at the same time -- race on the array and must be
 //    serialised by the caller;
 //  * the first call on a device looks up the array's device address (cudaGetSymbolAddress) with
-//    that device current and caches it; make that first call before any stream capture.
+//    that device current and caches it; make that first call before any stream capture. The
+//    cached address belongs to the device's primary context: after cudaDeviceReset (which
+//    destroys that context) it is stale, so do not call this entry point again in a process
+//    that has reset the device.
 #include <stdio.h>
 
 #include <mutex>
@@ -69,6 +72,10 @@ int scratch_address(void** out) {
 extern "C" int fd3_neighbor_fill_static(int64_t n_atoms, const double* d_pos_ang, const double* h_cell_ang,
                                         double r_cut_ang, int64_t capacity, int64_t* d_src, int64_t* d_dst,
                                         int32_t* d_shift, int64_t* h_count, void* stream) {
+  if (!d_pos_ang || !h_cell_ang || !d_src || !d_dst || !d_shift || !h_count) {
+    fd3::set_error("fd3_neighbor_fill_static", "null argument");
+    return FD3_EINVAL;
+  }
   size_t need = 0;
   int rc = fd3_neighbor_workspace_size(n_atoms, h_cell_ang, r_cut_ang, &need);
   if (rc) return rc;

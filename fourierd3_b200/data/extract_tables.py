@@ -7,9 +7,9 @@ loaded by ``src/fourierd3/utils.py:76-127``. They are physical parameters
 electronegativities), not code; the drop-in must use the identical values,
 including their float32 storage precision, so they are copied bit for bit.
 
-Run once, in a checkout that has the reference mounted::
+Run once, with the reference checkout's data directory as the argument::
 
-    python fourierd3_b200/data/extract_tables.py /root/reference/data
+    python fourierd3_b200/data/extract_tables.py <reference checkout>/data
 
 ``reference-c6.pt`` is absent from the reference checkout; it is not
 extracted (see ``fourierd3_b200/tables.py`` for how the C6 table is obtained).
@@ -33,4 +33,6 @@ def main(src_dir: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference/data")
+    if len(sys.argv) != 2:
+        sys.exit("usage: extract_tables.py <reference checkout>/data")
+    main(sys.argv[1])

@@ -187,16 +187,25 @@ class Engine:
             out[name] = int(v.value)
         return out
 
-    def probe_pencil_traffic(self, buf: torch.Tensor) -> None:
-        """Measurement helper: read and write back unchanged every value of ``buf`` (a device
-        buffer of at least S*R*nx*ny*(nz/2+1) complex floats) in the fused x-pass kernel's
-        pencil order and piece size, on the current stream. Timing it gives that access
-        pattern's bandwidth ceiling; it computes nothing."""
-        nbytes = buf.numel() * buf.element_size()
-        if not (buf.is_cuda and buf.is_contiguous()):
-            raise ValueError("probe_pencil_traffic needs a contiguous CUDA buffer")
-        _native.check(_native.lib().fd3_probe_pencil_traffic(self._plan, buf.data_ptr(), nbytes,
-                                                             _stream_ptr(buf.device)), "fd3_probe_pencil_traffic")
+    def atom_terms(self, n_atoms: int, cell_ang: Optional[np.ndarray] = None, r_cut_ang: float = 0.0,
+                   work: Optional[torch.Tensor] = None):
+        """Per-atom CN (after cncorr) and rank-r C6 factors (n_atoms, r) of the last call that used
+        this engine's workspace (or ``work``): the fused call when ``cell_ang`` is given, the
+        edge-list call otherwise (src/fourierd3/core.py:323-386, 449-478, 525-532)."""
+        nbins = 0
+        if cell_ang is not None:
+            nb, _ = self.cell_grid(cell_ang, r_cut_ang)
+            nbins = nb[0] * nb[1] * nb[2]
+        work = self._work if work is None else work
+        if work is None:
+            raise RuntimeError("atom_terms: no compute call has used this engine's workspace yet")
+        cn = torch.empty(n_atoms, dtype=torch.float64, device=self.device)
+        c6 = torch.empty((n_atoms, self.setup.n_rank), dtype=torch.float64, device=self.device)
+        _native.check(_native.lib().fd3_atom_terms(self._plan, n_atoms, nbins, ctypes.c_void_p(work.data_ptr()),
+                                                   work.numel(), ctypes.c_void_p(cn.data_ptr()),
+                                                   ctypes.c_void_p(c6.data_ptr()),
+                                                   ctypes.c_void_p(_stream_ptr(self.device))), "fd3_atom_terms")
+        return cn, c6
 
     def profile(self, on: bool = True) -> None:
         """Record CUDA events between pipeline stages of the following calls."""

@@ -124,9 +124,9 @@ def decomp(types: Sequence[int], c6tol: float, verbose: bool = False, seed: int 
         eigs, vecs = eigsh(m, k=k, v0=v0)
     err = _maxrel_err(m, vecs @ np.diag(eigs) @ vecs.T)
     if verbose:
-        print(f"Using {k}-rank decomposition with maximum relative error: {err * 100} %")
+        print(f"C6 decomposition: rank {k}, largest relative entry error {err * 100:.4g} %")
         if k == max_rank and err * 100 >= c6tol:
-            print(f"Warning: reached maximum rank {max_rank} without meeting tolerance {c6tol} %")
+            print(f"C6 decomposition: tolerance {c6tol} % not met at the largest rank tried ({max_rank})")
     return eigs, vecs, err
 
 

@@ -154,6 +154,16 @@ FD3_API int fd3_energy_forces_stress(fd3_plan* plan, int64_t n_atoms, const doub
                              double* d_forces, double* d_stress, void* stream);
 
 /*
+ * Per-atom intermediates of the last compute call that used this workspace: the coordination
+ * numbers after the optional cncorr correction (FourierD3.compute_cn_smooth, core.py:323-386)
+ * and the rank-r C6 factors c[i, r] = sum_p w_ip V[Z_i, p, r] (core.py:449-478, 525-532),
+ * row-major (n_atoms, r). n_atoms and n_bins must be those of that call (n_bins = 0 after
+ * fd3_energy_edges). Either output may be NULL. Stream-ordered device-to-device copies.
+ */
+FD3_API int fd3_atom_terms(const fd3_plan* plan, int64_t n_atoms, int64_t n_bins, const void* d_work,
+                           size_t work_bytes, double* d_cn, double* d_c6, void* stream);
+
+/*
  * Neighbour list export (replaces matscipy.neighbours.neighbour_list("ijS"),
  * calculator.py:94-123): all directed pairs (i, j, S) with
  * |x_j - x_i + S.cell| < r_cut, both directions, self-images included, (i,i,0) excluded.
@@ -179,7 +189,8 @@ FD3_API int fd3_neighbor_fill(int64_t n_atoms, const double* d_pos_ang, const do
  * array and leave their data in it (the parts that must start at zero are cleared on each
  * call), so calls that overlap on the GPU race and must be serialised by the caller. The
  * first call on a device looks up the array's address with that device current; make it
- * before any stream capture.
+ * before any stream capture. The address is cached for the life of the process, so the entry
+ * point must not be used after cudaDeviceReset on that device.
  */
 FD3_API int fd3_neighbor_fill_static(int64_t n_atoms, const double* d_pos_ang, const double* h_cell_ang,
                                      double r_cut_ang, int64_t capacity, int64_t* d_src, int64_t* d_dst,
@@ -192,13 +203,6 @@ FD3_API int fd3_neighbor_fill_static(int64_t n_atoms, const double* d_pos_ang, c
 FD3_API int fd3_profile_enable(fd3_plan* plan, int32_t on);
 FD3_API int fd3_profile_read(fd3_plan* plan, double* ms, int32_t max_stages, char* names, int32_t names_len,
                              int32_t* n_stages);
-
-/* Measurement helper (no reference counterpart; no compute path calls it): reads and writes
- * back unchanged every value of d_buf, a buffer shaped like the plan's float half spectrum
- * (S*R channels, (nx, ny, nz/2+1) complex float; bytes >= S*R*nx*ny*(nz/2+1)*8), pencil by
- * pencil in the order and piece size of the fused x-pass kernel (FD3_TUNE_XPENCIL width in
- * effect, else 4). Timing it gives the bandwidth ceiling of that kernel's access pattern. */
-FD3_API int fd3_probe_pencil_traffic(const fd3_plan* plan, void* d_buf, size_t bytes, void* stream);
 
 /* Last CUDA / cuFFT error text of the calling thread (static storage). */
 FD3_API const char* fd3_last_error(void);

@@ -11,7 +11,7 @@ stress -- is the reference's code, executed unmodified.
 
 Usage (needs the reference checkout; writes tests/golden/*.npz)::
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <reference checkout>
 """
 from __future__ import annotations
 
@@ -102,4 +102,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <reference checkout>")
+    main(sys.argv[1])

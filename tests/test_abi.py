@@ -85,7 +85,6 @@ def test_invalid_arguments_return_status_codes():
     v = ctypes.c_int32()
     assert lib.fd3_plan_get_tuning(None, _native.TUNE_FILTER_KT, ctypes.byref(v)) == _native.FD3_EINVAL
     assert lib.fd3_plan_set_tuning(None, _native.TUNE_XPENCIL, 4) == _native.FD3_EINVAL
-    assert lib.fd3_probe_pencil_traffic(None, None, 0, None) == _native.FD3_EINVAL
     # degenerate cell, non-positive cutoff
     nb = (ctypes.c_int32 * 3)()
     rr = (ctypes.c_int32 * 3)()
@@ -93,3 +92,12 @@ def test_invalid_arguments_return_status_codes():
     assert lib.fd3_cell_grid(_native.dptr(flat), 6.0, nb, rr) == _native.FD3_EINVAL
     assert lib.fd3_cell_grid(_native.dptr(cell), 0.0, nb, rr) == _native.FD3_EINVAL
     assert lib.fd3_neighbor_workspace_size(10, _native.dptr(flat), 6.0, ctypes.byref(nbytes)) == _native.FD3_EINVAL
+    # a null cell or an empty box is an argument error, not a host crash
+    assert lib.fd3_cell_grid(None, 6.0, nb, rr) == _native.FD3_EINVAL
+    assert lib.fd3_neighbor_workspace_size(10, None, 6.0, ctypes.byref(nbytes)) == _native.FD3_EINVAL
+    assert lib.fd3_neighbor_workspace_size(0, _native.dptr(cell), 6.0, ctypes.byref(nbytes)) == _native.FD3_EINVAL
+    count = ctypes.c_int64()
+    assert lib.fd3_neighbor_fill_static(10, None, None, 6.0, 16, None, None, None, ctypes.byref(count),
+                                        None) == _native.FD3_EINVAL
+    assert lib.fd3_energy_forces_stress(None, 10, None, None, None, None, 6.0, None, 0, None, None, None,
+                                        None) == _native.FD3_EINVAL

@@ -20,7 +20,10 @@ def test_reference_arm_json_line():
     assert d["metric"].startswith("E+F+stress atoms/s")
     assert d["unit"] == "atoms/s" and d["higher_is_better"] is True
     assert d["value"] > 0 and d["steps"] == 1 and d["warmup"] == 1
-    assert d["config"]["workload"] == "sio2_139968_spme_p5_h1.2_E+F+stress"
+    # the arm times a bounded sample of the benchmarked workload and names both
+    assert d["config"]["workload"] == "sio2_5184_spme_p5_h1.2_E+F+stress"
+    assert d["config"]["sample_of"] == "sio2_139968_spme_p5_h1.2_E+F+stress"
+    assert d["config"]["n_atoms"] == 5184
     cb = d["cpu_baseline"]
     assert cb["kind"] in ("port", "reference") and cb["cores"] >= 1 and cb["value"] == d["value"]
     assert d["e2e"]["h2d_bytes_per_step"] == 0 and d["e2e"]["d2h_bytes_per_step"] == 0

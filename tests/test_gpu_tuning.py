@@ -149,25 +149,3 @@ def test_autotune_fft_x_picks_a_timed_path(cuda_device):
     assert len(fused) == 1 and set(fused[0]) == {"0", "1/1", "1/2", "1/4"}   # SiO2: 64^3, 2 species
     e = b()[0]
     assert torch.allclose(e, e0, rtol=2e-6, atol=0.0)
-
-
-def test_pencil_traffic_probe_leaves_the_buffer_unchanged(cuda_device):
-    """fd3_probe_pencil_traffic reads and writes back every value of a spectrum-shaped buffer in
-    the fused x-pass order (pencil widths 4 and 1); the data are unchanged and a buffer smaller
-    than the plan's float spectrum is refused."""
-    from fourierd3_b200 import D3Model, structures as st
-
-    pos, cell, z = st.sio2_box(0)
-    m = D3Model(z, cell, precision="mixed", device=cuda_device, **KW)
-    nx, ny, nz = m.mesh
-    n = m.setup.n_species * m.setup.n_rank * nx * ny * (nz // 2 + 1) * 2
-    g = torch.Generator(device=cuda_device).manual_seed(5)
-    ref = torch.randn(n, generator=g, device=cuda_device)
-    for kz in (4, 1):
-        m.engine.set_tuning(fft_x=1, xpencil=kz)
-        buf = ref.clone()
-        m.engine.probe_pencil_traffic(buf)
-        torch.cuda.synchronize()
-        assert torch.equal(buf, ref), kz
-    with pytest.raises(ValueError):
-        m.engine.probe_pencil_traffic(ref[: n - 2].clone())

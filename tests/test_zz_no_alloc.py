@@ -52,6 +52,16 @@ def test_static_scratch_matches_workspace_entry_point(box, cuda_device):
         np.testing.assert_array_equal(sh.cpu().numpy(), s_ref.cpu().numpy())
 
 
+def test_static_scratch_reports_needed_capacity(cuda_device):
+    """An output one row too short: FD3_ECAPACITY, with the needed row count written back."""
+    p, c, _ = structures.sio2_box(0)
+    pos = torch.tensor(p, dtype=torch.float64, device=cuda_device)
+    n_ref = neighbour_list(pos, c, 6.0)[0].numel()
+    rc, count, *_ = _static_fill(pos, c, 6.0, n_ref - 1)
+    assert rc == _native.FD3_ECAPACITY
+    assert count == n_ref
+
+
 def test_static_scratch_rejects_oversize_input(cuda_device):
     p, c, _ = structures.sio2_box(0)
     big = structures.replicate(p, c, np.zeros(len(p), dtype=np.int64), (5, 5, 5))   # 81,000 atoms

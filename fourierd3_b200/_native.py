@@ -20,6 +20,8 @@ TUNE_SPREAD_ZC = 1
 TUNE_SPREAD_CAP = 2
 TUNE_FFT_X = 3
 TUNE_XPENCIL = 4
+TUNE_XQ = 5
+TUNE_XRANKS = 6
 
 _c_int32 = ctypes.c_int32
 _c_int64 = ctypes.c_int64
@@ -45,7 +47,8 @@ _SIGS = {
     "fd3_plan_set_tuning": (ctypes.c_int, [_vp, _c_int32, _c_int32]),
     "fd3_plan_get_tuning": (ctypes.c_int, [_vp, _c_int32, ctypes.POINTER(_c_int32)]),
     "fd3_workspace_size": (ctypes.c_int, [_vp, _c_int64, _c_int64, ctypes.POINTER(ctypes.c_size_t)]),
-    "fd3_cell_grid": (ctypes.c_int, [_dp, _c_double, ctypes.POINTER(_c_int32), ctypes.POINTER(_c_int32)]),
+    "fd3_edge_workspace_size": (ctypes.c_int, [_vp, _c_int64, _c_int64, ctypes.POINTER(ctypes.c_size_t)]),
+    "fd3_cell_grid":(ctypes.c_int, [_dp, _c_double, ctypes.POINTER(_c_int32), ctypes.POINTER(_c_int32)]),
     "fd3_energy_edges": (ctypes.c_int, [_vp, _c_int64, _vp, _vp, _vp, _c_int64, _vp, _vp, _vp, _c_int32, _vp,
                                         ctypes.c_size_t, _vp, _vp, _vp, _vp, _vp]),
     "fd3_energy_forces_stress": (ctypes.c_int, [_vp, _c_int64, _vp, _vp, _dp, _vp, _c_double, _vp,

@@ -127,8 +127,8 @@ class FourierD3(torch.nn.Module):
             raise ValueError("positions must be (n_atoms, 3) for the species given at construction")
         if edge_index.dim() != 2 or edge_index.shape[0] != 2 or shifts.shape != (edge_index.shape[1], 3):
             raise ValueError("edge_index must be (2, E) and shifts (E, 3)")
-        if edge_index.numel() and (int(edge_index.min()) < 0 or int(edge_index.max()) >= positions.shape[0]):
-            raise ValueError("edge_index refers to atoms outside 0..n_atoms-1")
+        # An edge index outside 0..n_atoms-1 is caught on the device (never dereferenced; the
+        # energy and its gradients come back NaN), so the call makes no host synchronisation.
         pos_b = positions.to(torch.float64) * self.angstrom_to_bohr                         # core.py:505
         sh_b = shifts.to(torch.float64) * self.angstrom_to_bohr                             # core.py:507
         e = _EdgeEnergy.apply(pos_b, sh_b, self.cell, edge_index.to(self.device), self._eng)

@@ -203,6 +203,8 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
       m.spread_zc = -1;
       m.spread_cap = 0;
       m.xpencil = -1;
+      m.xq = -1;
+      m.xranks = -1;
       m.fft_x = -1;   // default: off (3D cuFFT around the separate filter measured faster on B200)
       const size_t Mh = (size_t)m.n[0] * m.n[1] * m.nzh;
       m.win_axes = nullptr;
@@ -263,7 +265,7 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
       p->has_fft = true;
       p->fft_ws = ws1 > ws2 ? ws1 : ws2;
       // (y, z) planes for the fused x-pass: batch over the C channels and nx planes
-      if (xfilter_pencil(m, dp ? 1 : 0) > 0) {
+      if (xfilter_pencil(m, dp ? 1 : 0) > 0 || (!dp && xpass_applies(m, 8, 1))) {
         long long n2d[2] = {m.n[1], m.n[2]};
         const long long pr = (long long)m.n[1] * m.n[2], pc = (long long)m.n[1] * m.nzh;
         size_t ws3 = 0, ws4 = 0;
@@ -306,6 +308,23 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
   return FD3_OK;
 }
 
+// Unit shape of the TMA x-pass in effect: q values per unit (default 16: one 128-byte line per
+// spectrum row) and ranks per unit (default 1).
+static void xpass_shape(const fd3_plan* p, int* Q, int* RG) {
+  *Q = p->mg.xq > 0 ? p->mg.xq : 16;
+  *RG = p->mg.xranks > 0 ? p->mg.xranks : 1;
+}
+static bool xpass_on(const fd3_plan* p) {
+  int Q, RG;
+  xpass_shape(p, &Q, &RG);
+  return p->method != FD3_METHOD_EWALD && p->has_fft2 && p->precision == FD3_PREC_MIXED && p->mg.fft_x == 2 &&
+         xpass_applies(p->mg, Q, RG);
+}
+static bool old_xpass_on(const fd3_plan* p) {
+  return p->method != FD3_METHOD_EWALD && p->has_fft2 && p->mg.fft_x == 1 &&
+         xfilter_pencil(p->mg, p->precision == FD3_PREC_FP64 ? 1 : 0) > 0;
+}
+
 extern "C" int fd3_plan_set_tuning(fd3_plan* p, int32_t knob, int32_t value) {
   if (!p) return FD3_EINVAL;
   if (knob == FD3_TUNE_FILTER_KT) {
@@ -327,11 +346,27 @@ extern "C" int fd3_plan_set_tuning(fd3_plan* p, int32_t knob, int32_t value) {
     return FD3_OK;
   }
   if (knob == FD3_TUNE_FFT_X) {
-    if (value < -1 || value > 1) {
-      set_error("fd3_plan_set_tuning", "fused x-pass must be -1 (default), 0 (3D FFT + filter) or 1");
+    if (value < -1 || value > 2) {
+      set_error("fd3_plan_set_tuning", "fused x-pass must be -1 (default), 0 (3D FFT + filter), 1 or 2 (TMA)");
       return FD3_EINVAL;
     }
     p->mg.fft_x = value;
+    return FD3_OK;
+  }
+  if (knob == FD3_TUNE_XQ) {
+    if (value != -1 && value != 8 && value != 16 && value != 32) {
+      set_error("fd3_plan_set_tuning", "TMA x-pass q values per unit must be -1 (default), 8, 16 or 32");
+      return FD3_EINVAL;
+    }
+    p->mg.xq = value;
+    return FD3_OK;
+  }
+  if (knob == FD3_TUNE_XRANKS) {
+    if (value != -1 && value != 1 && value != 2) {
+      set_error("fd3_plan_set_tuning", "TMA x-pass ranks per unit must be -1 (default), 1 or 2");
+      return FD3_EINVAL;
+    }
+    p->mg.xranks = value;
     return FD3_OK;
   }
   if (knob == FD3_TUNE_XPENCIL) {
@@ -373,7 +408,14 @@ extern "C" int fd3_plan_get_tuning(const fd3_plan* p, int32_t knob, int32_t* val
     return FD3_OK;
   }
   if (knob == FD3_TUNE_FFT_X) {
-    *value = (p->has_fft2 && p->mg.fft_x == 1) ? 1 : 0;
+    *value = xpass_on(p) ? 2 : old_xpass_on(p) ? 1 : 0;
+    return FD3_OK;
+  }
+  if (knob == FD3_TUNE_XQ || knob == FD3_TUNE_XRANKS) {
+    int Q = 0, RG = 0;
+    xpass_shape(p, &Q, &RG);
+    const bool ok = p->has_fft2 && p->precision == FD3_PREC_MIXED && xpass_applies(p->mg, Q, RG);
+    *value = ok ? (knob == FD3_TUNE_XQ ? Q : RG) : 0;
     return FD3_OK;
   }
   if (knob == FD3_TUNE_XPENCIL) {
@@ -428,12 +470,14 @@ struct Work {
   CellList cl;
   HitStore hits;
   EwaldWork ew;
+  EdgeIndex ei;
   void *rho, *spec, *fftw;
   void* gtab;   // mixed-form Green table
 };
 
-// K = number of cell-list bins of the fused path, 0 for the edge-list path (no cell list).
-void carve(const fd3_plan* p, int64_t N, int64_t K_in, Carver& c, Work& w) {
+// K = number of cell-list bins of the fused path, 0 for the edge-list path (no cell list);
+// E = edges of the edge-list path.
+void carve(const fd3_plan* p, int64_t N, int64_t K_in, Carver& c, Work& w, int64_t E = 0) {
   const bool fused = K_in > 0;
   const int64_t K = fused ? K_in : 1;
   const size_t es = p->precision == FD3_PREC_FP64 ? sizeof(double) : sizeof(float);
@@ -489,6 +533,15 @@ void carve(const fd3_plan* p, int64_t N, int64_t K_in, Carver& c, Work& w) {
   w.spec = c.take<char>(mesh ? C * Mh * 2 * es : 1);
   w.fftw = c.take<char>(p->fft_ws);
   w.gtab = c.take<char>(mesh && p->precision == FD3_PREC_MIXED ? green_table_bytes(p->S) : 1);
+  // edge-list path: edges sorted by source and by destination
+  w.ei.ks = c.take<int>(E);
+  w.ei.kd = c.take<int>(E);
+  w.ei.ord_s = c.take<int>(E);
+  w.ei.ord_d = c.take<int>(E);
+  w.ei.cnt = c.take<int>(N);
+  w.ei.st_s = c.take<int>(N + 1);
+  w.ei.st_d = c.take<int>(N + 1);
+  w.ei.bad = c.take<int>(1);
   // direct Ewald sum
   if (!mesh) {
     const int64_t nk = (int64_t)p->ens[0] * p->ens[1] * p->ens[2];
@@ -527,16 +580,25 @@ extern "C" int fd3_cell_grid(const double* h_cell, double r_cut, int32_t* nb3, i
   return FD3_OK;
 }
 
-static int check_work(const fd3_plan* p, int64_t N, int64_t K, void* work, size_t bytes, Work& w) {
+extern "C" int fd3_edge_workspace_size(const fd3_plan* p, int64_t n_atoms, int64_t n_edges, size_t* bytes) {
+  if (!p || !bytes || n_atoms < 0 || n_edges < 0 || n_edges > INT32_MAX) return FD3_EINVAL;
   Carver c;
-  carve(p, N, K, c, w);
+  Work w;
+  carve(p, n_atoms, 0, c, w, n_edges);
+  *bytes = c.off + 256;
+  return FD3_OK;
+}
+
+static int check_work(const fd3_plan* p, int64_t N, int64_t K, void* work, size_t bytes, Work& w, int64_t E = 0) {
+  Carver c;
+  carve(p, N, K, c, w, E);
   if (!work || bytes < c.off + 256) {
-    set_error("workspace", "smaller than fd3_workspace_size");
+    set_error("workspace", E > 0 ? "smaller than fd3_edge_workspace_size" : "smaller than fd3_workspace_size");
     return FD3_ENOMEM;
   }
   Carver c2;
   c2.base = reinterpret_cast<char*>(((uintptr_t)work + 255) & ~(uintptr_t)255);
-  carve(p, N, K, c2, w);
+  carve(p, N, K, c2, w, E);
   return FD3_OK;
 }
 
@@ -560,7 +622,8 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
   prof_mark(p, s, "mesh_sort");
   FD3_TRY(launch_spread<T>(mg, N, pos, ps, species, w.c6, w.ci, w.mstart, w.morder, w.rec, (T*)w.rho, s));
   prof_mark(p, s, "spread");
-  if (p->has_fft2 && mg.fft_x == 1) {
+  const bool tma_x = sizeof(T) == 4 && xpass_on(p);
+  if (tma_x || old_xpass_on(p)) {
     // (y, z) transforms by cuFFT; x transform, filter and inverse x transform in one kernel
     FD3_CUFFT(cufftSetStream(p->fwd2, s));
     FD3_CUFFT(cufftSetWorkArea(p->fwd2, w.fftw));
@@ -570,8 +633,15 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
       FD3_CUFFT(cufftExecR2C(p->fwd2, (cufftReal*)w.rho, (cufftComplex*)w.spec));
     prof_mark(p, s, "fft_r2c");
     if (sizeof(T) == 4) FD3_TRY(launch_green_table(mg, w.ci, p->d_green, p->d_tab, w.gtab, s));
-    FD3_TRY(launch_xfilter<T>(mg, w.ci, p->d_green, p->d_green_f, (const float4*)w.gtab, p->d_tab, p->d_deconv,
-                              p->method == FD3_METHOD_SPME, w.spec, w.kspc_part, n_kspc, s));
+    if (tma_x) {
+      int Q, RG;
+      xpass_shape(p, &Q, &RG);
+      FD3_TRY(launch_xpass(mg, Q, RG, w.ci, p->d_green_f, (const float4*)w.gtab, p->d_tab, p->d_deconv,
+                           p->method == FD3_METHOD_SPME, w.spec, w.kspc_part, n_kspc, s));
+    } else {
+      FD3_TRY(launch_xfilter<T>(mg, w.ci, p->d_green, p->d_green_f, (const float4*)w.gtab, p->d_tab, p->d_deconv,
+                                p->method == FD3_METHOD_SPME, w.spec, w.kspc_part, n_kspc, s));
+    }
     prof_mark(p, s, "filter");
     *n_mcell = 0;
     if (!need_grad) return FD3_OK;
@@ -641,23 +711,24 @@ extern "C" int fd3_energy_edges(fd3_plan* p, int64_t n_atoms, const double* d_po
                                 double* d_energy, double* d_gpos, double* d_gshift, double* d_gcell, void* stream) {
   if (!p || n_atoms < 1 || n_atoms > (int64_t)1 << 30 || !d_pos || !d_species || !d_cell || !d_energy)
     return FD3_EINVAL;
-  if (n_edges < 0 || (n_edges > 0 && (!d_src || !d_dst || !d_shift))) return FD3_EINVAL;
+  if (n_edges < 0 || n_edges > INT32_MAX || (n_edges > 0 && (!d_src || !d_dst || !d_shift))) return FD3_EINVAL;
   if (need_grad && (!d_gpos || !d_gcell || (n_edges > 0 && !d_gshift))) return FD3_EINVAL;
   cudaStream_t s = (cudaStream_t)stream;
   const int N = (int)n_atoms;
   Work w;
-  FD3_TRY(check_work(p, N, 0, d_work, work_bytes, w));
+  FD3_TRY(check_work(p, N, 0, d_work, work_bytes, w, n_edges));
   prof_begin(p, s);
   FD3_TRY(launch_cellinfo(d_cell, 1.0, w.ci, s));
-  FD3_CUDA(cudaMemsetAsync(w.cn, 0, sizeof(double) * N, s));
-  FD3_TRY(launch_cn_edges(n_edges, d_pos, d_species, d_src, d_dst, d_shift, p->d_tab, w.cn, s));
+  // edges sorted by source and destination; the CN is summed per atom in edge order
+  FD3_TRY(launch_edge_index(n_edges, N, d_src, d_dst, w.ei, s));
+  FD3_TRY(launch_cn_edges_seg(n_edges, N, d_pos, d_species, d_src, d_dst, d_shift, p->d_tab, w.ei, w.cn, s));
   int n_self = 0, n_kspc = 0, n_mcell = 0;
   FD3_TRY(launch_c6_atoms(N, d_species, p->d_tab, p->d_eigvecs, p->R, w.cn, w.c6, w.dc6, w.self_part, &n_self, s));
   prof_mark(p, s, "cn_c6");
   FD3_TRY(run_mesh(p, N, d_pos, 1.0, d_species, w, need_grad != 0, d_gpos, w.mcell_part, &n_kspc, &n_mcell, s));
   if (need_grad)
-    FD3_TRY(launch_cn_adjoint_edges(n_edges, d_pos, d_species, d_src, d_dst, d_shift, p->d_tab, w.gcn, d_gpos,
-                                    d_gshift, s));
+    FD3_TRY(launch_cn_adjoint_edges_seg(n_edges, N, d_pos, d_species, d_src, d_dst, d_shift, p->d_tab, w.gcn, w.ei,
+                                        d_gpos, d_gshift, s));
   prof_mark(p, s, "cn_adjoint");
   Partials pa{w.self_part, n_self, w.kspc_part, n_kspc, w.cnv_part, 0, w.mcell_part, n_mcell};
   FD3_TRY(launch_finalize(pa, w.ci, 0, 1.0, d_energy, need_grad ? d_gcell : nullptr, s));

@@ -715,29 +715,148 @@ int launch_cn_adjoint_cells(const CellGrid& g, int n, const CellList& cl, const 
 }
 
 // ------------------------------------------------------------------ edge-list path
-__global__ void __launch_bounds__(256) k_cn_edges(int64_t ne, const double* __restrict__ x, const int32_t* __restrict__ species,
-                           const int64_t* __restrict__ src, const int64_t* __restrict__ dst,
-                           const double* __restrict__ sh, const Tables* __restrict__ tab, double* __restrict__ cn) {
+// ------------------------------------------------------------------ edge-list path, fixed order
+// Edge keys for the stable counting sorts by source and by destination. An edge whose source
+// or destination is outside 0..n-1 raises *bad and is keyed to bucket e mod n (so no bucket
+// grows with the number of bad edges); every consumer re-checks the range and skips it.
+__global__ void __launch_bounds__(256) k_edge_keys(int64_t ne, int n, const int64_t* __restrict__ src,
+                                                  const int64_t* __restrict__ dst, int* __restrict__ ks,
+                                                  int* __restrict__ kd, int* __restrict__ bad) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= ne) return;
   const int64_t i = src[e], j = dst[e];
-  const double v0 = x[3 * j] - x[3 * i] + sh[3 * e];
-  const double v1 = x[3 * j + 1] - x[3 * i + 1] + sh[3 * e + 1];
-  const double v2 = x[3 * j + 2] - x[3 * i + 2] + sh[3 * e + 2];
-  const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-  double f, df;
-  cn_edge(r, tab->rcov[species[i]] + tab->rcov[species[j]], tab->r_cut, f, df);
-  atomicAdd(&cn[i], f);
+  const bool ok = i >= 0 && i < n && j >= 0 && j < n;
+  const int spill = (int)(e % n);
+  ks[e] = ok ? (int)i : spill;
+  kd[e] = ok ? (int)j : spill;
+  if (!ok) atomicOr(bad, 1);
 }
 
-int launch_cn_edges(int64_t n_edges, const double* pos, const int32_t* species, const int64_t* src,
-                    const int64_t* dst, const double* shift, const Tables* tab, double* cn, cudaStream_t s) {
-  if (n_edges == 0) return FD3_OK;
-  const int tb = 256;
-  k_cn_edges<<<(unsigned)((n_edges + tb - 1) / tb), tb, 0, s>>>(n_edges, pos, species, src, dst, shift, tab, cn);
+int launch_edge_index(int64_t n_edges, int n, const int64_t* src, const int64_t* dst, const EdgeIndex& ei,
+                      cudaStream_t s) {
+  FD3_CUDA(cudaMemsetAsync(ei.bad, 0, sizeof(int), s));
+  if (n_edges > 0) {
+    const int tb = 256;
+    k_edge_keys<<<(unsigned)((n_edges + tb - 1) / tb), tb, 0, s>>>(n_edges, n, src, dst, ei.ks, ei.kd, ei.bad);
+    FD3_LAUNCHED();
+  }
+  int rc = counting_sort(ei.ks, (int)n_edges, n, ei.cnt, ei.st_s, ei.ord_s, s);
+  if (rc) return rc;
+  return counting_sort(ei.kd, (int)n_edges, n, ei.cnt, ei.st_d, ei.ord_d, s);
+}
+
+// CN of atom a: the sum of the smooth-cutoff function over its source edges in edge order
+// (core.py:323-386, index_add_ on edge_index[0]); one warp per atom, lanes over the edges, a
+// fixed butterfly reduction -- the same result on every run. NaN for every atom when an edge
+// index was out of range (the range check the reference leaves to torch indexing).
+__global__ void __launch_bounds__(256) k_cn_edges_seg(int n, int64_t ne, const int* __restrict__ st,
+                                                     const int* __restrict__ ord, const double* __restrict__ x,
+                                                     const int32_t* __restrict__ species,
+                                                     const int64_t* __restrict__ src, const int64_t* __restrict__ dst,
+                                                     const double* __restrict__ sh, const Tables* __restrict__ tab,
+                                                     const int* __restrict__ bad, double* __restrict__ cn) {
+  const int lane = threadIdx.x & 31;
+  const int a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (a >= n) return;
+  const double rca = tab->rcov[species[a]];
+  double sum = 0.0;
+  for (int p = st[a] + lane; p < st[a + 1]; p += 32) {
+    const int e = ord[p];
+    const int64_t i = src[e], j = dst[e];
+    if (i != a || j < 0 || j >= n) continue;
+    const double v0 = x[3 * j] - x[3 * i] + sh[3 * (int64_t)e];
+    const double v1 = x[3 * j + 1] - x[3 * i + 1] + sh[3 * (int64_t)e + 1];
+    const double v2 = x[3 * j + 2] - x[3 * i + 2] + sh[3 * (int64_t)e + 2];
+    double f, df;
+    cn_edge(sqrt(v0 * v0 + v1 * v1 + v2 * v2), rca + tab->rcov[species[j]], tab->r_cut, f, df);
+    sum += f;
+  }
+  sum = warp_sum(sum);
+  if (lane == 0) cn[a] = *bad ? __longlong_as_double(0x7ff8000000000000LL) : sum;
+}
+
+int launch_cn_edges_seg(int64_t n_edges, int n, const double* pos, const int32_t* species, const int64_t* src,
+                        const int64_t* dst, const double* shift, const Tables* tab, const EdgeIndex& ei, double* cn,
+                        cudaStream_t s) {
+  const int wpb = 8;
+  k_cn_edges_seg<<<(n + wpb - 1) / wpb, 32 * wpb, 0, s>>>(n, n_edges, ei.st_s, ei.ord_s, pos, species, src, dst,
+                                                          shift, tab, ei.bad, cn);
   FD3_LAUNCHED();
   return FD3_OK;
 }
+
+// dE/dshift of every edge, g_e = dE/dCN_i f'(r) v / r (zero for an edge out of range).
+__global__ void __launch_bounds__(256) k_edge_grad(int64_t ne, int n, const double* __restrict__ x,
+                                                  const int32_t* __restrict__ species, const int64_t* __restrict__ src,
+                                                  const int64_t* __restrict__ dst, const double* __restrict__ sh,
+                                                  const Tables* __restrict__ tab, const double* __restrict__ gcn,
+                                                  double* __restrict__ gshift) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= ne) return;
+  const int64_t i = src[e], j = dst[e];
+  double g0 = 0, g1 = 0, g2 = 0;
+  if (i >= 0 && i < n && j >= 0 && j < n) {
+    const double v0 = x[3 * j] - x[3 * i] + sh[3 * e];
+    const double v1 = x[3 * j + 1] - x[3 * i + 1] + sh[3 * e + 1];
+    const double v2 = x[3 * j + 2] - x[3 * i + 2] + sh[3 * e + 2];
+    const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+    double f, df;
+    cn_edge(r, tab->rcov[species[i]] + tab->rcov[species[j]], tab->r_cut, f, df);
+    if (r > 1e-6) {
+      const double a = gcn[i] * df / r;
+      g0 = a * v0;
+      g1 = a * v1;
+      g2 = a * v2;
+    }
+  }
+  gshift[3 * e] = g0;
+  gshift[3 * e + 1] = g1;
+  gshift[3 * e + 2] = g2;
+}
+
+// dE/dpos_a += sum over edges into a of g_e - sum over edges out of a of g_e, each in edge order.
+__global__ void __launch_bounds__(256) k_edge_grad_atoms(int n, const int* __restrict__ st_s,
+                                                        const int* __restrict__ ord_s, const int* __restrict__ st_d,
+                                                        const int* __restrict__ ord_d,
+                                                        const double* __restrict__ gshift, double* __restrict__ gpos) {
+  const int lane = threadIdx.x & 31;
+  const int a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (a >= n) return;
+  double g[3] = {0.0, 0.0, 0.0};
+  for (int p = st_d[a] + lane; p < st_d[a + 1]; p += 32) {
+    const int64_t e = ord_d[p];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) g[c] += gshift[3 * e + c];
+  }
+  for (int p = st_s[a] + lane; p < st_s[a + 1]; p += 32) {
+    const int64_t e = ord_s[p];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) g[c] -= gshift[3 * e + c];
+  }
+#pragma unroll
+  for (int c = 0; c < 3; ++c) g[c] = warp_sum(g[c]);
+  if (lane == 0) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) gpos[3 * (int64_t)a + c] += g[c];
+  }
+}
+
+int launch_cn_adjoint_edges_seg(int64_t n_edges, int n, const double* pos, const int32_t* species,
+                                const int64_t* src, const int64_t* dst, const double* shift, const Tables* tab,
+                                const double* gcn, const EdgeIndex& ei, double* gpos, double* gshift,
+                                cudaStream_t s) {
+  if (n_edges > 0) {
+    const int tb = 256;
+    k_edge_grad<<<(unsigned)((n_edges + tb - 1) / tb), tb, 0, s>>>(n_edges, n, pos, species, src, dst, shift, tab,
+                                                                   gcn, gshift);
+    FD3_LAUNCHED();
+  }
+  const int wpb = 8;
+  k_edge_grad_atoms<<<(n + wpb - 1) / wpb, 32 * wpb, 0, s>>>(n, ei.st_s, ei.ord_s, ei.st_d, ei.ord_d, gshift, gpos);
+  FD3_LAUNCHED();
+  return FD3_OK;
+}
+
 
 // Softmax interpolation over the 7 reference CNs and the rank-r factors
 // c_r = sum_p w_p V[s, p, r] (core.py:449-478, 525-532), their CN derivative (times the
@@ -809,52 +928,6 @@ int launch_c6_atoms(int n, const int32_t* species, const Tables* tab, const doub
   return FD3_OK;
 }
 
-__global__ void __launch_bounds__(256) k_cn_adjoint_edges(int64_t ne, const double* __restrict__ x, const int32_t* __restrict__ species,
-                                   const int64_t* __restrict__ src, const int64_t* __restrict__ dst,
-                                   const double* __restrict__ sh, const Tables* __restrict__ tab,
-                                   const double* __restrict__ gcn, double* __restrict__ gpos,
-                                   double* __restrict__ gshift) {
-  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= ne) return;
-  const int64_t i = src[e], j = dst[e];
-  const double v0 = x[3 * j] - x[3 * i] + sh[3 * e];
-  const double v1 = x[3 * j + 1] - x[3 * i + 1] + sh[3 * e + 1];
-  const double v2 = x[3 * j + 2] - x[3 * i + 2] + sh[3 * e + 2];
-  const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
-  double f, df;
-  cn_edge(r, tab->rcov[species[i]] + tab->rcov[species[j]], tab->r_cut, f, df);
-  double g0 = 0, g1 = 0, g2 = 0;
-  if (r > 1e-6) {
-    const double a = gcn[i] * df / r;
-    g0 = a * v0;
-    g1 = a * v1;
-    g2 = a * v2;
-  }
-  if (gshift) {
-    gshift[3 * e] = g0;
-    gshift[3 * e + 1] = g1;
-    gshift[3 * e + 2] = g2;
-  }
-  if (gpos && (g0 != 0 || g1 != 0 || g2 != 0)) {
-    atomicAdd(&gpos[3 * j], g0);
-    atomicAdd(&gpos[3 * j + 1], g1);
-    atomicAdd(&gpos[3 * j + 2], g2);
-    atomicAdd(&gpos[3 * i], -g0);
-    atomicAdd(&gpos[3 * i + 1], -g1);
-    atomicAdd(&gpos[3 * i + 2], -g2);
-  }
-}
-
-int launch_cn_adjoint_edges(int64_t n_edges, const double* pos, const int32_t* species, const int64_t* src,
-                            const int64_t* dst, const double* shift, const Tables* tab, const double* gcn,
-                            double* gpos, double* gshift, cudaStream_t s) {
-  if (n_edges == 0) return FD3_OK;
-  const int tb = 256;
-  k_cn_adjoint_edges<<<(unsigned)((n_edges + tb - 1) / tb), tb, 0, s>>>(n_edges, pos, species, src, dst, shift, tab,
-                                                                       gcn, gpos, gshift);
-  FD3_LAUNCHED();
-  return FD3_OK;
-}
 
 // ------------------------------------------------------------------ neighbour export
 __global__ void __launch_bounds__(256) k_nbr_count(GridDev g, int n, const int* __restrict__ bin_start,

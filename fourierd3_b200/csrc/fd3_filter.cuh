@@ -133,22 +133,16 @@ __device__ __forceinline__ void virial_acc(const KPoint<T>& q, T dq, double* acc
 }
 
 
-// Filter of one k-point for up to MAXS species: G, dG and the Hermitian-averaged Gh of every
-// pair (float64 closed form, or the mixed form's table), the pair sums of the energy and virial,
-// and H_X = sum_Y Gh_XY S_Y written over the S*R spectrum values v[c * cs] (c = X R + r).
-// Ranks are processed in chunks of MAXR whose S x MAXR values are all loaded before any
-// arithmetic. Per-k terms are formed in T and accumulated in float64 into acc[0..6].
-template <typename T, int MAXS, int MAXR>
-__device__ __forceinline__ void filter_point(const KPoint<T>& q, int S, int R,
-                                             const typename GreenPairOf<T>::type* __restrict__ gp,
-                                             const float4* __restrict__ gtab, float inv_h, T s6, T s8,
-                                             const Tables* __restrict__ tab, typename Cplx<T>::type* v, size_t cs,
-                                             double* acc) {
-  using C2 = typename Cplx<T>::type;
+// G, dG and the Hermitian-averaged Gh of every species pair at one k-point (float64 closed
+// form, or the mixed form's table), each divided by the SPME window; unused slots are zero.
+template <typename T, int MAXS>
+__device__ __forceinline__ void green_block(const KPoint<T>& q, int S,
+                                            const typename GreenPairOf<T>::type* __restrict__ gp,
+                                            const float4* __restrict__ gtab, float inv_h, T s6, T s8,
+                                            T (&G)[MAXS][MAXS], T (&dG)[MAXS][MAXS], T (&Gh)[MAXS][MAXS]) {
   int tj = 0;
   HermiteF hb{};
   if constexpr (sizeof(T) == 4) table_pos(q.knorm, inv_h, tj, hb);
-  T G[MAXS][MAXS], dG[MAXS][MAXS], Gh[MAXS][MAXS];
 #pragma unroll
   for (int X = 0; X < MAXS; ++X)
 #pragma unroll
@@ -187,6 +181,22 @@ __device__ __forceinline__ void filter_point(const KPoint<T>& q, int S, int R,
           Gh[X][Y] = Gh[Y][X] = T(0.5) * (G[X][Y] + gv * q.inv_sc);
         }
   }
+}
+
+// Filter of one k-point for up to MAXS species: G, dG and Gh of every pair (green_block), the
+// pair sums of the energy and virial, and H_X = sum_Y Gh_XY S_Y written over the S*R spectrum
+// values v[c * cs] (c = X R + r). Ranks are processed in chunks of MAXR whose S x MAXR values are
+// all loaded before any arithmetic. Per-k terms are formed in T and accumulated in float64 into
+// acc[0..6].
+template <typename T, int MAXS, int MAXR>
+__device__ __forceinline__ void filter_point(const KPoint<T>& q, int S, int R,
+                                             const typename GreenPairOf<T>::type* __restrict__ gp,
+                                             const float4* __restrict__ gtab, float inv_h, T s6, T s8,
+                                             const Tables* __restrict__ tab, typename Cplx<T>::type* v, size_t cs,
+                                             double* acc) {
+  using C2 = typename Cplx<T>::type;
+  T G[MAXS][MAXS], dG[MAXS][MAXS], Gh[MAXS][MAXS];
+  green_block<T, MAXS>(q, S, gp, gtab, inv_h, s6, s8, G, dG, Gh);
   T qq = T(0), dq = T(0);
   const bool full = S == MAXS && R % MAXR == 0;   // every slot holds a channel: no predication
   const size_t xs = (size_t)R * cs;               // channel stride between species

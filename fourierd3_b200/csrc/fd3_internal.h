@@ -85,14 +85,27 @@ int launch_cn_adjoint_cells(const CellGrid& g, int n, const CellList& cl, const 
                             cudaStream_t s);
 
 // edge-list CN path
-int launch_cn_edges(int64_t n_edges, const double* pos, const int32_t* species, const int64_t* src,
-                    const int64_t* dst, const double* shift, const Tables* tab, double* cn, cudaStream_t s);
+// Edges sorted by source and by destination (stable counting sorts of the edge ids): the
+// per-atom segments the fixed-order CN sum and its adjoint walk.
+struct EdgeIndex {
+  int *ks, *kd;         // [E] source / destination keys
+  int *ord_s, *ord_d;   // [E] edge ids by source / by destination
+  int* cnt;             // [N] counting-sort scratch
+  int *st_s, *st_d;     // [N+1] segment starts
+  int* bad;             // [1] set when an edge index is outside 0..N-1
+};
+int launch_edge_index(int64_t n_edges, int n, const int64_t* src, const int64_t* dst, const EdgeIndex& ei,
+                      cudaStream_t s);
+int launch_cn_edges_seg(int64_t n_edges, int n, const double* pos, const int32_t* species, const int64_t* src,
+                        const int64_t* dst, const double* shift, const Tables* tab, const EdgeIndex& ei, double* cn,
+                        cudaStream_t s);
+int launch_cn_adjoint_edges_seg(int64_t n_edges, int n, const double* pos, const int32_t* species,
+                                const int64_t* src, const int64_t* dst, const double* shift, const Tables* tab,
+                                const double* gcn, const EdgeIndex& ei, double* gpos, double* gshift,
+                                cudaStream_t s);
 int launch_c6_atoms(int n, const int32_t* species, const Tables* tab, const double* eigvecs, int R,
                     const double* cn, double* c6, double* dc6, double* self_part, int* n_self_blocks,
                     cudaStream_t s);
-int launch_cn_adjoint_edges(int64_t n_edges, const double* pos, const int32_t* species, const int64_t* src,
-                            const int64_t* dst, const double* shift, const Tables* tab, const double* gcn,
-                            double* gpos, double* gshift, cudaStream_t s);
 
 // neighbour export
 int launch_nbr_count(const CellGrid& g, int n, const CellList& cl, const double* pos_ang, int* counts,
@@ -115,6 +128,8 @@ struct MeshGeom {
   int spread_cap; // staged atoms per column chunk at most (0: as many as shared memory holds)
   int fft_x;      // fused x-pass (2D cuFFT + x FFT/filter kernel): 1 on, 0 off, -1 default
   int xpencil;    // kz values per pencil of the fused x-pass (1, 2, 4), -1 default
+  int xq;         // TMA x-pass: q values per unit (8, 16, 32), -1 default
+  int xranks;     // TMA x-pass: ranks per unit (1, 2), -1 default
   const float* win_axes;  // SPME, mixed form: sinc(m/n)^(2p) per axis, [nx | ny | nz/2+1] (null: none)
 };
 int launch_cellinfo(const double* cell, double scale, CellInfo* ci, cudaStream_t s);
@@ -143,6 +158,11 @@ int launch_xfilter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, 
                    int* n_blocks, cudaStream_t s);
 // kz width of the fused x-pass pencils for this mesh (0: the fused path does not apply)
 int xfilter_pencil(const MeshGeom& mg, int is_double);
+// TMA fused x-pass (float spectrum): units of Q flattened (y, kz) values x all x x RG ranks x S
+bool xpass_applies(const MeshGeom& mg, int Q, int RG);
+int launch_xpass(const MeshGeom& mg, int Q, int RG, const CellInfo* ci, const GreenPairF* gpf, const float4* gtab,
+                 const Tables* tab, const float* deconv, int spme, void* spec, double* part, int* n_blocks,
+                 cudaStream_t s);
 // mixed form: per-call table of G and its k-derivatives per species pair (gtab of the filter)
 int launch_green_table(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab, void* table,
                        cudaStream_t s);

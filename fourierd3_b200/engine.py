@@ -145,6 +145,16 @@ class Engine:
             self._work = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
         return self._work
 
+    def edge_workspace(self, n_atoms: int, n_edges: int) -> torch.Tensor:
+        """Workspace of the edge-list entry point (grown, never shrunk, so a fixed edge count
+        keeps every pointer fixed, e.g. across CUDA-graph replays)."""
+        nbytes = ctypes.c_size_t()
+        _native.check(_native.lib().fd3_edge_workspace_size(self._plan, n_atoms, n_edges, ctypes.byref(nbytes)),
+                      "fd3_edge_workspace_size")
+        if self._work is None or self._work.numel() < nbytes.value:
+            self._work = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
+        return self._work
+
     def workspace_bytes(self, n_atoms: int, cell_ang: np.ndarray, r_cut_ang: float) -> int:
         """Bytes of device workspace one fused call on this structure shape needs."""
         nb, _ = self.cell_grid(cell_ang, r_cut_ang)
@@ -163,18 +173,21 @@ class Engine:
 
     _KNOBS = {"filter_kt": _native.TUNE_FILTER_KT, "spread_zc": _native.TUNE_SPREAD_ZC,
               "spread_cap": _native.TUNE_SPREAD_CAP, "fft_x": _native.TUNE_FFT_X,
-              "xpencil": _native.TUNE_XPENCIL}
+              "xpencil": _native.TUNE_XPENCIL, "xq": _native.TUNE_XQ, "xranks": _native.TUNE_XRANKS}
 
     def set_tuning(self, filter_kt: Optional[int] = None, spread_zc: Optional[int] = None,
                    spread_cap: Optional[int] = None, fft_x: Optional[int] = None,
-                   xpencil: Optional[int] = None) -> None:
+                   xpencil: Optional[int] = None, xq: Optional[int] = None,
+                   xranks: Optional[int] = None) -> None:
         """Launch-shape knobs (results agree to rounding): ``filter_kt`` = k-points per filter
         tile, ``spread_zc`` = z-tiles per column chunk of the spread, ``spread_cap`` = staged
-        atoms per chunk at most, ``fft_x`` = fused x-pass (2D cuFFT + x FFT/filter kernel) on
-        or off, ``xpencil`` = kz values per pencil of the fused x-pass (1, 2, 4); -1 (0 for the
-        cap) restores a default."""
+        atoms per chunk at most, ``fft_x`` = 0 (3D cuFFT around the filter), 1 (2D cuFFT and the
+        x FFT / filter / inverse x FFT in one kernel, pencils of ``xpencil`` = 1, 2 or 4 kz values
+        of every channel) or 2 (the same with TMA-moved units of ``xq`` = 8, 16 or 32 flattened
+        (y, kz) values of ``xranks`` = 1 or 2 ranks, mixed precision); -1 (0 for the cap)
+        restores a default."""
         for name, val in (("filter_kt", filter_kt), ("spread_zc", spread_zc), ("spread_cap", spread_cap),
-                          ("fft_x", fft_x), ("xpencil", xpencil)):
+                          ("fft_x", fft_x), ("xpencil", xpencil), ("xq", xq), ("xranks", xranks)):
             if val is not None:
                 _native.check(_native.lib().fd3_plan_set_tuning(self._plan, self._KNOBS[name], int(val)),
                               "fd3_plan_set_tuning")
@@ -239,7 +252,7 @@ class Engine:
         gpos = torch.empty_like(pos) if need_grad else None
         gsh = torch.empty_like(sh) if need_grad else None
         gcell = torch.empty((3, 3), dtype=torch.float64, device=self.device) if need_grad else None
-        work = self.workspace(n, 0)
+        work = self.edge_workspace(n, e)
 
         def ptr(t):
             return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else None

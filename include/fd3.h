@@ -105,6 +105,8 @@ FD3_API int fd3_plan_destroy(fd3_plan* plan);
 #define FD3_TUNE_SPREAD_CAP 2
 #define FD3_TUNE_FFT_X 3
 #define FD3_TUNE_XPENCIL 4
+#define FD3_TUNE_XQ 5
+#define FD3_TUNE_XRANKS 6
 FD3_API int fd3_plan_set_tuning(fd3_plan* plan, int32_t knob, int32_t value);
 FD3_API int fd3_plan_get_tuning(const fd3_plan* plan, int32_t knob, int32_t* value);
 
@@ -129,7 +131,12 @@ FD3_API int fd3_cell_grid(const double* h_cell_ang, double r_cut_ang, int32_t* n
  *   d_gpos     [N*3]  dE/dpos      (Hartree/Bohr)
  *   d_gshift   [E*3]  dE/dshift    (Hartree/Bohr)
  *   d_gcell    [9]    dE/dcell     (Hartree/Bohr), positions and shifts held fixed
+ * The workspace is sized by fd3_edge_workspace_size (it holds the edges sorted by source and
+ * by destination). Edges may come in any order; every per-atom sum is taken in edge order, so
+ * repeated calls give bitwise-equal results. No host synchronisation: an edge index outside
+ * 0..N-1 is not dereferenced, and it makes the energy and gradients NaN.
  */
+FD3_API int fd3_edge_workspace_size(const fd3_plan* plan, int64_t n_atoms, int64_t n_edges, size_t* bytes);
 FD3_API int fd3_energy_edges(fd3_plan* plan, int64_t n_atoms, const double* d_pos, const int32_t* d_species,
                      const double* d_cell, int64_t n_edges, const int64_t* d_src, const int64_t* d_dst,
                      const double* d_shift, int32_t need_grad, void* d_work, size_t work_bytes,

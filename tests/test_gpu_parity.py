@@ -115,6 +115,51 @@ def test_fused_is_deterministic(cuda_device):
         np.testing.assert_array_equal(x, y)
 
 
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_module_edges_is_deterministic(dtype, cuda_device):
+    """The module (edge-list) path sums every per-atom CN and gradient in edge order: repeated
+    calls are bitwise equal, and a shuffled edge list gives the same result to rounding."""
+    from fourierd3_b200 import FourierD3
+
+    rec = gc.load("hcno_240_spme_p6")
+    kw = gc.model_kwargs(rec["config"])
+    m = FourierD3(rec["numbers"], rec["cell"], dtype=dtype, device=cuda_device, verbose=False, **kw)
+    ei, S = _oracle_edges("hcno_240_spme_p6")
+    runs = [_strain_protocol(m, rec["positions"], rec["cell"], ei, S, cuda_device) for _ in range(3)]
+    for e, f, s in runs[1:]:
+        assert e == runs[0][0]
+        np.testing.assert_array_equal(f, runs[0][1])
+        np.testing.assert_array_equal(s, runs[0][2])
+    perm = np.random.default_rng(0).permutation(ei.shape[1])
+    e, f, s = _strain_protocol(m, rec["positions"], rec["cell"], ei[:, perm], S[perm], cuda_device)
+    tol = 1e-12 if dtype == torch.float64 else 1e-6
+    assert abs(e - runs[0][0]) <= tol * abs(runs[0][0])
+    np.testing.assert_allclose(f, runs[0][1], rtol=0, atol=1e-10 if dtype == torch.float64 else 1e-5)
+
+
+def test_module_edges_out_of_range_index_gives_nan(cuda_device):
+    """An edge index outside 0..n_atoms-1 is caught on the device (no host synchronisation):
+    it is never dereferenced and the energy comes back NaN; the next valid call is unaffected."""
+    from fourierd3_b200 import FourierD3
+
+    rec = gc.load("sio2_648_spme_p5")
+    kw = gc.model_kwargs(rec["config"])
+    m = FourierD3(rec["numbers"], rec["cell"], dtype=torch.float64, device=cuda_device, verbose=False, **kw)
+    ei, S = _oracle_edges("sio2_648_spme_p5")
+    cell_t = torch.tensor(rec["cell"], dtype=torch.float64, device=cuda_device)
+    pos = torch.tensor(rec["positions"], dtype=torch.float64, device=cuda_device)
+    bad = ei.copy()
+    bad[1, 5] = len(rec["numbers"])          # one past the last atom
+    bad[0, 7] = -3
+    m._update_cell(cell_t)
+    e_bad = m(pos, torch.as_tensor(bad, device=cuda_device), torch.as_tensor(S, dtype=torch.float64,
+                                                                             device=cuda_device) @ cell_t)
+    assert torch.isnan(e_bad).item()
+    e_ok = m(pos, torch.as_tensor(ei, device=cuda_device), torch.as_tensor(S, dtype=torch.float64,
+                                                                           device=cuda_device) @ cell_t)
+    assert abs(float(e_ok) * 27.21138505 - float(rec["energy_ev"])) <= E_REL * abs(float(rec["energy_ev"]))
+
+
 def test_fused_dense_box_uses_fallback_paths(cuda_device):
     """A dense light-element box overflows the shared-memory bin stage (and records), so the
     CN and its adjoint take the global-memory traversals; results must still match the oracle."""

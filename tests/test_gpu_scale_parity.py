@@ -77,8 +77,18 @@ def test_sio2_256_mesh_matches_oracle(precision, cuda_device):
         _check(m(pos, cell), ref, precision, f"fused x-pass, xpencil={kz}")
     assert len(widths) >= 2
     if precision == "mixed":
+        # the TMA-moved x-pass at every unit shape that fits (nx = 256: 16 x 16 register DFTs)
+        shapes = 0
+        for xq in (8, 16, 32):
+            for xr in (1, 2):
+                m.engine.set_tuning(fft_x=2, xq=xq, xranks=xr)
+                if m.engine.tuning()["fft_x"] != 2:
+                    continue
+                shapes += 1
+                _check(m(pos, cell), ref, precision, f"tma x-pass xq={xq} xranks={xr}")
+        assert shapes >= 3
         # the launch knobs the benchmark settles on for this mesh
-        m.engine.set_tuning(fft_x=1, xpencil=4, spread_zc=4)
+        m.engine.set_tuning(fft_x=2, xq=16, xranks=1, spread_zc=4)
         _check(m(pos, cell), ref, precision, "benchmark knobs")
     torch.cuda.synchronize()
     del m

@@ -125,6 +125,55 @@ def test_fused_x_pass_agrees_with_3d_fft(precision, cuda_device):
         m.engine.set_tuning(xpencil=3)
 
 
+def test_tma_x_pass_agrees_with_3d_fft(cuda_device):
+    """The TMA-moved fused x-pass (mixed precision) against 3D cuFFT around the separate filter,
+    for SPME and PME, one to four species, nx = 64 and 128, units of 8, 16 and 32 flattened
+    (y, kz) values and of one or two ranks (an odd rank count leaves a padded last group)."""
+    import golden_cases as gc
+    from fourierd3_b200 import D3Model
+
+    ran = 0
+    for name in ("sio2_648_spme_p5", "sio2_648_pme_p5", "hcno_240_spme_p6", "hcno_240_spme_p4_tol1e-4",
+                 "tiny_6_spme_p4"):
+        rec = gc.load(name)
+        m = D3Model(rec["numbers"], rec["cell"], precision="mixed", device=cuda_device,
+                    **gc.model_kwargs(rec["config"]))
+        m.engine.set_tuning(fft_x=0)
+        e0, f0, s0 = (t.clone() for t in m(rec["positions"], rec["cell"]))
+        for xq in (8, 16, 32):
+            for xr in (1, 2):
+                m.engine.set_tuning(fft_x=2, xq=xq, xranks=xr)
+                t = m.engine.tuning()
+                if t["fft_x"] != 2:
+                    continue   # nx outside 64/128/256, more than 4 species, or the unit does not fit twice
+                assert (t["xq"], t["xranks"]) == (xq, xr)
+                ran += 1
+                e, f, s = m(rec["positions"], rec["cell"])
+                assert abs(float(e) - float(e0)) <= 2e-6 * abs(float(e0)), (name, xq, xr, float(e), float(e0))
+                assert (f - f0).abs().max().item() <= 1e-5, (name, xq, xr)
+                assert (s - s0).abs().max().item() <= 1e-5, (name, xq, xr)
+        m.engine.set_tuning(fft_x=2, xq=-1, xranks=-1)
+    assert ran >= 12
+    with pytest.raises(ValueError):
+        m.engine.set_tuning(xq=12)
+    with pytest.raises(ValueError):
+        m.engine.set_tuning(xranks=3)
+
+
+def test_tma_x_pass_float64_plan_keeps_its_path(cuda_device):
+    """fft_x = 2 is a mixed-precision path; a float64 plan reports the path it actually runs."""
+    import golden_cases as gc
+    from fourierd3_b200 import D3Model
+
+    rec = gc.load("sio2_648_spme_p5")
+    m = D3Model(rec["numbers"], rec["cell"], precision="fp64", device=cuda_device, **gc.model_kwargs(rec["config"]))
+    m.engine.set_tuning(fft_x=2)
+    t = m.engine.tuning()
+    assert t["fft_x"] == 0 and t["xq"] == 0
+    e, f, s = m(rec["positions"], rec["cell"])
+    assert abs(float(e) - float(rec["energy_ev"])) <= 1e-10 * abs(float(rec["energy_ev"]))
+
+
 def test_autotune_fft_x_picks_a_timed_path(cuda_device):
     """batch.autotune_fft_x times the 3D path and the fused x-pass at each pencil width on the
     plan's heaviest structure, leaves the fastest set on the plan, and the batch results agree

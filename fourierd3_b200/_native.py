@@ -45,7 +45,8 @@ _SIGS = {
     "fd3_plan_create": (ctypes.c_int, [ctypes.POINTER(PlanDesc), ctypes.POINTER(_vp)]),
     "fd3_plan_destroy": (ctypes.c_int, [_vp]),
     "fd3_plan_set_tuning": (ctypes.c_int, [_vp, _c_int32, _c_int32]),
-    "fd3_plan_get_tuning": (ctypes.c_int, [_vp, _c_int32, ctypes.POINTER(_c_int32)]),
+    "fd3_plan_set_edge_cutoff": (ctypes.c_int, [_vp, _c_int32]),
+    "fd3_plan_get_tuning":(ctypes.c_int, [_vp, _c_int32, ctypes.POINTER(_c_int32)]),
     "fd3_workspace_size": (ctypes.c_int, [_vp, _c_int64, _c_int64, ctypes.POINTER(ctypes.c_size_t)]),
     "fd3_edge_workspace_size": (ctypes.c_int, [_vp, _c_int64, _c_int64, ctypes.POINTER(ctypes.c_size_t)]),
     "fd3_cell_grid":(ctypes.c_int, [_dp, _c_double, ctypes.POINTER(_c_int32), ctypes.POINTER(_c_int32)]),

@@ -12,6 +12,7 @@ using namespace fd3;
 
 struct fd3_plan {
   int S = 0, R = 0, method = 0, P = 0, precision = 0;
+  int edge_cutoff = 0;   // 1: edge-list edges at or beyond the CN cutoff contribute nothing
   MeshGeom mg{};
   int ens[3] = {0, 0, 0};
   Tables h_tab{};
@@ -426,6 +427,12 @@ extern "C" int fd3_plan_get_tuning(const fd3_plan* p, int32_t knob, int32_t* val
   return FD3_EINVAL;
 }
 
+extern "C" int fd3_plan_set_edge_cutoff(fd3_plan* p, int32_t on) {
+  if (!p || (on != 0 && on != 1)) return FD3_EINVAL;
+  p->edge_cutoff = on;
+  return FD3_OK;
+}
+
 extern "C" int fd3_plan_destroy(fd3_plan* p) {
   if (!p) return FD3_OK;
   for (int k = 0; k < fd3_plan::kMaxMarks; ++k)
@@ -720,15 +727,17 @@ extern "C" int fd3_energy_edges(fd3_plan* p, int64_t n_atoms, const double* d_po
   prof_begin(p, s);
   FD3_TRY(launch_cellinfo(d_cell, 1.0, w.ci, s));
   // edges sorted by source and destination; the CN is summed per atom in edge order
+  const double mask_r2 = p->edge_cutoff ? p->h_tab.r_cut * p->h_tab.r_cut : INFINITY;
   FD3_TRY(launch_edge_index(n_edges, N, d_src, d_dst, w.ei, s));
-  FD3_TRY(launch_cn_edges_seg(n_edges, N, d_pos, d_species, d_src, d_dst, d_shift, p->d_tab, w.ei, w.cn, s));
+  FD3_TRY(launch_cn_edges_seg(n_edges, N, d_pos, d_species, d_src, d_dst, d_shift, p->d_tab, mask_r2, w.ei, w.cn,
+                              s));
   int n_self = 0, n_kspc = 0, n_mcell = 0;
   FD3_TRY(launch_c6_atoms(N, d_species, p->d_tab, p->d_eigvecs, p->R, w.cn, w.c6, w.dc6, w.self_part, &n_self, s));
   prof_mark(p, s, "cn_c6");
   FD3_TRY(run_mesh(p, N, d_pos, 1.0, d_species, w, need_grad != 0, d_gpos, w.mcell_part, &n_kspc, &n_mcell, s));
   if (need_grad)
-    FD3_TRY(launch_cn_adjoint_edges_seg(n_edges, N, d_pos, d_species, d_src, d_dst, d_shift, p->d_tab, w.gcn, w.ei,
-                                        d_gpos, d_gshift, s));
+    FD3_TRY(launch_cn_adjoint_edges_seg(n_edges, N, d_pos, d_species, d_src, d_dst, d_shift, p->d_tab, mask_r2,
+                                        w.gcn, w.ei, d_gpos, d_gshift, s));
   prof_mark(p, s, "cn_adjoint");
   Partials pa{w.self_part, n_self, w.kspc_part, n_kspc, w.cnv_part, 0, w.mcell_part, n_mcell};
   FD3_TRY(launch_finalize(pa, w.ci, 0, 1.0, d_energy, need_grad ? d_gcell : nullptr, s));

@@ -748,13 +748,15 @@ int launch_edge_index(int64_t n_edges, int n, const int64_t* src, const int64_t*
 // CN of atom a: the sum of the smooth-cutoff function over its source edges in edge order
 // (core.py:323-386, index_add_ on edge_index[0]); one warp per atom, lanes over the edges, a
 // fixed butterfly reduction -- the same result on every run. NaN for every atom when an edge
-// index was out of range (the range check the reference leaves to torch indexing).
+// index was out of range (the range check the reference leaves to torch indexing). Edges with
+// |r|^2 >= mask_r2 contribute nothing (mask_r2 = +inf: every edge counts, as in the reference).
 __global__ void __launch_bounds__(256) k_cn_edges_seg(int n, int64_t ne, const int* __restrict__ st,
                                                      const int* __restrict__ ord, const double* __restrict__ x,
                                                      const int32_t* __restrict__ species,
                                                      const int64_t* __restrict__ src, const int64_t* __restrict__ dst,
                                                      const double* __restrict__ sh, const Tables* __restrict__ tab,
-                                                     const int* __restrict__ bad, double* __restrict__ cn) {
+                                                     double mask_r2, const int* __restrict__ bad,
+                                                     double* __restrict__ cn) {
   const int lane = threadIdx.x & 31;
   const int a = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (a >= n) return;
@@ -767,8 +769,10 @@ __global__ void __launch_bounds__(256) k_cn_edges_seg(int n, int64_t ne, const i
     const double v0 = x[3 * j] - x[3 * i] + sh[3 * (int64_t)e];
     const double v1 = x[3 * j + 1] - x[3 * i + 1] + sh[3 * (int64_t)e + 1];
     const double v2 = x[3 * j + 2] - x[3 * i + 2] + sh[3 * (int64_t)e + 2];
+    const double r2 = v0 * v0 + v1 * v1 + v2 * v2;
+    if (r2 >= mask_r2) continue;
     double f, df;
-    cn_edge(sqrt(v0 * v0 + v1 * v1 + v2 * v2), rca + tab->rcov[species[j]], tab->r_cut, f, df);
+    cn_edge(sqrt(r2), rca + tab->rcov[species[j]], tab->r_cut, f, df);
     sum += f;
   }
   sum = warp_sum(sum);
@@ -776,11 +780,11 @@ __global__ void __launch_bounds__(256) k_cn_edges_seg(int n, int64_t ne, const i
 }
 
 int launch_cn_edges_seg(int64_t n_edges, int n, const double* pos, const int32_t* species, const int64_t* src,
-                        const int64_t* dst, const double* shift, const Tables* tab, const EdgeIndex& ei, double* cn,
-                        cudaStream_t s) {
+                        const int64_t* dst, const double* shift, const Tables* tab, double mask_r2,
+                        const EdgeIndex& ei, double* cn, cudaStream_t s) {
   const int wpb = 8;
   k_cn_edges_seg<<<(n + wpb - 1) / wpb, 32 * wpb, 0, s>>>(n, n_edges, ei.st_s, ei.ord_s, pos, species, src, dst,
-                                                          shift, tab, ei.bad, cn);
+                                                          shift, tab, mask_r2, ei.bad, cn);
   FD3_LAUNCHED();
   return FD3_OK;
 }
@@ -789,8 +793,8 @@ int launch_cn_edges_seg(int64_t n_edges, int n, const double* pos, const int32_t
 __global__ void __launch_bounds__(256) k_edge_grad(int64_t ne, int n, const double* __restrict__ x,
                                                   const int32_t* __restrict__ species, const int64_t* __restrict__ src,
                                                   const int64_t* __restrict__ dst, const double* __restrict__ sh,
-                                                  const Tables* __restrict__ tab, const double* __restrict__ gcn,
-                                                  double* __restrict__ gshift) {
+                                                  const Tables* __restrict__ tab, double mask_r2,
+                                                  const double* __restrict__ gcn, double* __restrict__ gshift) {
   const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= ne) return;
   const int64_t i = src[e], j = dst[e];
@@ -799,10 +803,11 @@ __global__ void __launch_bounds__(256) k_edge_grad(int64_t ne, int n, const doub
     const double v0 = x[3 * j] - x[3 * i] + sh[3 * e];
     const double v1 = x[3 * j + 1] - x[3 * i + 1] + sh[3 * e + 1];
     const double v2 = x[3 * j + 2] - x[3 * i + 2] + sh[3 * e + 2];
-    const double r = sqrt(v0 * v0 + v1 * v1 + v2 * v2);
+    const double r2 = v0 * v0 + v1 * v1 + v2 * v2;
+    const double r = sqrt(r2);
     double f, df;
     cn_edge(r, tab->rcov[species[i]] + tab->rcov[species[j]], tab->r_cut, f, df);
-    if (r > 1e-6) {
+    if (r > 1e-6 && r2 < mask_r2) {
       const double a = gcn[i] * df / r;
       g0 = a * v0;
       g1 = a * v1;
@@ -843,12 +848,12 @@ __global__ void __launch_bounds__(256) k_edge_grad_atoms(int n, const int* __res
 
 int launch_cn_adjoint_edges_seg(int64_t n_edges, int n, const double* pos, const int32_t* species,
                                 const int64_t* src, const int64_t* dst, const double* shift, const Tables* tab,
-                                const double* gcn, const EdgeIndex& ei, double* gpos, double* gshift,
-                                cudaStream_t s) {
+                                double mask_r2, const double* gcn, const EdgeIndex& ei, double* gpos,
+                                double* gshift, cudaStream_t s) {
   if (n_edges > 0) {
     const int tb = 256;
     k_edge_grad<<<(unsigned)((n_edges + tb - 1) / tb), tb, 0, s>>>(n_edges, n, pos, species, src, dst, shift, tab,
-                                                                   gcn, gshift);
+                                                                   mask_r2, gcn, gshift);
     FD3_LAUNCHED();
   }
   const int wpb = 8;

@@ -96,13 +96,14 @@ struct EdgeIndex {
 };
 int launch_edge_index(int64_t n_edges, int n, const int64_t* src, const int64_t* dst, const EdgeIndex& ei,
                       cudaStream_t s);
+// edges with |r|^2 >= mask_r2 (Bohr^2) contribute nothing; +inf: every edge counts
 int launch_cn_edges_seg(int64_t n_edges, int n, const double* pos, const int32_t* species, const int64_t* src,
-                        const int64_t* dst, const double* shift, const Tables* tab, const EdgeIndex& ei, double* cn,
-                        cudaStream_t s);
+                        const int64_t* dst, const double* shift, const Tables* tab, double mask_r2,
+                        const EdgeIndex& ei, double* cn, cudaStream_t s);
 int launch_cn_adjoint_edges_seg(int64_t n_edges, int n, const double* pos, const int32_t* species,
                                 const int64_t* src, const int64_t* dst, const double* shift, const Tables* tab,
-                                const double* gcn, const EdgeIndex& ei, double* gpos, double* gshift,
-                                cudaStream_t s);
+                                double mask_r2, const double* gcn, const EdgeIndex& ei, double* gpos,
+                                double* gshift, cudaStream_t s);
 int launch_c6_atoms(int n, const int32_t* species, const Tables* tab, const double* eigvecs, int R,
                     const double* cn, double* c6, double* dc6, double* self_part, int* n_self_blocks,
                     cudaStream_t s);

@@ -200,7 +200,12 @@ class Engine:
             out[name] = int(v.value)
         return out
 
-    def atom_terms(self, n_atoms: int, cell_ang: Optional[np.ndarray] = None, r_cut_ang: float = 0.0,
+    def set_edge_cutoff(self, on: bool) -> None:
+        """Edge-list path: edges at or beyond the CN cutoff contribute nothing (a Verlet list
+        with a skin can then be passed unchanged between rebuilds)."""
+        _native.check(_native.lib().fd3_plan_set_edge_cutoff(self._plan, 1 if on else 0), "fd3_plan_set_edge_cutoff")
+
+    def atom_terms(self, n_atoms: int,cell_ang: Optional[np.ndarray] = None, r_cut_ang: float = 0.0,
                    work: Optional[torch.Tensor] = None):
         """Per-atom CN (after cncorr) and rank-r C6 factors (n_atoms, r) of the last call that used
         this engine's workspace (or ``work``): the fused call when ``cell_ang`` is given, the

@@ -49,16 +49,32 @@ class MDState:
 
 
 class VelocityVerlet:
+    """``verlet_edges``: pass the Verlet list (r_cut + skin) unchanged between rebuilds and let
+    the kernels drop the pairs beyond r_cut (fd3_plan_set_edge_cutoff) instead of cutting the
+    list before every call; the edge count then stays fixed between rebuilds. ``graph``
+    (needs ``verlet_edges``): each step -- half kick, drift, forces and stress through the
+    module's autograd.Function, half kick -- is one CUDA-graph replay, re-captured after each
+    list rebuild; the only host synchronisation per step is the rebuild test. In graph mode the
+    state's energy and stress stay device tensors."""
+
     def __init__(self, numbers, positions, cell, *, dt: float = 1.0, temperature: float = 300.0, seed: int = 0,
-                 skin: float = 0.5, r_cut: float = 6.0, dtype=torch.float32, device=None, **model_kw):
+                 skin: float = 0.5, r_cut: float = 6.0, dtype=torch.float32, device=None,
+                 verlet_edges: bool = False, graph: bool = False, **model_kw):
+        if graph and not verlet_edges:
+            raise ValueError("graph=True needs verlet_edges=True (a fixed edge count between rebuilds)")
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         self.numbers = np.asarray(numbers)
         self.cell = np.asarray(cell, dtype=np.float64)
         self.dt = float(dt)
         self.skin = float(skin)
         self.r_cut = float(r_cut)
+        self.verlet_edges = bool(verlet_edges)
+        self.use_graph = bool(graph)
+        self._graph = None
         self.model = FourierD3(self.numbers, self.cell, dtype=dtype, device=self.device, verbose=False,
                                r_cut=r_cut, **model_kw)
+        if self.verlet_edges:
+            self.model._eng.set_edge_cutoff(True)
         self.masses = torch.tensor(masses_of(self.numbers), dtype=torch.float64, device=self.device)
         self.cell_t = torch.tensor(self.cell, dtype=torch.float64, device=self.device)
         pos = torch.tensor(np.asarray(positions, dtype=np.float64), device=self.device)
@@ -69,12 +85,20 @@ class VelocityVerlet:
         self.state = MDState(0, pos, vel, f, e, s)
 
     # -- neighbours --------------------------------------------------------------------------
+    def _needs_rebuild(self, pos: torch.Tensor) -> bool:
+        return self._ref_pos is None or (pos - self._ref_pos).norm(dim=1).max().item() > 0.5 * self.skin
+
+    def _rebuild(self, pos: torch.Tensor) -> None:
+        i, j, S = neighbour_list(pos, self.cell, self.r_cut + self.skin)
+        self._vi, self._vj, self._vS = i, j, S.to(torch.float64)
+        self._ref_pos = pos.clone()
+        self.rebuilds += 1
+
     def _edges(self, pos: torch.Tensor):
-        if self._ref_pos is None or (pos - self._ref_pos).norm(dim=1).max().item() > 0.5 * self.skin:
-            i, j, S = neighbour_list(pos, self.cell, self.r_cut + self.skin)
-            self._vi, self._vj, self._vS = i, j, S.to(torch.float64)
-            self._ref_pos = pos.clone()
-            self.rebuilds += 1
+        if self._needs_rebuild(pos):
+            self._rebuild(pos)
+        if self.verlet_edges:
+            return torch.stack((self._vi, self._vj)), self._vS
         d = pos[self._vj] - pos[self._vi] + self._vS @ self.cell_t
         keep = (d * d).sum(1) < self.r_cut * self.r_cut
         return torch.stack((self._vi[keep], self._vj[keep])), self._vS[keep]
@@ -83,6 +107,12 @@ class VelocityVerlet:
     def forces(self, pos: torch.Tensor, model: Optional[FourierD3] = None):
         model = model or self.model
         edge_index, ushift = self._edges(pos)
+        e, f, s = self._forces_device(pos, edge_index, ushift, model)
+        return float(e), f, s.cpu().numpy()
+
+    def _forces_device(self, pos, edge_index, ushift, model):
+        """Energy [eV] (0-d), forces [eV/A] and stress [eV/A^3] on the device, by the strain protocol
+        of src/fourierd3/calculator.py:146-188 (no host synchronisation)."""
         strain = torch.zeros(3, 3, dtype=torch.float64, device=self.device, requires_grad=True)
         scell = self.cell_t + torch.einsum("ab,Ab->Aa", strain, self.cell_t)
         model._update_cell(scell)
@@ -90,14 +120,16 @@ class VelocityVerlet:
         sp = p + torch.einsum("ab,ib->ia", strain, p)
         energy = model(sp, edge_index, ushift @ scell).to(torch.float64) * HARTREE_TO_EV
         energy.backward()
-        stress = (strain.grad / model.volume.detach() * ANGSTROM_TO_BOHR ** 3).cpu().numpy()
-        return float(energy.detach()), -p.grad.detach(), stress
+        stress = strain.grad / model.volume.detach() * ANGSTROM_TO_BOHR ** 3
+        return energy.detach(), -p.grad.detach(), stress.detach()
 
     def kinetic(self) -> float:
         v = self.state.velocities
         return float(0.5 * (self.masses[:, None] * v * v).sum() / ACC)
 
     def step(self) -> MDState:
+        if self.use_graph:
+            return self._graph_step()
         st = self.state
         a = st.forces * ACC / self.masses[:, None]
         v_half = st.velocities + 0.5 * self.dt * a
@@ -105,4 +137,50 @@ class VelocityVerlet:
         e, f, s = self.forces(pos)
         v = v_half + 0.5 * self.dt * f * ACC / self.masses[:, None]
         self.state = MDState(st.step + 1, pos, v, f, e, s)
+        return self.state
+
+    # -- CUDA-graph steps ---------------------------------------------------------------------
+    def _step_body(self) -> None:
+        """One velocity-Verlet step on the static buffers (recorded into the graph)."""
+        g = self._static
+        v_half = g["vel"] + 0.5 * self.dt * g["f"] * ACC / self.masses[:, None]
+        pos = g["pos"] + self.dt * v_half
+        e, f, s = self._forces_device(pos, g["ei"], g["us"], self.model)
+        g["vel"].copy_(v_half + 0.5 * self.dt * f * ACC / self.masses[:, None])
+        g["pos"].copy_(pos)
+        g["f"].copy_(f)
+        g["e"].copy_(e)
+        g["s"].copy_(s)
+
+    def _capture(self) -> None:
+        st = self.state
+        self._static = {"pos": st.positions.clone(), "vel": st.velocities.clone(), "f": st.forces.clone(),
+                        "e": torch.zeros((), dtype=torch.float64, device=self.device),
+                        "s": torch.zeros((3, 3), dtype=torch.float64, device=self.device),
+                        "ei": torch.stack((self._vi, self._vj)).contiguous(), "us": self._vS.contiguous()}
+        # one eager step on a side stream warms the allocator and sizes the workspace for this
+        # edge count; the state is restored before the capture
+        keep = {k: self._static[k].clone() for k in ("pos", "vel", "f")}
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(side):
+            self._step_body()
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        for k, v in keep.items():
+            self._static[k].copy_(v)
+        self._graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(self._graph):
+            self._step_body()
+
+    def _graph_step(self) -> MDState:
+        st = self.state
+        rebuild = self._needs_rebuild(st.positions)
+        if rebuild:
+            self._rebuild(st.positions)
+        if rebuild or self._graph is None:
+            self._capture()
+        self._graph.replay()
+        g = self._static
+        self.state = MDState(st.step + 1, g["pos"].clone(), g["vel"].clone(), g["f"].clone(), g["e"].clone(),
+                             g["s"].clone())
         return self.state

@@ -137,6 +137,13 @@ FD3_API int fd3_cell_grid(const double* h_cell_ang, double r_cut_ang, int32_t* n
  * 0..N-1 is not dereferenced, and it makes the energy and gradients NaN.
  */
 FD3_API int fd3_edge_workspace_size(const fd3_plan* plan, int64_t n_atoms, int64_t n_edges, size_t* bytes);
+
+/* Edge-list option (no reference counterpart; off by default, as in the reference, where every
+ * edge passed to forward counts): on = 1 makes edges with |r| >= the CN cutoff contribute
+ * nothing to the CN and its gradients, so an MD driver can pass its Verlet list (cutoff + skin)
+ * unchanged between rebuilds -- a fixed edge count, which a captured CUDA graph needs --
+ * instead of cutting it back to the cutoff before every call. */
+FD3_API int fd3_plan_set_edge_cutoff(fd3_plan* plan, int32_t on);
 FD3_API int fd3_energy_edges(fd3_plan* plan, int64_t n_atoms, const double* d_pos, const int32_t* d_species,
                      const double* d_cell, int64_t n_edges, const int64_t* d_src, const int64_t* d_dst,
                      const double* d_shift, int32_t need_grad, void* d_work, size_t work_bytes,

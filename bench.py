@@ -626,7 +626,9 @@ def main():
             tuned[prec]["spread_ms"] = {str(k): round(v, 4) for k, v in sp[0][1].items()}
             tuned[prec]["fft_filter_ms"] = {str(k): round(v, 4) for k, v in fx[0][1].items()}
         models[prec].engine.set_tuning(spread_zc=tuned[prec]["spread_zc"], fft_x=tuned[prec]["fft_x"],
-                                       xpencil=tuned[prec]["xpencil"] if tuned[prec]["fft_x"] == 1 else -1)
+                                       xpencil=tuned[prec]["xpencil"] if tuned[prec]["fft_x"] == 1 else -1,
+                                       xq=tuned[prec]["xq"] if tuned[prec]["fft_x"] == 2 else -1,
+                                       xranks=tuned[prec]["xranks"] if tuned[prec]["fft_x"] == 2 else -1)
         b.capture()
         graphs[prec] = b
 

@@ -37,7 +37,12 @@ class PlanDesc(ctypes.Structure):
         ("has_cncorr", _c_int32), ("r_cut", _c_double), ("params", _c_double * 4),
         ("rcov", _dp), ("cnref", _dp), ("eigvecs", _dp), ("eigs", _dp), ("sqrtq", _dp),
         ("cncorr", _dp), ("deconv", ctypes.POINTER(ctypes.c_float)),
+        ("cnfunc", _c_int32), ("rcov_cn", _dp), ("en", _dp),
     ]
+
+
+CN_SMOOTH, CN_D4 = 0, 1
+CNFUNCS = {"smooth_cut": CN_SMOOTH, "d4": CN_D4}
 
 
 # symbol -> (restype, argtypes); mirrors include/fd3.h

@@ -356,12 +356,14 @@ def autotune_spread(batch: "D3Batch", candidates: Sequence[int] = (0, 2, 4, 8, 1
     return out
 
 
-def autotune_fft_x(batch: "D3Batch", pencils: Sequence[int] = (1, 2, 4), reps: int = 2) -> dict:
+def autotune_fft_x(batch: "D3Batch", pencils: Sequence[int] = (1, 2, 4), reps: int = 2,
+                   tma_units: Sequence[tuple] = ((16, 1), (8, 2), (8, 4), (4, 4))) -> dict:
     """Choose per plan between the 3D cuFFT transforms around the separate filter ("0") and the
-    (y, z) 2D cuFFT transforms around the fused x-FFT / filter / inverse x-FFT kernel with
-    pencils of ``pencils`` kz values ("1/<kz>"), by the summed time of the forward transform,
-    filter and inverse transform stages of the plan's heaviest structure. Plans where the fused
-    path does not apply keep "0". Returns {plan index: (choice, {choice: ms})}. Drops a
+    (y, z) 2D cuFFT transforms around a fused x-FFT / filter / inverse x-FFT kernel: pencils of
+    ``pencils`` kz values of every channel ("1/<kz>"), or TMA-moved units of (q values, ranks)
+    from ``tma_units`` ("2/<q>/<ranks>", mixed precision), by the summed time of the forward
+    transform, filter and inverse transform stages of the plan's heaviest structure. Plans where
+    no fused path applies keep "0". Returns {plan index: (choice, {choice: ms})}. Drops a
     captured graph."""
     batch._graph = None
     heaviest: dict = {}
@@ -380,11 +382,20 @@ def autotune_fft_x(batch: "D3Batch", pencils: Sequence[int] = (1, 2, 4), reps: i
             if t["fft_x"] != 1 or t["xpencil"] != kz:
                 continue   # no fused kernel for this mesh, species or rank count, or too wide
             times[f"1/{kz}"] = _profiled_stage(batch, i, stages, reps)
+        for xq, xr in tma_units:
+            eng.set_tuning(fft_x=2, xq=xq, xranks=xr)
+            t = eng.tuning()
+            if t["fft_x"] != 2 or (t["xq"], t["xranks"]) != (xq, xr):
+                continue   # float64 plan, or the unit does not apply to this mesh / rank count
+            times[f"2/{xq}/{xr}"] = _profiled_stage(batch, i, stages, reps)
         best = min(times, key=times.get)
+        parts = best.split("/")
         if best == "0":
             eng.set_tuning(fft_x=0, xpencil=-1)
+        elif parts[0] == "1":
+            eng.set_tuning(fft_x=1, xpencil=int(parts[1]))
         else:
-            eng.set_tuning(fft_x=1, xpencil=int(best.split("/")[1]))
+            eng.set_tuning(fft_x=2, xq=int(parts[1]), xranks=int(parts[2]))
         out[n] = (best, times)
     return out
 

@@ -71,14 +71,14 @@ class FourierD3ASECalculator(Calculator):
         self._cell = None
 
     def _build_model(self, atoms):
-        if self.cnfunc != "smooth_cut":
-            raise ValueError(f"Unknown cnfunc '{self.cnfunc}'. This build supports 'smooth_cut'.")
+        if self.cnfunc not in ("smooth_cut", "d4"):
+            raise ValueError(f"Unknown cnfunc '{self.cnfunc}'. Expected 'smooth_cut' or 'd4'.")   # calculator.py:174
         if self.params is None and self.xcfunc != "pbe":
             raise NotImplementedError
         self._model = D3Model(atoms.numbers, _cell_array(atoms), method=self.method,
                               mesh_spacing=self.mesh_spacing, interpolation_nodes=self.interpolation_nodes,
                               c6tol=self.c6tol, params=self.params, r_cut=self.r_cut, k_cutoff=self.k_cutoff,
-                              precision=self.precision, device=self.device)
+                              precision=self.precision, cnfunc=self.cnfunc, device=self.device)
         if self.verbose:
             print(f"Using {self._model.setup.n_rank}-rank decomposition; mesh {self._model.mesh}")
 

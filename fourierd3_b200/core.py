@@ -65,8 +65,8 @@ class FourierD3(torch.nn.Module):
             assert bool(torch.as_tensor(pbc).all()), "particle-mesh only supports 3d pbc"   # core.py:96-97
         if verbose:
             print("Assuming 3D PBC are satisfied")
-        if cnfunc != "smooth_cut":
-            raise NotImplementedError("cnfunc='d4' (k-space CN) is not provided by this build; use 'smooth_cut'")
+        if cnfunc not in ("smooth_cut", "d4"):
+            raise ValueError(f"Unknown cnfunc '{cnfunc}'. Expected 'smooth_cut' or 'd4'.")
         if params is None:
             if xcfunc != "pbe":
                 raise NotImplementedError                                                # core.py:169-170
@@ -112,7 +112,7 @@ class FourierD3(torch.nn.Module):
         self._eng = _engine.Engine(setup, method=method, order=interpolation_nodes, mesh=mesh, ewald_ns=ens,
                                    precision=self.precision, r_cut_bohr=self.r_cut, params=params,
                                    cncorr=None if cncorr is None else np.asarray(torch.as_tensor(cncorr).cpu()),
-                                   device=device)
+                                   cnfunc=cnfunc, device=device)
 
     def _update_cell(self, cell):
         """Set the (possibly strained, grad-carrying) cell in Angstrom (core.py:244-267)."""
@@ -121,10 +121,14 @@ class FourierD3(torch.nn.Module):
 
     def forward(self, positions: torch.Tensor, edge_index: torch.Tensor = None,
                 shifts: torch.Tensor = None) -> torch.Tensor:
-        if edge_index is None or shifts is None:
-            raise ValueError("cnfunc='smooth_cut' needs edge_index and shifts")
         if positions.dim() != 2 or positions.shape[1] != 3 or positions.shape[0] != self.species.shape[0]:
             raise ValueError("positions must be (n_atoms, 3) for the species given at construction")
+        if self.cnfunc == "d4":
+            # k-space CN: no neighbour list; edges, if given, are not used (core.py:512-516)
+            edge_index = torch.zeros((2, 0), dtype=torch.long, device=self.device)
+            shifts = torch.zeros((0, 3), dtype=torch.float64, device=self.device)
+        elif edge_index is None or shifts is None:
+            raise ValueError("cnfunc='smooth_cut' needs edge_index and shifts")
         if edge_index.dim() != 2 or edge_index.shape[0] != 2 or shifts.shape != (edge_index.shape[1], 3):
             raise ValueError("edge_index must be (2, E) and shifts (E, 3)")
         # An edge index outside 0..n_atoms-1 is caught on the device (never dereferenced; the

@@ -20,6 +20,11 @@ struct fd3_plan {
   double* d_eigvecs = nullptr;
   GreenPair* d_green = nullptr;
   GreenPairF* d_green_f = nullptr;
+  // D4 k-space CN: pair constants, self terms, (S channels) 3D transforms
+  int cnfunc = FD3_CN_SMOOTH;
+  CnPair* d_cnpair = nullptr;
+  double* d_cnself = nullptr;
+  cufftHandle fwd_cn = 0, inv_cn = 0;
   float* d_deconv = nullptr;
   float* d_win_axes = nullptr;
   cufftHandle fwd = 0, inv = 0;
@@ -97,6 +102,16 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
   }
   if (d->method != FD3_METHOD_SPME && d->method != FD3_METHOD_PME && d->method != FD3_METHOD_EWALD) return FD3_EINVAL;
   if (d->precision != FD3_PREC_FP64 && d->precision != FD3_PREC_MIXED) return FD3_EINVAL;
+  if (d->cnfunc != FD3_CN_SMOOTH && d->cnfunc != FD3_CN_D4) {
+    set_error("fd3_plan_create", "cnfunc must be FD3_CN_SMOOTH or FD3_CN_D4");
+    return FD3_EINVAL;
+  }
+  if (d->cnfunc == FD3_CN_D4) {
+    if (d->method == FD3_METHOD_EWALD || S > kCn4MaxSpecies || !d->rcov_cn || !d->en) {
+      set_error("fd3_plan_create", "the D4 k-space CN needs method spme or pme, at most 8 species, rcov_cn and en");
+      return FD3_EINVAL;
+    }
+  }
   const bool mesh = d->method != FD3_METHOD_EWALD;
   if (mesh) {
     if (d->order < 1 || d->order > FD3_MAX_ORDER) {
@@ -133,7 +148,9 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
   t.s6 = d->params[0];
   t.s8 = d->params[1];
   t.r_cut = d->r_cut;
-  t.has_cncorr = d->has_cncorr && d->cncorr;
+  // cncorr belongs to the smooth-cutoff CN (core.py:383-384); the D4 CN does not apply it
+  t.has_cncorr = d->has_cncorr && d->cncorr && d->cnfunc == FD3_CN_SMOOTH;
+  p->cnfunc = d->cnfunc;
   for (int s = 0; s < S; ++s) {
     t.rcov[s] = d->rcov[s];
     for (int q = 0; q < 7; ++q) t.cnref[7 * s + q] = d->cnref[7 * s + q];
@@ -287,6 +304,50 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
         if (ws3 > p->fft_ws) p->fft_ws = ws3;
         if (ws4 > p->fft_ws) p->fft_ws = ws4;
       }
+      if (d->cnfunc == FD3_CN_D4) {
+        // D4 CN: 3D transforms of the S species channels, the erfc pair constants and self terms
+        size_t ws5 = 0, ws6 = 0;
+        if ((fr = cufftCreate(&p->fwd_cn)) != CUFFT_SUCCESS || (fr = cufftCreate(&p->inv_cn)) != CUFFT_SUCCESS ||
+            (fr = cufftSetAutoAllocation(p->fwd_cn, 0)) != CUFFT_SUCCESS ||
+            (fr = cufftSetAutoAllocation(p->inv_cn, 0)) != CUFFT_SUCCESS ||
+            (fr = cufftMakePlanMany64(p->fwd_cn, 3, n, nullptr, 1, M, nullptr, 1, Mhi, dp ? CUFFT_D2Z : CUFFT_R2C,
+                                      S, &ws5)) != CUFFT_SUCCESS ||
+            (fr = cufftMakePlanMany64(p->inv_cn, 3, n, nullptr, 1, Mhi, nullptr, 1, M, dp ? CUFFT_Z2D : CUFFT_C2R,
+                                      S, &ws6)) != CUFFT_SUCCESS) {
+          char b[64];
+          snprintf(b, sizeof(b), "cufft status %d", (int)fr);
+          set_error("fd3_plan_create: cufft CN plan", b);
+          rc = FD3_ECUFFT;
+          break;
+        }
+        if (ws5 > p->fft_ws) p->fft_ws = ws5;
+        if (ws6 > p->fft_ws) p->fft_ws = ws6;
+        CnPair* cp = new CnPair[S * S];
+        double* cs = new double[S];
+        const double A = 1.0 / 3.0 + 1.0 / (2.0 * kCn4K0 * kCn4K0);                   // pair_pot.py:321-324
+        const double B = 1.0 / 30.0 + 1.0 / (6.0 * kCn4K0 * kCn4K0) + 1.0 / (8.0 * pow(kCn4K0, 4.0));
+        for (int X = 0; X < S; ++X)
+          for (int Y = 0; Y < S; ++Y) {
+            CnPair& c = cp[X * S + Y];
+            c.r0 = d->rcov_cn[X] + d->rcov_cn[Y];
+            const double ed = fabs(d->en[X] - d->en[Y]) + kCn4K2;
+            c.delta = kCn4K1 * exp(-ed * ed / kCn4K3);
+            c.c0 = 4.0 * kPi * c.delta * c.r0 * c.r0 * c.r0 * A;
+            c.c2 = 4.0 * kPi * c.delta * c.r0 * c.r0 * c.r0 * c.r0 * c.r0 * B;
+            if (X == Y) cs[X] = c.delta / 2.0 * erfc(-kCn4K0);                        // pair_pot.py:330-331
+          }
+        const bool ok = cudaMalloc(&p->d_cnpair, sizeof(CnPair) * S * S) == cudaSuccess &&
+                        cudaMalloc(&p->d_cnself, sizeof(double) * S) == cudaSuccess &&
+                        cudaMemcpy(p->d_cnpair, cp, sizeof(CnPair) * S * S, cudaMemcpyHostToDevice) == cudaSuccess &&
+                        cudaMemcpy(p->d_cnself, cs, sizeof(double) * S, cudaMemcpyHostToDevice) == cudaSuccess;
+        delete[] cp;
+        delete[] cs;
+        if (!ok) {
+          set_error("fd3_plan_create", "upload of the D4 CN constants failed");
+          rc = FD3_ECUDA;
+          break;
+        }
+      }
       // side stream and fork/join events of the fused entry (without them it runs on one stream)
       if (cudaStreamCreateWithFlags(&p->side, cudaStreamNonBlocking) != cudaSuccess ||
           cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
@@ -355,16 +416,16 @@ extern "C" int fd3_plan_set_tuning(fd3_plan* p, int32_t knob, int32_t value) {
     return FD3_OK;
   }
   if (knob == FD3_TUNE_XQ) {
-    if (value != -1 && value != 8 && value != 16 && value != 32) {
-      set_error("fd3_plan_set_tuning", "TMA x-pass q values per unit must be -1 (default), 8, 16 or 32");
+    if (value != -1 && value != 4 && value != 8 && value != 16 && value != 32) {
+      set_error("fd3_plan_set_tuning", "TMA x-pass q values per unit must be -1 (default), 4, 8, 16 or 32");
       return FD3_EINVAL;
     }
     p->mg.xq = value;
     return FD3_OK;
   }
   if (knob == FD3_TUNE_XRANKS) {
-    if (value != -1 && value != 1 && value != 2) {
-      set_error("fd3_plan_set_tuning", "TMA x-pass ranks per unit must be -1 (default), 1 or 2");
+    if (value != -1 && value != 1 && value != 2 && value != 4) {
+      set_error("fd3_plan_set_tuning", "TMA x-pass ranks per unit must be -1 (default), 1, 2 or 4");
       return FD3_EINVAL;
     }
     p->mg.xranks = value;
@@ -440,6 +501,10 @@ extern "C" int fd3_plan_destroy(fd3_plan* p) {
   if (p->fwd) cufftDestroy(p->fwd);
   if (p->inv) cufftDestroy(p->inv);
   if (p->fwd2) cufftDestroy(p->fwd2);
+  if (p->fwd_cn) cufftDestroy(p->fwd_cn);
+  if (p->inv_cn) cufftDestroy(p->inv_cn);
+  cudaFree(p->d_cnpair);
+  cudaFree(p->d_cnself);
   if (p->inv2) cufftDestroy(p->inv2);
   if (p->ev_fork) cudaEventDestroy(p->ev_fork);
   if (p->ev_join) cudaEventDestroy(p->ev_join);
@@ -478,6 +543,8 @@ struct Work {
   HitStore hits;
   EwaldWork ew;
   EdgeIndex ei;
+  void *cn4_rho, *cn4_phi, *cn4_rhat, *cn4_spec;
+  double *cn4_vals, *cn4_part;
   void *rho, *spec, *fftw;
   void* gtab;   // mixed-form Green table
 };
@@ -501,7 +568,9 @@ void carve(const fd3_plan* p, int64_t N, int64_t K_in, Carver& c, Work& w, int64
   // mesh-cell partials: one per gather CTA (atom warps or (tile, species) CTAs)
   int64_t ngt = 1;
   if (p->method != FD3_METHOD_EWALD) ngt = (int64_t)p->mg.nt[0] * p->mg.nt[1] * p->mg.nt[2] * p->S;
-  w.mcell_part = c.take<double>(9 * ((nblk > ngt ? nblk : ngt) + 1));
+  // (+ the D4 CN gradient gather's blocks, appended after the dispersion gather's)
+  const int64_t ncn4 = p->cnfunc == FD3_CN_D4 ? cn4_gather_blocks((int)N) : 0;
+  w.mcell_part = c.take<double>(9 * ((nblk > ngt ? nblk : ngt) + ncn4 + 1));
   const bool mesh = p->method != FD3_METHOD_EWALD;
   size_t Mh = 0, M = 0;
   int64_t Kmesh = 1;
@@ -540,6 +609,16 @@ void carve(const fd3_plan* p, int64_t N, int64_t K_in, Carver& c, Work& w, int64
   w.spec = c.take<char>(mesh ? C * Mh * 2 * es : 1);
   w.fftw = c.take<char>(p->fft_ws);
   w.gtab = c.take<char>(mesh && p->precision == FD3_PREC_MIXED ? green_table_bytes(p->S) : 1);
+  // D4 k-space CN: density / sigma / psi, phi, the density spectrum (kept for the adjoint), the
+  // working spectrum, per-atom spread values and the strain partials
+  const bool d4 = mesh && p->cnfunc == FD3_CN_D4;
+  const size_t S_ = (size_t)p->S;
+  w.cn4_rho = c.take<char>(d4 ? S_ * M * es : 1);
+  w.cn4_phi = c.take<char>(d4 ? S_ * M * es : 1);
+  w.cn4_rhat = c.take<char>(d4 ? S_ * Mh * 2 * es : 1);
+  w.cn4_spec = c.take<char>(d4 ? S_ * Mh * 2 * es : 1);
+  w.cn4_vals = c.take<double>(d4 ? N : 1);
+  w.cn4_part = c.take<double>(d4 ? 9 * ((size_t)cn4_gather_blocks((int)N) + filter_max_blocks() + 2) : 1);
   // edge-list path: edges sorted by source and by destination
   w.ei.ks = c.take<int>(E);
   w.ei.kd = c.take<int>(E);
@@ -711,6 +790,81 @@ static int run_mesh(fd3_plan* p, int N, const double* pos, double ps, const int3
   return mesh_pipeline<float>(p, N, pos, ps, species, w, need_grad, gpos, mcell, n_kspc, n_mcell, presorted, s);
 }
 
+// ------------------------------------------------------------------ D4 k-space CN stages
+// Forward: one-hot species density -> 3D R2C (spectrum kept for the adjoint) -> G^CN -> C2R ->
+// CN values (w.cn). Needs the mesh sort of this call (w.mstart, w.morder).
+template <typename T>
+static int cn4_forward(fd3_plan* p, int N, const double* pos, double ps, const int32_t* species, Work& w,
+                       cudaStream_t s) {
+  MeshGeom m1 = p->mg;
+  m1.R = 1;
+  const int spme = p->method == FD3_METHOD_SPME;
+  FD3_TRY(launch_cn4_values(N, 0, nullptr, w.ci, w.cn4_vals, s));
+  FD3_TRY(launch_spread<T>(m1, N, pos, ps, species, w.cn4_vals, w.ci, w.mstart, w.morder, w.rec, (T*)w.cn4_rho, s));
+  FD3_CUFFT(cufftSetStream(p->fwd_cn, s));
+  FD3_CUFFT(cufftSetWorkArea(p->fwd_cn, w.fftw));
+  if (sizeof(T) == 8)
+    FD3_CUFFT(cufftExecD2Z(p->fwd_cn, (cufftDoubleReal*)w.cn4_rho, (cufftDoubleComplex*)w.cn4_rhat));
+  else
+    FD3_CUFFT(cufftExecR2C(p->fwd_cn, (cufftReal*)w.cn4_rho, (cufftComplex*)w.cn4_rhat));
+  int nb = 0;
+  FD3_TRY(launch_cn4_filter<T>(p->mg, 0, w.ci, p->d_cnpair, p->d_deconv, spme, w.cn4_rhat, w.cn4_spec, nullptr, &nb,
+                               s));
+  FD3_CUFFT(cufftSetStream(p->inv_cn, s));
+  FD3_CUFFT(cufftSetWorkArea(p->inv_cn, w.fftw));
+  if (sizeof(T) == 8)
+    FD3_CUFFT(cufftExecZ2D(p->inv_cn, (cufftDoubleComplex*)w.cn4_spec, (cufftDoubleReal*)w.cn4_phi));
+  else
+    FD3_CUFFT(cufftExecC2R(p->inv_cn, (cufftComplex*)w.cn4_spec, (cufftReal*)w.cn4_phi));
+  return launch_cn4_gather<T>(p->mg, N, 0, pos, ps, w.ci, w.morder, w.rec, w.cn4_phi, nullptr, p->d_cnself, nullptr,
+                              w.cn, nullptr, 0.0, nullptr, nullptr, s);
+}
+
+// Adjoint (after the dispersion gather has written dE/dCN to w.gcn): sigma spread -> R2C -> k-space
+// strain partials and G^CN sigma -> C2R -> gradient gather: gpos = out_scale (gpos + dE/dx_CN),
+// strain partials in w.cn4_part (*n_cnv blocks), positions-fixed cell partials appended to mcell.
+template <typename T>
+static int cn4_adjoint(fd3_plan* p, int N, const double* pos, double ps, const int32_t* species, Work& w,
+                       double* gpos, double out_scale, double* mcell, int* n_cnv, cudaStream_t s) {
+  MeshGeom m1 = p->mg;
+  m1.R = 1;
+  const int spme = p->method == FD3_METHOD_SPME;
+  FD3_TRY(launch_cn4_values(N, 1, w.gcn, w.ci, w.cn4_vals, s));
+  FD3_TRY(launch_spread<T>(m1, N, pos, ps, species, w.cn4_vals, w.ci, w.mstart, w.morder, w.rec, (T*)w.cn4_rho, s));
+  FD3_CUFFT(cufftSetStream(p->fwd_cn, s));
+  FD3_CUFFT(cufftSetWorkArea(p->fwd_cn, w.fftw));
+  if (sizeof(T) == 8)
+    FD3_CUFFT(cufftExecD2Z(p->fwd_cn, (cufftDoubleReal*)w.cn4_rho, (cufftDoubleComplex*)w.cn4_spec));
+  else
+    FD3_CUFFT(cufftExecR2C(p->fwd_cn, (cufftReal*)w.cn4_rho, (cufftComplex*)w.cn4_spec));
+  const int nbg = cn4_gather_blocks(N);
+  int nbf = 0;
+  FD3_TRY(launch_cn4_filter<T>(p->mg, 1, w.ci, p->d_cnpair, p->d_deconv, spme, w.cn4_rhat, w.cn4_spec,
+                               w.cn4_part + 9 * (size_t)nbg, &nbf, s));
+  FD3_CUFFT(cufftSetStream(p->inv_cn, s));
+  FD3_CUFFT(cufftSetWorkArea(p->inv_cn, w.fftw));
+  if (sizeof(T) == 8)
+    FD3_CUFFT(cufftExecZ2D(p->inv_cn, (cufftDoubleComplex*)w.cn4_spec, (cufftDoubleReal*)w.cn4_rho));
+  else
+    FD3_CUFFT(cufftExecC2R(p->inv_cn, (cufftComplex*)w.cn4_spec, (cufftReal*)w.cn4_rho));
+  FD3_TRY(launch_cn4_gather<T>(p->mg, N, 1, pos, ps, w.ci, w.morder, w.rec, w.cn4_phi, w.cn4_rho, p->d_cnself, w.gcn,
+                               w.cn, gpos, out_scale, w.cn4_part, mcell, s));
+  *n_cnv = nbg + nbf;
+  return FD3_OK;
+}
+
+static int cn4_forward_any(fd3_plan* p, int N, const double* pos, double ps, const int32_t* species, Work& w,
+                           cudaStream_t s) {
+  return p->precision == FD3_PREC_FP64 ? cn4_forward<double>(p, N, pos, ps, species, w, s)
+                                       : cn4_forward<float>(p, N, pos, ps, species, w, s);
+}
+static int cn4_adjoint_any(fd3_plan* p, int N, const double* pos, double ps, const int32_t* species, Work& w,
+                           double* gpos, double out_scale, double* mcell, int* n_cnv, cudaStream_t s) {
+  return p->precision == FD3_PREC_FP64
+             ? cn4_adjoint<double>(p, N, pos, ps, species, w, gpos, out_scale, mcell, n_cnv, s)
+             : cn4_adjoint<float>(p, N, pos, ps, species, w, gpos, out_scale, mcell, n_cnv, s);
+}
+
 // ------------------------------------------------------------------ edge-list entry
 extern "C" int fd3_energy_edges(fd3_plan* p, int64_t n_atoms, const double* d_pos, const int32_t* d_species,
                                 const double* d_cell, int64_t n_edges, const int64_t* d_src, const int64_t* d_dst,
@@ -726,6 +880,26 @@ extern "C" int fd3_energy_edges(fd3_plan* p, int64_t n_atoms, const double* d_po
   FD3_TRY(check_work(p, N, 0, d_work, work_bytes, w, n_edges));
   prof_begin(p, s);
   FD3_TRY(launch_cellinfo(d_cell, 1.0, w.ci, s));
+  if (p->cnfunc == FD3_CN_D4) {
+    // k-space D4 CN: no edges (the reference's forward ignores them, core.py:512-516)
+    int n_self = 0, n_kspc = 0, n_mcell = 0, n_cnv = 0;
+    FD3_TRY(mesh_sort(p, N, d_pos, 1.0, d_species, w, s));
+    FD3_TRY(cn4_forward_any(p, N, d_pos, 1.0, d_species, w, s));
+    FD3_TRY(launch_c6_atoms(N, d_species, p->d_tab, p->d_eigvecs, p->R, w.cn, w.c6, w.dc6, w.self_part, &n_self, s));
+    prof_mark(p, s, "cn_c6");
+    FD3_TRY(run_mesh(p, N, d_pos, 1.0, d_species, w, need_grad != 0, d_gpos, w.mcell_part, &n_kspc, &n_mcell, s,
+                     true));
+    if (need_grad) {
+      FD3_TRY(cn4_adjoint_any(p, N, d_pos, 1.0, d_species, w, d_gpos, 1.0, w.mcell_part + 9 * (size_t)n_mcell,
+                              &n_cnv, s));
+      n_mcell += cn4_gather_blocks(N);
+    }
+    prof_mark(p, s, "cn_adjoint");
+    Partials pa{w.self_part, n_self, w.kspc_part, n_kspc, w.cn4_part, n_cnv, w.mcell_part, n_mcell};
+    FD3_TRY(launch_finalize(pa, w.ci, 0, 1.0, d_energy, need_grad ? d_gcell : nullptr, s));
+    prof_mark(p, s, "finalize");
+    return FD3_OK;
+  }
   // edges sorted by source and destination; the CN is summed per atom in edge order
   const double mask_r2 = p->edge_cutoff ? p->h_tab.r_cut * p->h_tab.r_cut : INFINITY;
   FD3_TRY(launch_edge_index(n_edges, N, d_src, d_dst, w.ei, s));
@@ -763,6 +937,23 @@ extern "C" int fd3_energy_forces_stress(fd3_plan* p, int64_t n_atoms, const doub
   FD3_TRY(check_work(p, N, K, d_work, work_bytes, w));
   prof_begin(p, s);
   FD3_TRY(launch_cellinfo(d_cell_ang, kAngToBohr, w.ci, s));
+  if (p->cnfunc == FD3_CN_D4) {
+    // k-space D4 CN: no neighbour search (calculator.py:171-173)
+    int n_self = 0, n_kspc = 0, n_mcell = 0, n_cnv = 0;
+    FD3_TRY(mesh_sort(p, N, d_pos_ang, kAngToBohr, d_species, w, s));
+    FD3_TRY(cn4_forward_any(p, N, d_pos_ang, kAngToBohr, d_species, w, s));
+    FD3_TRY(launch_c6_atoms(N, d_species, p->d_tab, p->d_eigvecs, p->R, w.cn, w.c6, w.dc6, w.self_part, &n_self, s));
+    prof_mark(p, s, "cn_c6");
+    FD3_TRY(run_mesh(p, N, d_pos_ang, kAngToBohr, d_species, w, true, d_forces, nullptr, &n_kspc, &n_mcell, s,
+                     true));
+    FD3_TRY(cn4_adjoint_any(p, N, d_pos_ang, kAngToBohr, d_species, w, d_forces, -kHartreeToEv * kAngToBohr,
+                            nullptr, &n_cnv, s));
+    prof_mark(p, s, "cn_adjoint");
+    Partials pa{w.self_part, n_self, w.kspc_part, n_kspc, w.cn4_part, n_cnv, nullptr, 0};
+    FD3_TRY(launch_finalize(pa, w.ci, 1, kHartreeToEv, d_energy, d_stress, s));
+    prof_mark(p, s, "finalize");
+    return FD3_OK;
+  }
   const bool fork = p->side != nullptr && p->method != FD3_METHOD_EWALD;
   if (fork) {   // mesh sort on the side stream, beside the cell list and the CN stage
     FD3_CUDA(cudaEventRecord(p->ev_fork, s));

@@ -178,6 +178,27 @@ int launch_gather(const MeshGeom& mg, int n, const double* pos, double pos_scale
                   const int* key_start, const MeshRecords& rec, const T* phi, double* gcn, double* gpos,
                   double* mcell_part, int* n_blocks, cudaStream_t s);
 
+// ---- D4 coordination numbers in k-space (cnfunc = 'd4') ----------------------------------
+// Per species pair of the erfc CN function (pair_pot.py:286-325): r0 = rcov_cn_A + rcov_cn_B,
+// delta = k1 exp(-(|EN_A - EN_B| + k2)^2 / k3), Taylor constants c0, c2 of the small-k branch.
+struct CnPair {
+  double r0, delta, c0, c2;
+};
+constexpr double kCn4K0 = 7.5, kCn4K1 = 4.10451, kCn4K2 = 19.08857, kCn4K3 = 2.0 * 11.28174 * 11.28174;
+constexpr int kCn4MaxSpecies = 8;
+int cn4_gather_blocks(int n);
+int launch_cn4_values(int n, int adjoint, const double* gcn, const CellInfo* ci, double* vals, cudaStream_t s);
+// forward (adjoint = 0): out = G rhat; adjoint: k-space strain partials (9 per block) and out <- G out
+template <typename T>
+int launch_cn4_filter(const MeshGeom& mg, int adjoint, const CellInfo* ci, const CnPair* cp, const float* deconv,
+                      int spme, const void* rhat, void* out, double* part, int* n_blocks, cudaStream_t s);
+// mode 0: CN values from phi; mode 1: gradient gather (phi, psi), volume strain partials, cell partials
+template <typename T>
+int launch_cn4_gather(const MeshGeom& mg, int n, int mode, const double* pos, double ps, const CellInfo* ci,
+                      const int* order, const MeshRecords& rec, const void* phi, const void* psi,
+                      const double* cnself, const double* gcn, double* cn, double* gpos, double out_scale,
+                      double* vir_part, double* mcell_part, cudaStream_t s);
+
 // ---- direct Ewald k-sum --------------------------------------------------------------
 struct EwaldGeom {
   int ns[3];   // Miller-index box (fftfreq order per axis)

@@ -547,12 +547,14 @@ __global__ void __launch_bounds__(1024) k_finalize(Partials p, const CellInfo* _
   for (int a = 0; a < 3; ++a)
     for (int b = 0; b < 3; ++b) Wk[3 * a + b] = ((a == b ? Q : 0.0) + Vs[3 * a + b]) / (2.0 * vol);
   if (mode == 0) {
+    // the strain derivative (k-space, plus the D4 CN's when present) converted to dE/dcell with
+    // positions fixed: (W_ab - sum_i g_ia x_ib) inv_bA
     *energy = E * e_scale;
     if (out9) {
       for (int A = 0; A < 3; ++A)
         for (int a = 0; a < 3; ++a) {
           double s = 0.0;
-          for (int b = 0; b < 3; ++b) s += Wk[3 * a + b] * ci->inv[3 * b + A];
+          for (int b = 0; b < 3; ++b) s += (Wk[3 * a + b] + tot[8 + 3 * a + b]) * ci->inv[3 * b + A];
           out9[3 * A + a] = (s - tot[17 + 3 * A + a]) * e_scale;
         }
     }

@@ -28,8 +28,8 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 // strides must be multiples of 16 bytes) and two units in shared memory.
 bool xpass_applies(const MeshGeom& mg, int Q, int RG) {
   if (mg.n[0] != 64 && mg.n[0] != 128 && mg.n[0] != 256) return false;
-  if (mg.S > 4 || RG > mg.R || (RG != 1 && RG != 2)) return false;
-  if (Q != 8 && Q != 16 && Q != 32) return false;
+  if (mg.S > 4 || RG > mg.R || (RG != 1 && RG != 2 && RG != 4)) return false;
+  if (Q != 4 && Q != 8 && Q != 16 && Q != 32) return false;
   if ((((long long)mg.n[1] * mg.nzh) & 1) != 0) return false;
   return xpass_stages((size_t)mg.S * RG * mg.n[0] * Q * sizeof(float2)) >= 2;
 }

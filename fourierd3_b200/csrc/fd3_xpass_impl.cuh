@@ -78,11 +78,13 @@ template <int N1, int N2, int Q>
 int launch_xpass_r(const XpassArgs& a) {
   if (a.RG == 1) return launch_xpass_s<N1, N2, Q, 1>(a);
   if (a.RG == 2) return launch_xpass_s<N1, N2, Q, 2>(a);
+  if (a.RG == 4) return launch_xpass_s<N1, N2, Q, 4>(a);
   return FD3_EINVAL;
 }
 
 template <int N1, int N2>
 int launch_xpass_nx(const XpassArgs& a) {
+  if (a.Q == 4) return launch_xpass_r<N1, N2, 4>(a);
   if (a.Q == 8) return launch_xpass_r<N1, N2, 8>(a);
   if (a.Q == 16) return launch_xpass_r<N1, N2, 16>(a);
   if (a.Q == 32) return launch_xpass_r<N1, N2, 32>(a);

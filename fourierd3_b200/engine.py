@@ -37,6 +37,8 @@ class SpeciesSetup:
     cnref: np.ndarray      # (S, 7)
     sqrtq: np.ndarray      # (S,)
     c6_err: float
+    rcov_cn: np.ndarray = None   # (S,) D4 CN covalent radii, float32 values widened (pair_pot.py:294)
+    en: np.ndarray = None        # (S,) electronegativities (pair_pot.py:301)
 
     @property
     def n_species(self) -> int:
@@ -59,7 +61,8 @@ def species_setup(numbers: Sequence[int], c6tol: float) -> SpeciesSetup:
         eigs=np.ascontiguousarray(eigs, dtype=np.float64),
         eigvecs=np.ascontiguousarray(vecs, dtype=np.float64),
         rcov=t["rcov"][uniq].astype(np.float64), cnref=t["cnref"][uniq].astype(np.float64),
-        sqrtq=t["sqrtQz"][uniq].astype(np.float64), c6_err=float(err))
+        sqrtq=t["sqrtQz"][uniq].astype(np.float64), c6_err=float(err),
+        rcov_cn=t["rcov_cn"][uniq].astype(np.float64), en=t["en"][uniq].astype(np.float64))
 
 
 def _stream_ptr(device: torch.device) -> int:
@@ -72,13 +75,20 @@ class Engine:
     def __init__(self, setup: SpeciesSetup, *, method: str, order: int, mesh: Sequence[int],
                  ewald_ns: Sequence[int] = (0, 0, 0), precision: str = "fp64", r_cut_bohr: float,
                  params: Sequence[float] = PBE_BJ, cncorr: Optional[np.ndarray] = None,
-                 device: torch.device):
+                 cnfunc: str = "smooth_cut", device: torch.device):
         if device.type != "cuda":
             raise RuntimeError("fourierd3_b200 computes on CUDA devices only (B200, sm_100a)")
         if method not in _native.METHODS:
             raise ValueError(f"unknown method {method!r}; expected 'spme', 'pme' or 'ewald'")
         if precision not in ("fp64", "mixed"):
             raise ValueError("precision must be 'fp64' or 'mixed'")
+        if cnfunc not in _native.CNFUNCS:
+            raise ValueError(f"Unknown cnfunc '{cnfunc}'. Expected 'smooth_cut' or 'd4'.")
+        if cnfunc == "d4" and (method == "ewald" or setup.n_species > 8):
+            raise NotImplementedError(
+                "cnfunc='d4' is built for the mesh methods ('spme', 'pme') with at most 8 species; the reference's "
+                "own Ewald branch of the D4 CN reads an attribute it never defines (src/fourierd3/core.py:436)")
+        self.cnfunc = cnfunc
         self.setup = setup
         self.method = method
         self.order = int(order)
@@ -112,6 +122,10 @@ class Engine:
         if cncorr is not None:
             d.has_cncorr = 1
             d.cncorr = _native.dptr(keep(np.asarray(cncorr, dtype=np.float64).reshape(-1, 2)))
+        d.cnfunc = _native.CNFUNCS[cnfunc]
+        if cnfunc == "d4":
+            d.rcov_cn = _native.dptr(keep(setup.rcov_cn))
+            d.en = _native.dptr(keep(setup.en))
         if method == "spme":
             win = keep(geometry.spme_window(self.mesh, self.order), np.float32)
             d.deconv = win.ctypes.data_as(ctypes.POINTER(ctypes.c_float))

@@ -22,7 +22,7 @@ class D3Model:
 
     def __init__(self, numbers, cell, *, method: str = "spme", mesh_spacing: float = 1.2,
                  interpolation_nodes: int = 5, c6tol: float = 1.0, params=None, r_cut: float = 6.0,
-                 k_cutoff: float = 10.0, cncorr=None, precision: str = "fp64",
+                 k_cutoff: float = 10.0, cncorr=None, precision: str = "fp64", cnfunc: str = "smooth_cut",
                  device: Optional[torch.device] = None):
         self.device = torch.device(device) if device is not None else torch.device("cuda")
         self.numbers = np.asarray(numbers)
@@ -38,7 +38,7 @@ class D3Model:
                                      ewald_ns=ens, precision=precision,
                                      r_cut_bohr=self.r_cut * geometry.ANGSTROM_TO_BOHR,
                                      params=params if params is not None else _engine.PBE_BJ,
-                                     cncorr=cncorr, device=self.device)
+                                     cncorr=cncorr, cnfunc=cnfunc, device=self.device)
 
     def __call__(self, positions, cell, out=None):
         pos = torch.as_tensor(positions, dtype=torch.float64)

@@ -127,14 +127,23 @@ class VelocityVerlet:
         v = self.state.velocities
         return float(0.5 * (self.masses[:, None] * v * v).sum() / ACC)
 
+    def _drift(self, pos, vel, f):
+        """Half kick and drift: (v(t + dt/2), x(t + dt))."""
+        v_half = vel + 0.5 * self.dt * f * ACC / self.masses[:, None]
+        return v_half, pos + self.dt * v_half
+
     def step(self) -> MDState:
         if self.use_graph:
             return self._graph_step()
         st = self.state
-        a = st.forces * ACC / self.masses[:, None]
-        v_half = st.velocities + 0.5 * self.dt * a
-        pos = st.positions + self.dt * v_half
-        e, f, s = self.forces(pos)
+        v_half, pos = self._drift(st.positions, st.velocities, st.forces)
+        if self.verlet_edges:
+            if self._needs_rebuild(pos):
+                self._rebuild(pos)
+            e, f, s = self._forces_device(pos, torch.stack((self._vi, self._vj)), self._vS, self.model)
+            e, s = float(e), s.cpu().numpy()
+        else:
+            e, f, s = self.forces(pos)
         v = v_half + 0.5 * self.dt * f * ACC / self.masses[:, None]
         self.state = MDState(st.step + 1, pos, v, f, e, s)
         return self.state
@@ -143,8 +152,7 @@ class VelocityVerlet:
     def _step_body(self) -> None:
         """One velocity-Verlet step on the static buffers (recorded into the graph)."""
         g = self._static
-        v_half = g["vel"] + 0.5 * self.dt * g["f"] * ACC / self.masses[:, None]
-        pos = g["pos"] + self.dt * v_half
+        v_half, pos = self._drift(g["pos"], g["vel"], g["f"])
         e, f, s = self._forces_device(pos, g["ei"], g["us"], self.model)
         g["vel"].copy_(v_half + 0.5 * self.dt * f * ACC / self.masses[:, None])
         g["pos"].copy_(pos)
@@ -174,9 +182,12 @@ class VelocityVerlet:
 
     def _graph_step(self) -> MDState:
         st = self.state
-        rebuild = self._needs_rebuild(st.positions)
+        # the positions the step will evaluate forces at (the same ops the graph runs, so the
+        # same values): the list is rebuilt there, exactly as the eager step does
+        _, pos = self._drift(st.positions, st.velocities, st.forces)
+        rebuild = self._needs_rebuild(pos)
         if rebuild:
-            self._rebuild(st.positions)
+            self._rebuild(pos)
         if rebuild or self._graph is None:
             self._capture()
         self._graph.replay()

@@ -70,7 +70,13 @@ typedef struct {
                              sinc^(2p) clamped at 1e-10, exactly as the reference
                              builds it (pair_pot.py:180-207); NULL: evaluate it in
                              float64 inside the filter kernel instead            */
+  int32_t cnfunc;         /* FD3_CN_SMOOTH (core.py:323-386, needs neighbours) or
+                             FD3_CN_D4 (k-space D4 CN, core.py:388-447: spme/pme,
+                             at most 8 species, no neighbour list; cncorr unused) */
+  const double* rcov_cn;  /* [S] D4 CN covalent radii, Bohr (pair_pot.py:294); D4 */
+  const double* en;       /* [S] electronegativities (pair_pot.py:301); D4 only   */
 } fd3_plan_desc;
+enum { FD3_CN_SMOOTH = 0, FD3_CN_D4 = 1 };
 
 /* Replaces: FourierD3.__init__ buffers + KSpaceFilterD3 / MeshInterpolatorD3 /
  * D3Potential construction (src/fourierd3/core.py:50-242). */

@@ -101,6 +101,47 @@ class GreenD3:
         return f6 + self.qq[ex] * f8
 
 
+class CNPotentialD4:
+    """Fourier transform of the D4 CN pair function f_AB(r) = delta_AB / 2 erfc(k0 (r - r0_AB) / r0_AB)
+    (pair_pot.py:235-406): r0_AB = rcov_cn_A + rcov_cn_B, delta_AB = k1 exp(-(|EN_A - EN_B| + k2)^2 / k3),
+    closed form for k r0 >= 1e-3 and a k^2 Taylor branch below; self term delta_AA / 2 erfc(-k0)."""
+
+    K0, K1, K2, K3 = 7.5, 4.10451, 19.08857, 2 * 11.28174 ** 2      # pair_pot.py:275-278
+
+    def __init__(self, types, dtype=torch.float64):
+        t = tables.load_tables()
+        idx = torch.as_tensor(list(types))
+        rc = torch.tensor(t["rcov_cn"])[idx].to(dtype)               # pair_pot.py:294-297
+        self.r0 = rc.unsqueeze(0) + rc.unsqueeze(1)
+        en = torch.tensor(t["en"])[idx].to(dtype)                    # pair_pot.py:301-305
+        ed = torch.abs(en.unsqueeze(0) - en.unsqueeze(1))
+        self.delta = self.K1 * torch.exp(-torch.square(ed + self.K2) / self.K3)
+        k0 = torch.tensor(self.K0, dtype=dtype)
+        self.k0sq = k0 * k0
+        self.pi = torch.tensor(math.pi, dtype=dtype)
+        A = 1.0 / 3.0 + 1.0 / (2.0 * self.K0 ** 2)                   # pair_pot.py:321-324
+        B = 1.0 / 30.0 + 1.0 / (6.0 * self.K0 ** 2) + 1.0 / (8.0 * self.K0 ** 4)
+        r0sq = self.r0 * self.r0
+        self.c0 = 4.0 * self.pi * self.delta * r0sq * self.r0 * A
+        self.c2 = 4.0 * self.pi * self.delta * r0sq * r0sq * self.r0 * B
+        self.selfcont = (torch.diagonal(self.delta) / 2.0 * torch.erfc(-k0)).view(-1)   # pair_pot.py:330-331
+
+    def __call__(self, k: torch.Tensor) -> torch.Tensor:
+        """|k| of any shape -> hat f of shape (S, S, *k.shape) (pair_pot.py:336-376)."""
+        ex = (slice(None), slice(None)) + (None,) * k.dim()
+        r0, delta = self.r0[ex], self.delta[ex]
+        kk = k.unsqueeze(0).unsqueeze(0)
+        small = kk * r0 < 1e-3
+        ks = torch.where(small, torch.ones_like(kk), kk)
+        kr0 = ks * r0
+        gauss = torch.exp(-kr0 * kr0 / (4.0 * self.k0sq))
+        s, c = torch.sin(kr0), torch.cos(kr0)
+        term1 = (s - kr0 * c) / (ks * ks * ks)
+        term2 = r0 * r0 * s / (2.0 * self.k0sq * ks)
+        large = 4.0 * self.pi * delta * gauss * (term1 + term2)
+        return torch.where(small, self.c0[ex] - self.c2[ex] * kk * kk, large)
+
+
 def sinc_window(ns, order: int) -> torch.Tensor:
     """prod_a sinc(m_a / n_a)^(2p), clamped at 1e-10, on the rfft half grid (pair_pot.py:184-207).
 
@@ -132,9 +173,13 @@ class OracleFourierD3:
 
     def __init__(self, numbers: Sequence[int], cell, mesh_spacing: float = 1.2, c6tol: float = 1.0,
                  method: str = "spme", params=None, interpolation_nodes: int = 5,
-                 k_cutoff: float = 10.0, r_cut: float = 6.0, cncorr: Optional[np.ndarray] = None):
+                 k_cutoff: float = 10.0, r_cut: float = 6.0, cncorr: Optional[np.ndarray] = None,
+                 cnfunc: str = "smooth_cut"):
         dt = torch.float64
         self.dtype = dt
+        if cnfunc not in ("smooth_cut", "d4"):
+            raise ValueError(f"Unknown cnfunc '{cnfunc}'")                # calculator.py:174
+        self.cnfunc = cnfunc
         self.method = method
         self.order = int(interpolation_nodes)
         numbers = np.asarray(numbers)
@@ -158,6 +203,7 @@ class OracleFourierD3:
         p = params if params is not None else PBE_BJ
         self.params = torch.tensor(p, dtype=dt)
         self.green = GreenD3(sqrtq, self.params)
+        self.cnpot = CNPotentialD4(self.types, dt) if cnfunc == "d4" else None   # core.py:177-179
         self.cncorr = None if cncorr is None else torch.as_tensor(np.asarray(cncorr), dtype=dt)
         if method in ("spme", "pme"):
             self.ns_mesh = pme.get_ns_mesh(cell_b, mesh_spacing * ANGSTROM_TO_BOHR)   # core.py:186
@@ -194,15 +240,13 @@ class OracleFourierD3:
         w = torch.softmax(logits, dim=1)
         return torch.einsum("nk,nkr->nr", w, self.vq[self.species])
 
-    def kspace_mesh(self, pos_b, c6, cell_b):
-        """SPME/PME k-space sum (core.py:553-561, mesh_interpolator_d3.py:74-138,
-        kspace_filter_d3.py:29-70)."""
+    def _stencil(self, pos_b, cell_b):
+        """Per-atom stencil weights (N, p^3) and flat mesh indices (N p^3,) of the torch-pme
+        interpolator (MeshInterpolator.compute_weights, core.py:555)."""
         n_atoms = pos_b.shape[0]
-        S, R = self.n_species, self.n_rank
         nx, ny, nz = (int(v) for v in self.ns_mesh)
-        inv = inv3(cell_b)
         p = self.order
-        w, base = pme.mesh_weights(pos_b, inv, self.ns_mesh, p,
+        w, base = pme.mesh_weights(pos_b, inv3(cell_b), self.ns_mesh, p,
                                    "P3M" if self.method == "spme" else "Lagrange")
         sh = torch.arange(p)
         ix = (base[:, 0][:, None] + sh[None, :]) % nx                # (N, p)
@@ -211,6 +255,57 @@ class OracleFourierD3:
         wx, wy, wz = w[:, :, 0].T, w[:, :, 1].T, w[:, :, 2].T        # (N, p)
         wgeo = (wx[:, :, None, None] * wy[:, None, :, None] * wz[:, None, None, :]).reshape(n_atoms, -1)
         lin = (iz[:, None, None, :] + nz * (iy[:, None, :, None] + ny * ix[:, :, None, None])).reshape(-1)
+        return wgeo, lin
+
+    # --- core.py:388-447: D4 CN in k-space (no neighbour list) -----------------------
+    def cn_d4(self, pos_b, cell_b, volume):
+        """CN_i = phi_{X_i}(r_i) / volume - f_{X_i X_i}(0), phi_X = sum_Y G^CN_XY * rho_Y with rho the
+        one-hot species density. The mesh branch spreads with the interpolation weights of the
+        current positions and the Ewald branch uses the (N, S) one-hot species matrix: the
+        reference's own code reads weights only computed later in forward (core.py:514 vs 555)
+        and an attribute it never defines (core.py:436); this is the algorithm with both repaired."""
+        n_atoms = pos_b.shape[0]
+        S = self.n_species
+        if self.method in ("spme", "pme"):
+            nx, ny, nz = (int(v) for v in self.ns_mesh)
+            wgeo, lin = self._stencil(pos_b, cell_b)
+            onehot = torch.zeros(n_atoms, S, dtype=self.dtype)
+            onehot[torch.arange(n_atoms), self.species] = 1.0            # core.py:417-418
+            vals = (onehot.unsqueeze(1) * wgeo.unsqueeze(2)).flatten(0, 1)
+            rho = torch.zeros(nx * ny * nz, S, dtype=self.dtype).index_add(0, lin, vals)
+            rho = rho.t().contiguous().view(S, nx, ny, nz)
+            hat = torch.fft.rfftn(rho, norm="backward", dim=(1, 2, 3))   # kspace_filter_d3.py:142
+            kvec = pme.generate_kvectors(cell_b, self.ns_mesh, for_ewald=False)
+            G = self.cnpot(torch.linalg.norm(kvec, dim=-1))              # (S, S, nx, ny, nzh)
+            if self.method == "spme":
+                G = G / sinc_window(self.ns_mesh, self.order)           # pair_pot.py:378-399
+            Gf = G.flatten(2).permute(2, 0, 1).to(torch.complex128)     # (nk, S, S)
+            interm = torch.einsum("kab,bk->ak", Gf, hat.flatten(1))     # kspace_filter_d3.py:148
+            phi = torch.fft.irfftn(interm.view(hat.shape), norm="forward", s=(nx, ny, nz), dim=(1, 2, 3))
+            flat = phi.reshape(S, -1).t()                                # (M, S)
+            g = flat[lin, :].view(n_atoms, -1, S)
+            phi_atoms = (wgeo.unsqueeze(2) * g).sum(dim=1)              # mesh_interpolator_d3.py:140-189
+        else:
+            kvec = pme.generate_kvectors(cell_b, self.ns, for_ewald=True)
+            G = self.cnpot(torch.linalg.norm(kvec, dim=1))               # (S, S, nk)
+            arg = torch.matmul(kvec, pos_b.T)
+            ex = torch.stack([torch.cos(arg), torch.sin(arg)], dim=0)   # (2, nk, N)
+            nk = ex.shape[1]
+            onehot = torch.nn.functional.one_hot(self.species, S).to(self.dtype)
+            Sf = torch.mm(ex.reshape(2 * nk, n_atoms), onehot).view(2, nk, S)   # core.py:436
+            F = torch.einsum("tkj,kij->tki", Sf, G.permute(2, 0, 1))
+            phi_atoms = torch.einsum("tka,tki->ai", ex, F)
+        cn_raw = phi_atoms[torch.arange(n_atoms), self.species]
+        return cn_raw / volume - self.cnpot.selfcont[self.species]      # core.py:444-446
+
+    def kspace_mesh(self, pos_b, c6, cell_b):
+        """SPME/PME k-space sum (core.py:553-561, mesh_interpolator_d3.py:74-138,
+        kspace_filter_d3.py:29-70)."""
+        n_atoms = pos_b.shape[0]
+        S, R = self.n_species, self.n_rank
+        nx, ny, nz = (int(v) for v in self.ns_mesh)
+        p = self.order
+        wgeo, lin = self._stencil(pos_b, cell_b)
         onehot = torch.zeros(n_atoms, S, R, dtype=self.dtype).index_put(
             (torch.arange(n_atoms), self.species), c6)               # core.py:537-543
         vals = (onehot.reshape(n_atoms, S * R).unsqueeze(1) * wgeo.unsqueeze(2)).flatten(0, 1)
@@ -249,7 +344,10 @@ class OracleFourierD3:
         volume = torch.abs(det3(cell_b))                             # core.py:255
         pos_b = pos_ang * self.a2b                                   # core.py:505
         shifts_b = shifts_ang * self.a2b                             # core.py:507
-        cn = self.cn(pos_b, edge_index, shifts_b)
+        if self.cnfunc == "d4":
+            cn = self.cn_d4(pos_b, cell_b, volume)                   # core.py:517-524
+        else:
+            cn = self.cn(pos_b, edge_index, shifts_b)
         c6 = self.c6_factors(cn)
         tmp = torch.sum(torch.square(c6) * self.green.selfcont[self.species].unsqueeze(1), dim=0)
         vself = torch.dot(self.eigs, tmp)                            # core.py:547-550
@@ -269,7 +367,10 @@ class OracleFourierD3:
         scell = cell_t + torch.einsum("ab,Ab->Aa", strain, cell_t)
         pos = torch.tensor(np.asarray(positions), dtype=dt, requires_grad=True)
         spos = pos + torch.einsum("ab,ib->ia", strain, pos)
-        if edges is None:
+        if self.cnfunc == "d4":                                       # calculator.py:171-173
+            edge_index = torch.zeros((2, 0), dtype=torch.long)
+            ushift = torch.zeros((0, 3), dtype=dt)
+        elif edges is None:
             i, j, S = neighbour_list(np.asarray(positions, dtype=np.float64),
                                      np.asarray(cell, dtype=np.float64), self.r_cut_ang)
             edge_index = torch.tensor(np.stack((i, j)), dtype=torch.long)

@@ -85,7 +85,7 @@ def lagrange_weights(x: torch.Tensor, p: int) -> torch.Tensor:
 def mesh_weights(positions: torch.Tensor, inverse_cell: torch.Tensor, ns_mesh, p: int, method: str):
     """Return (weights (p, N, 3), base (N, 3) int64) -- base is the first stencil node
     (not yet wrapped); node k of axis a sits at (base[:, a] + k) mod n_a."""
-    ns = torch.as_tensor([int(v) for v in ns_mesh], dtype=positions.dtype)
+    ns = torch.as_tensor([int(v) for v in ns_mesh], dtype=positions.dtype, device=positions.device)
     u = ns * torch.matmul(positions, inverse_cell)
     if p % 2 == 0:
         ref = torch.floor(u)

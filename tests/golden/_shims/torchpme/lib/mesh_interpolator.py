@@ -25,9 +25,10 @@ class MeshInterpolator:
         p = self.interpolation_nodes
         w, base = mesh_weights(positions, self.inverse_cell, self.ns_mesh, p, self.method)
         self.interpolation_weights = w                                   # (p, N, 3)
-        sx, sy, sz = torch.meshgrid(torch.arange(p), torch.arange(p), torch.arange(p), indexing="ij")
+        ar = torch.arange(p, device=positions.device)
+        sx, sy, sz = torch.meshgrid(ar, ar, ar, indexing="ij")
         self.x_shifts, self.y_shifts, self.z_shifts = sx.flatten(), sy.flatten(), sz.flatten()
-        nodes = base.unsqueeze(0) + torch.arange(p).view(p, 1, 1)        # (p, N, 3)
+        nodes = base.unsqueeze(0) + ar.view(p, 1, 1)                     # (p, N, 3)
         self.x_indices = nodes[self.x_shifts, :, 0] % int(self.ns_mesh[0])
         self.y_indices = nodes[self.y_shifts, :, 1] % int(self.ns_mesh[1])
         self.z_indices = nodes[self.z_shifts, :, 2] % int(self.ns_mesh[2])

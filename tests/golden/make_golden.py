@@ -35,7 +35,30 @@ def _import_reference(ref_root: str):
     from fourierd3_b200 import tables
 
     futils.load_c6ref = lambda types: tables.c6ref_matrix(list(types))
+    _repair_d4(fourierd3)
     return fourierd3
+
+
+def _repair_d4(fourierd3):
+    """The reference's D4 CN (cnfunc='d4') does not run as written: the mesh branch of
+    compute_cn_d4 spreads with interpolation weights that forward only computes afterwards
+    (src/fourierd3/core.py:514-516 vs :555), and the Ewald branch multiplies by
+    self.one_hot_species, which is never defined (core.py:436). This wrapper supplies both --
+    the weights at the positions passed in, and the (N, S) one-hot species matrix -- and then
+    runs the reference's own compute_cn_d4 unchanged."""
+    import torch
+
+    core = fourierd3.core
+    orig = core.FourierD3.compute_cn_d4
+
+    def compute_cn_d4(self, positions, ex=None, nk=None):
+        if self.method in ("pme", "spme"):
+            self.mesh_interpolator.compute_weights(positions)
+        else:
+            self.one_hot_species = torch.nn.functional.one_hot(self.species, self.n_species).to(positions.dtype)
+        return orig(self, positions, ex, nk)
+
+    core.FourierD3.compute_cn_d4 = compute_cn_d4
 
 
 def cases():
@@ -58,6 +81,11 @@ def cases():
     out.append(("tiny_6_spme_p4", pt, ct, zt, dict(base, interpolation_nodes=4, mesh_spacing=0.8)))
     # cncorr: the optional affine CN correction (core.py:383-384)
     out.append(("sio2_648_spme_p5_cncorr", p, c, z, dict(base, cncorr=[[0.05, 0.9], [-0.02, 1.1]])))
+    # D4 coordination numbers in k-space (no neighbour list)
+    out.append(("sio2_648_spme_p5_d4", p, c, z, dict(base, cnfunc="d4")))
+    out.append(("hcno_240_pme_p6_d4", ph, ch, zh, dict(base, method="pme", mesh_spacing=1.0, interpolation_nodes=6,
+                                                       c6tol=1e-2, cnfunc="d4")))
+    out.append(("rand_96_ewald_k3_d4", pr, cr, zr, dict(base, method="ewald", k_cutoff=3.0, cnfunc="d4")))
     return out
 
 
@@ -85,7 +113,14 @@ def main(ref_root: str) -> None:
             model._update_cell(cell_t)
             pos_b = torch.tensor(pos) * a2b
             sh_b = torch.matmul(ushift, cell_t) * a2b
-            cn = model.compute_cn_smooth(pos_b, edge_index, sh_b)
+            if cfg.get("cnfunc") == "d4" and model.method == "ewald":
+                arg = torch.matmul(model.kvectors, pos_b.T)             # core.py:519-523
+                cn = model.compute_cn_d4(pos_b, torch.stack([torch.cos(arg), torch.sin(arg)], dim=0),
+                                         arg.shape[0])
+            elif cfg.get("cnfunc") == "d4":
+                cn = model.compute_cn_d4(pos_b)
+            else:
+                cn = model.compute_cn_smooth(pos_b, edge_index, sh_b)
             w = model.compute_c6_weights(cn)
             c6 = torch.einsum("nk,nkr->nr", w, model.v_q_reshaped[model.species])
         rec = dict(

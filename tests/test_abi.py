@@ -29,7 +29,9 @@ def test_plan_desc_layout_matches_header():
     # int32 x 12 (n_species..has_cncorr with two int[3]) then doubles and pointers
     d = _native.PlanDesc
     assert d.r_cut.offset == 48 and d.params.offset == 56 and d.rcov.offset == 88
-    assert ctypes.sizeof(d) == 88 + 7 * 8
+    # cnfunc (int32, padded) and the two D4 table pointers follow the original seven pointers
+    assert d.cnfunc.offset == 88 + 7 * 8 and d.rcov_cn.offset == 152 and d.en.offset == 160
+    assert ctypes.sizeof(d) == 168
 
 
 def test_cell_grid_host_geometry():

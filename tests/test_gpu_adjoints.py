@@ -12,7 +12,8 @@ def _energy(m, pos, cell):
     return float(e)
 
 
-@pytest.mark.parametrize("name", ["sio2_648_spme_p5", "hcno_240_spme_p6", "rand_96_pme_p6", "rand_96_ewald_k3_tol1e-2"])
+@pytest.mark.parametrize("name", ["sio2_648_spme_p5", "hcno_240_spme_p6", "rand_96_pme_p6", "rand_96_ewald_k3_tol1e-2",
+                                  "sio2_648_spme_p5_d4", "hcno_240_pme_p6_d4"])
 def test_forces_and_stress_vs_central_differences(name, cuda_device):
     from fourierd3_b200 import D3Model
 

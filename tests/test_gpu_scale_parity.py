@@ -108,6 +108,7 @@ def test_hcno_12000_matches_oracle(precision, cuda_device):
 def test_cn_and_c6_factors_match_reference(name, cuda_device):
     """Coordination numbers and C6 factors of the fused path (cell-list CN kernel, float64 in
     the plain form) and of the edge-list path against the reference's own values."""
+    gc.skip_unbuilt(name)
     from fourierd3_b200 import D3Model, FourierD3, neighbour_list
 
     rec = gc.load(name)

@@ -42,6 +42,7 @@ def parse():
                     help="'reference-gpu': only the reference package's float64 torch path on this GPU "
                          "(the headline run starts it as a child process for the plain_fp64_reference_gpu block)")
     ap.add_argument("--no-reference-gpu", action="store_true")
+    ap.add_argument("--no-batch", action="store_true", help="skip the ragged-batch block of the headline line")
     ap.add_argument("--reps", type=int, default=6)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--precision", default="both", choices=["both", "mixed", "fp64"],
@@ -363,16 +364,14 @@ def run_reference_gpu(args, local):
     print(json.dumps(out), flush=True)
 
 
-def reference_gpu_subprocess(args, local, timeout_s=900):
-    """Runs run_reference_gpu in a child process (its memory is released when it exits, and a
-    failure there cannot end the headline run); returns its JSON record."""
-    cmd = [sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference-gpu", "--reps", str(args.reps),
-           "--steps", str(max(3, min(args.steps, 5))), "--warmup", "1"]
+def child_json(cmd, local, label, timeout_s):
+    """Runs a bench leg in a child process (its memory is released when it exits, and a failure
+    there cannot end the headline run); returns the last JSON line it prints."""
     env = dict(os.environ, LOCAL_RANK=str(local), WORLD_SIZE="1", RANK="0")
     try:
         r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s, env=env)
     except subprocess.TimeoutExpired:
-        return {"impl": "reference-gpu-fp64", "unavailable": f"did not finish within {timeout_s} s"}
+        return {"leg": label, "unavailable": f"did not finish within {timeout_s} s"}
     for line in reversed(r.stdout.splitlines()):
         if line.startswith("{"):
             try:
@@ -380,7 +379,22 @@ def reference_gpu_subprocess(args, local, timeout_s=900):
             except ValueError:
                 break
     tail = (r.stderr or r.stdout).strip().splitlines()[-3:]
-    return {"impl": "reference-gpu-fp64", "unavailable": f"exit {r.returncode}: " + " | ".join(tail)}
+    return {"leg": label, "unavailable": f"exit {r.returncode}: " + " | ".join(tail)}
+
+
+def reference_gpu_subprocess(args, local, timeout_s=900):
+    """run_reference_gpu in a child process; returns its JSON record."""
+    cmd = [sys.executable, os.path.join(REPO, "bench.py"), "--impl", "reference-gpu", "--reps", str(args.reps),
+           "--steps", str(max(3, min(args.steps, 5))), "--warmup", "1"]
+    return child_json(cmd, local, "reference-gpu-fp64", timeout_s)
+
+
+def batch_subprocess(args, local, timeout_s=900):
+    """The ragged-batch workload (256 structures, 32-4,096 atoms, Z 1-54) in a child process, 3
+    timed graph replays after 3 warm-up replays; returns its JSON record (value, ms per batch,
+    heaviest structure's stages, clocks)."""
+    cmd = [sys.executable, os.path.join(REPO, "bench.py"), "--workload", "batch", "--steps", "3", "--warmup", "3"]
+    return child_json(cmd, local, "batch", timeout_s)
 
 
 BATCH_WORKLOAD = "batch256_N32-4096_Z1-54_spme_p5_h1.2_E+F+stress"
@@ -693,9 +707,14 @@ def main():
     # DRAM bytes (read + write) per launch from one ncu capture of each kernel on this
     # 256^3 x 8-channel mixed mesh; mesh-side traffic does not depend on N. When the autotuner
     # chose the fused x-pass, its kernel is the "filter" stage.
-    fused = bool(tuned.get(head, {}).get("fft_x", 0))
-    traffic_by_stage = {"filter": (547.0e6 + 492.3e6) if fused else (541.3e6 + 481.7e6),
-                        "spread": (20.3e6 + 492.5e6)}
+    # DRAM bytes (read + write) per launch from one-kernel ncu captures on this 256^3 x 8-channel mixed
+    # mesh (the mesh-side traffic does not depend on N), for the filter kernel the tuner picked:
+    # 3D-path filter, the cp.async pencil x-pass (fft_x 1) or the TMA x-pass (fft_x 2, 4 q x 4 ranks)
+    fx = int(tuned.get(head, {}).get("fft_x", 0))
+    filter_traffic = {0: 541.3e6 + 481.7e6, 1: 547.0e6 + 492.3e6, 2: 541.2e6 + 488.1e6}[fx]
+    if fx == 2 and (tuned[head].get("xq"), tuned[head].get("xranks")) != (4, 4):
+        filter_traffic = None
+    traffic_by_stage = {"filter": filter_traffic, "spread": (20.3e6 + 492.5e6)}
     mesh_match = tuple(mesh) == (256, 256, 256) and C == 8 and head == "mixed"
     roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
             "unit": "GB/s", "frac": achieved / peak,
@@ -718,6 +737,10 @@ def main():
     ref_gpu = None
     if rank == 0 and ws == 1 and not args.no_reference_gpu:
         ref_gpu = reference_gpu_subprocess(args, local)
+    # the batched form of the metric ("mixed/batched"): the ragged 256-structure batch
+    batch = None
+    if rank == 0 and ws == 1 and not args.no_batch:
+        batch = batch_subprocess(args, local)
 
     ms = res[head]
     line = {
@@ -736,6 +759,7 @@ def main():
                   "note": "the same step launched from the host without graph capture"},
         "mixed_over_fp64": res["fp64"] / ms if "fp64" in res and head == "mixed" else None,
         "plain_fp64_reference_gpu": ref_gpu,
+        "batch": batch,
         "mixed_over_reference_fp64_gpu": (ref_gpu["ms_per_step"] / ms
                                           if ref_gpu and "ms_per_step" in ref_gpu else None),
         "fp64_over_reference_fp64_gpu": (ref_gpu["ms_per_step"] / res["fp64"]

@@ -936,7 +936,9 @@ extern "C" int fd3_energy_forces_stress(fd3_plan* p, int64_t n_atoms, const doub
   Work w;
   FD3_TRY(check_work(p, N, K, d_work, work_bytes, w));
   prof_begin(p, s);
-  FD3_TRY(launch_cellinfo(d_cell_ang, kAngToBohr, w.ci, s));
+  // the cell list below is built from the host cell: a device cell that differs (a captured graph
+  // replayed after a cell change) makes every output NaN instead of silently dropping pairs
+  FD3_TRY(launch_cellinfo(d_cell_ang, kAngToBohr, w.ci, s, p->cnfunc == FD3_CN_D4 ? nullptr : h_cell_ang));
   if (p->cnfunc == FD3_CN_D4) {
     // k-space D4 CN: no neighbour search (calculator.py:171-173)
     int n_self = 0, n_kspc = 0, n_mcell = 0, n_cnv = 0;
@@ -976,6 +978,7 @@ extern "C" int fd3_energy_forces_stress(fd3_plan* p, int64_t n_atoms, const doub
   prof_mark(p, s, "cn_adjoint");
   Partials pa{w.self_part, n_self, w.kspc_part, n_kspc, w.cnv_part, n_cnv, nullptr, 0};
   FD3_TRY(launch_finalize(pa, w.ci, 1, kHartreeToEv, d_energy, d_stress, s));
+  FD3_TRY(launch_poison_if_stale(w.ci, N, d_energy, d_forces, d_stress, s));
   prof_mark(p, s, "finalize");
   return FD3_OK;
 }

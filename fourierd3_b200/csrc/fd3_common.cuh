@@ -23,7 +23,8 @@ struct CellInfo {
   double inv[9];    // adjugate / determinant inverse (utils.py:142-167)
   double recip[9];  // rows b_i = 2 pi inv[:, i]
   double volume;    // |det| (utils.py:130-139)
-  double pad[5];
+  double stale;     // 1: the device cell differs from the host cell the call's geometry came from
+  double pad[4];
 };
 
 // Per species-pair constants of the BJ Green's function (pair_pot.py:63-105).

@@ -133,7 +133,13 @@ struct MeshGeom {
   int xranks;     // TMA x-pass: ranks per unit (1, 2), -1 default
   const float* win_axes;  // SPME, mixed form: sinc(m/n)^(2p) per axis, [nx | ny | nz/2+1] (null: none)
 };
-int launch_cellinfo(const double* cell, double scale, CellInfo* ci, cudaStream_t s);
+// h_expect (optional, host, copied into the launch): the cell the caller's host-side geometry (cell
+// list bins) was built from; a device cell that differs sets ci->stale
+int launch_cellinfo(const double* cell, double scale, CellInfo* ci, cudaStream_t s,
+                    const double* h_expect = nullptr);
+// energy, forces [n*3] and stress [9] made NaN when ci->stale is set
+int launch_poison_if_stale(const CellInfo* ci, int n, double* energy, double* forces, double* stress,
+                           cudaStream_t s);
 int launch_mesh_keys(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
                      const CellInfo* ci, int* keys, cudaStream_t s);
 // Per-atom stencil records in (tile, species)-sorted order, written by the spread launcher and

@@ -17,10 +17,21 @@
 namespace fd3 {
 
 // ------------------------------------------------------------------ cell info
-__global__ void __launch_bounds__(32) k_cellinfo(const double* __restrict__ cell, double scale, CellInfo* __restrict__ ci) {
+struct CellExpect {
+  double c[9];
+  int on;
+};
+
+__global__ void __launch_bounds__(32) k_cellinfo(const double* __restrict__ cell, double scale, CellExpect ex,
+                                                CellInfo* __restrict__ ci) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
   double m[9];
-  for (int k = 0; k < 9; ++k) m[k] = cell[k] * scale;
+  bool stale = false;
+  for (int k = 0; k < 9; ++k) {
+    m[k] = cell[k] * scale;
+    stale |= ex.on && cell[k] != ex.c[k];
+  }
+  ci->stale = stale ? 1.0 : 0.0;
   // utils.py:142-167 (adjugate / determinant) and utils.py:130-139 (cofactor determinant)
   const double c00 = m[4] * m[8] - m[5] * m[7];
   const double c01 = m[2] * m[7] - m[1] * m[8];
@@ -43,8 +54,31 @@ __global__ void __launch_bounds__(32) k_cellinfo(const double* __restrict__ cell
   ci->volume = fabs(det);
 }
 
-int launch_cellinfo(const double* cell, double scale, CellInfo* ci, cudaStream_t s) {
-  k_cellinfo<<<1, 32, 0, s>>>(cell, scale, ci);
+int launch_cellinfo(const double* cell, double scale, CellInfo* ci, cudaStream_t s, const double* h_expect) {
+  CellExpect ex{};
+  ex.on = h_expect != nullptr;
+  if (h_expect)
+    for (int k = 0; k < 9; ++k) ex.c[k] = h_expect[k];
+  k_cellinfo<<<1, 32, 0, s>>>(cell, scale, ex, ci);
+  FD3_LAUNCHED();
+  return FD3_OK;
+}
+
+__global__ void __launch_bounds__(256) k_poison_if_stale(const CellInfo* __restrict__ ci, int n,
+                                                        double* __restrict__ energy, double* __restrict__ forces,
+                                                        double* __restrict__ stress) {
+  if (ci->stale == 0.0) return;
+  const double nan = __longlong_as_double(0x7ff8000000000000LL);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < 3 * n) forces[i] = nan;
+  if (i < 9) stress[i] = nan;
+  if (i == 0) *energy = nan;
+}
+
+int launch_poison_if_stale(const CellInfo* ci, int n, double* energy, double* forces, double* stress,
+                           cudaStream_t s) {
+  const int m = 3 * n > 9 ? 3 * n : 9;
+  k_poison_if_stale<<<(m + 255) / 256, 256, 0, s>>>(ci, n, energy, forces, stress);
   FD3_LAUNCHED();
   return FD3_OK;
 }

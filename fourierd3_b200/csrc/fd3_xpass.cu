@@ -31,7 +31,12 @@ bool xpass_applies(const MeshGeom& mg, int Q, int RG) {
   if (mg.S > 4 || RG > mg.R || (RG != 1 && RG != 2 && RG != 4)) return false;
   if (Q != 4 && Q != 8 && Q != 16 && Q != 32) return false;
   if ((((long long)mg.n[1] * mg.nzh) & 1) != 0) return false;
-  return xpass_stages((size_t)mg.S * RG * mg.n[0] * Q * sizeof(float2)) >= 2;
+  if (mg.n[0] + mg.n[1] + mg.nzh > 1024) return false;   // the per-axis window's shared-memory slot
+  // the x transform as N1 x N2 register DFTs (64: 8 x 8, 128: 8 x 16, 256: 16 x 16) and the
+  // padded working copy of XpWork
+  const int n1 = mg.n[0] == 64 ? 8 : mg.n[0] == 128 ? 8 : 16, n2 = mg.n[0] / n1;
+  const size_t work = (size_t)mg.S * RG * n1 * (n2 * Q + (Q < 16 ? Q : 0)) * sizeof(float2);
+  return xpass_stages((size_t)mg.S * RG * mg.n[0] * Q * sizeof(float2), work) >= 2;
 }
 
 // Spectrum (float2, layout (S, R, nx, ny, nz/2+1)) as a 4-D float tensor

@@ -15,7 +15,8 @@
 //
 // One CTA per SM: a producer warp keeps a ring of `nstage` unit buffers full (mbarrier
 // complete_tx), issues the TMA store of each finished unit, and reuses its buffer for the unit
-// `nstage` ahead once the store has read it; 8 compute warps run the two register-DFT passes,
+// `nstage` ahead once the store has read it; 16 compute warps (96 registers each, one item per
+// loop trip) run the two register-DFT passes,
 // the filter and the two inverse passes on each buffer. Every mbarrier wait is bounded; a wait
 // that runs out marks the block's energy partial NaN and ends the block.
 #pragma once
@@ -25,10 +26,10 @@
 
 namespace fd3 {
 
-constexpr int kXpCompute = 256;          // compute threads (8 warps); the producer warp follows
+constexpr int kXpCompute = 512;          // compute threads (16 warps); the producer warp follows
 constexpr int kXpThreads = kXpCompute + 32;
 constexpr int kXpMaxStages = 4;
-constexpr int kXpTwBytes = 4096;         // twiddle table (at most 16 x 17 float2), rounded up
+constexpr int kXpTwBytes = 8192;         // twiddles (at most 16 x 17 float2) + per-axis SPME window
 constexpr int kXpAlignPad = 1024;        // room to align the unit buffers (dynamic shared memory)
 constexpr long long kXpWaitCycles = 4000000000LL;   // about two seconds at B200 clocks
 
@@ -90,7 +91,7 @@ __device__ __forceinline__ void compute_bar() {
 template <int MAXS, int RG>
 __device__ __forceinline__ void filter_group(const KPoint<float>& q, int S, int R, int r0,
                                              const GreenPairF* __restrict__ gp, const float4* __restrict__ gtab,
-                                             float inv_h, float s6, float s8, const Tables* __restrict__ tab,
+                                             float inv_h, float s6, float s8, const float (&lam)[RG],
                                              float2* v, int cs, double* acc) {
   float G[MAXS][MAXS], dG[MAXS][MAXS], Gh[MAXS][MAXS];
   green_block<float, MAXS>(q, S, gp, gtab, inv_h, s6, s8, G, dG, Gh);
@@ -116,9 +117,8 @@ __device__ __forceinline__ void filter_group(const KPoint<float>& q, int S, int 
         }
         if (full || X < S) v[(X * RG + r) * cs] = float2{hre, him};
       }
-      const float lam = (float)tab->eigs[r0 + r];
-      qq += lam * qr;
-      dq += lam * dqr;
+      qq += lam[r] * qr;
+      dq += lam[r] * dqr;
     }
   }
   acc[0] += (double)(q.wk * qq);
@@ -126,51 +126,73 @@ __device__ __forceinline__ void filter_group(const KPoint<float>& q, int S, int 
 }
 
 // ------------------------------------------------------------------ register-DFT passes
-// Unit buffer: channel ch (0 .. Cg-1), x slot, q offset (0 .. Q-1): buf[(ch NX + x) Q + qq].
+// Two layouts of a unit's values (channel ch < Cg, x slot, q offset qq < Q):
+//  * dense, as the TMA box lands: buf[(ch NX + x) Q + qq];
+//  * padded working copy: wk[ch CS + (x >> log2 N2) GS + (x mod N2) Q + qq], GS = N2 Q + PADG.
+// The forward pass 1 reads the dense unit and writes the working copy, the inverse pass 1 reads the
+// working copy and writes the dense unit back for the TMA store; pass 2 and the filter stay in the
+// working copy. Pass 2 walks the N2 slots of one k1 group, and with Q < 16 the lanes of a warp span
+// several k1 groups: a group stride of N2 Q values (a multiple of 128 bytes) would put them on the
+// same banks, so each group carries PADG = Q padding values.
 // Forward: natural x order in, slot N2 k1 + k2 holding ix = k1 + N1 k2 out. Inverse: reverse.
 template <int N1, int N2, int Q>
-__device__ __forceinline__ void xp_pass_n1(float2* buf, const float2* tw, int Cg, bool inverse) {
+struct XpWork {
+  static constexpr int PADG = Q < 16 ? Q : 0;
+  static constexpr int GS = N2 * Q + PADG;   // values per k1 group
+  static constexpr int CS = N1 * GS;         // values per channel
+  static constexpr int LN2 = log2_n<N2>();
+  __host__ __device__ static constexpr size_t bytes(int Cg) { return (size_t)Cg * CS * sizeof(float2); }
+  __device__ static int off(int ch, int x, int qq) { return ch * CS + (x >> LN2) * GS + (x & (N2 - 1)) * Q + qq; }
+};
+
+template <int N1, int N2, int Q>
+__device__ __forceinline__ void xp_pass_n1(float2* buf, float2* wk, const float2* tw, int Cg, bool inverse) {
+  using W = XpWork<N1, N2, Q>;
   constexpr int NX = N1 * N2, LQ = log2_n<Q>(), LN2 = log2_n<N2>();
   const int items = (Cg * N2) << LQ;
+#pragma unroll 1
   for (int it = threadIdx.x; it < items; it += kXpCompute) {
     const int qq = it & (Q - 1), n2 = (it >> LQ) & (N2 - 1), ch = it >> (LQ + LN2);
-    float2* b = buf + ((size_t)ch * NX + n2) * Q + qq;
+    float2* d = buf + ((size_t)ch * NX + n2) * Q + qq;      // dense: x = N2 n1 + n2 at d[n1 N2 Q]
+    float2* w = wk + ch * W::CS + n2 * Q + qq;             // working: slot N2 k1 + n2 at w[k1 GS]
     float re[N1], im[N1];
     if (!inverse) {
 #pragma unroll
       for (int n1 = 0; n1 < N1; ++n1) {
-        const float2 v = b[n1 * N2 * Q];
+        const float2 v = d[n1 * N2 * Q];
         re[n1] = v.x;
         im[n1] = v.y;
       }
       dft_reg<float, N1, -1>(re, im);
 #pragma unroll
       for (int k1 = 0; k1 < N1; ++k1) {
-        const float2 w = tw[n2 * (N1 + 1) + k1];   // exp(-2 pi i n2 k1 / NX)
-        b[k1 * N2 * Q] = float2{re[k1] * w.x - im[k1] * w.y, re[k1] * w.y + im[k1] * w.x};
+        const float2 t = tw[n2 * (N1 + 1) + k1];   // exp(-2 pi i n2 k1 / NX)
+        w[k1 * W::GS] = float2{re[k1] * t.x - im[k1] * t.y, re[k1] * t.y + im[k1] * t.x};
       }
     } else {
 #pragma unroll
       for (int k1 = 0; k1 < N1; ++k1) {
-        const float2 v = b[k1 * N2 * Q];
-        const float2 w = tw[n2 * (N1 + 1) + k1];   // conj: exp(+2 pi i n2 k1 / NX)
-        re[k1] = v.x * w.x + v.y * w.y;
-        im[k1] = v.y * w.x - v.x * w.y;
+        const float2 v = w[k1 * W::GS];
+        const float2 t = tw[n2 * (N1 + 1) + k1];   // conj: exp(+2 pi i n2 k1 / NX)
+        re[k1] = v.x * t.x + v.y * t.y;
+        im[k1] = v.y * t.x - v.x * t.y;
       }
       dft_reg<float, N1, 1>(re, im);
 #pragma unroll
-      for (int n1 = 0; n1 < N1; ++n1) b[n1 * N2 * Q] = float2{re[n1], im[n1]};
+      for (int n1 = 0; n1 < N1; ++n1) d[n1 * N2 * Q] = float2{re[n1], im[n1]};
     }
   }
 }
 
 template <int N1, int N2, int Q>
-__device__ __forceinline__ void xp_pass_n2(float2* buf, int Cg, bool inverse) {
-  constexpr int NX = N1 * N2, LQ = log2_n<Q>(), LN1 = log2_n<N1>();
+__device__ __forceinline__ void xp_pass_n2(float2* wk, int Cg, bool inverse) {
+  using W = XpWork<N1, N2, Q>;
+  constexpr int LQ = log2_n<Q>(), LN1 = log2_n<N1>();
   const int items = (Cg * N1) << LQ;
+#pragma unroll 1
   for (int it = threadIdx.x; it < items; it += kXpCompute) {
     const int qq = it & (Q - 1), k1 = (it >> LQ) & (N1 - 1), ch = it >> (LQ + LN1);
-    float2* b = buf + ((size_t)ch * NX + k1 * N2) * Q + qq;
+    float2* b = wk + ch * W::CS + k1 * W::GS + qq;
     float re[N2], im[N2];
 #pragma unroll
     for (int n2 = 0; n2 < N2; ++n2) {
@@ -205,6 +227,8 @@ __global__ void __launch_bounds__(kXpThreads, 1)
   float2* bufs = reinterpret_cast<float2*>(xp_base + kXpTwBytes);
   const int S = g.S, R = g.R, Cg = S * RG;
   const int buf_elems = (Cg * NX) << LQ;
+  using W = XpWork<N1, N2, Q>;
+  float2* wk = bufs + (size_t)nstage * buf_elems;   // padded working copy of the unit in flight
   const uint32_t buf_bytes = (uint32_t)buf_elems * 8u;
   const int tid = threadIdx.x;
   if (tid == 0) {
@@ -216,6 +240,11 @@ __global__ void __launch_bounds__(kXpThreads, 1)
     prod_fail = 0;
     mbar_fence_init();
   }
+  // the mixed form's per-axis SPME window (nx + ny + nz/2+1 floats), read per k-point, in shared memory
+  float* s_win = reinterpret_cast<float*>(xp_base + kXpTwBytes / 2);
+  const int nwin = g.n[0] + g.n[1] + g.nzh;
+  if (g.win_axes)
+    for (int m = tid; m < nwin; m += blockDim.x) s_win[m] = g.win_axes[m];
   for (int m = tid; m < N2 * (N1 + 1); m += blockDim.x) {
     const int a = m / (N1 + 1), b = m % (N1 + 1);
     double sn, cs;
@@ -261,9 +290,10 @@ __global__ void __launch_bounds__(kXpThreads, 1)
     float rc[9];
     load_recip<float>(ci, rc);
     const float inv_h = green_inv_h(g, ci);
+    MeshDev gs = g;
+    if (g.win_axes) gs.win_axes = s_win;
     const int n1 = g.n[1], nzh = g.nzh;
     const int nq = n1 * nzh;
-    const int cs = NX << LQ;   // channel stride of the unit buffer
     for (int k = 0;; ++k) {
       const int u = blockIdx.x + k * gridDim.x;
       if (u >= nunits) break;
@@ -274,10 +304,14 @@ __global__ void __launch_bounds__(kXpThreads, 1)
       if (*(volatile int*)&xp_fail) break;
       float2* buf = bufs + (size_t)s * buf_elems;
       const int grp = u / nqb, qb = u - grp * nqb;
-      xp_pass_n1<N1, N2, Q>(buf, tw, Cg, false);
+      xp_pass_n1<N1, N2, Q>(buf, wk, tw, Cg, false);
       compute_bar();
-      xp_pass_n2<N1, N2, Q>(buf, Cg, false);
+      xp_pass_n2<N1, N2, Q>(wk, Cg, false);
       compute_bar();
+      float lam[RG];   // lambda of the unit's ranks (padding ranks: 0, never used)
+#pragma unroll
+      for (int r = 0; r < RG; ++r) lam[r] = grp * RG + r < R ? (float)tab->eigs[grp * RG + r] : 0.f;
+#pragma unroll 1
       for (int pt = tid; pt < (NX << LQ); pt += kXpCompute) {
         const int qq = pt & (Q - 1), slot = pt >> LQ;
         const int qf = qb * Q + qq;
@@ -286,13 +320,14 @@ __global__ void __launch_bounds__(kXpThreads, 1)
         const int iz = qf - y * nzh;
         const int ix = (slot >> LN2) + N1 * (slot & (N2 - 1));
         const size_t kflat = ((size_t)ix * n1 + y) * nzh + iz;
-        const KPoint<float> q = kpoint_idx<float>(g, ix, y, iz, kflat, rc, deconv, spme, P);
-        filter_group<MAXS, RG>(q, S, R, grp * RG, gp, gtab, inv_h, s6, s8, tab, buf + pt, cs, acc);
+        const KPoint<float> q = kpoint_idx<float>(gs, ix, y, iz, kflat, rc, deconv, spme, P);
+        filter_group<MAXS, RG>(q, S, R, grp * RG, gp, gtab, inv_h, s6, s8, lam, wk + W::off(0, slot, qq), W::CS,
+                               acc);
       }
       compute_bar();
-      xp_pass_n2<N1, N2, Q>(buf, Cg, true);
+      xp_pass_n2<N1, N2, Q>(wk, Cg, true);
       compute_bar();
-      xp_pass_n1<N1, N2, Q>(buf, tw, Cg, true);
+      xp_pass_n1<N1, N2, Q>(buf, wk, tw, Cg, true);
       fence_proxy_async_smem();
       mbar_arrive(&done_bar[s]);
     }

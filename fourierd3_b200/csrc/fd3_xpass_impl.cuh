@@ -8,9 +8,12 @@ namespace fd3 {
 // kernel's static shared memory).
 constexpr size_t kXpSmemCap = 220 * 1024;
 
-// Ring stages that fit for a unit of the given size, at most kXpMaxStages (0: fewer than 2 fit).
-inline int xpass_stages(size_t unit_bytes) {
-  const size_t n = (kXpSmemCap - kXpAlignPad - kXpTwBytes) / unit_bytes;
+// Ring stages that fit for a unit of the given size beside its padded working copy, at most
+// kXpMaxStages (0: fewer than 2 fit).
+inline int xpass_stages(size_t unit_bytes, size_t work_bytes) {
+  const size_t fixed = kXpAlignPad + kXpTwBytes + work_bytes;
+  if (fixed >= kXpSmemCap) return 0;
+  const size_t n = (kXpSmemCap - fixed) / unit_bytes;
   if (n < 2) return 0;
   return n > (size_t)kXpMaxStages ? kXpMaxStages : (int)n;
 }
@@ -35,12 +38,13 @@ int launch_xpass_t(const XpassArgs& a) {
   constexpr int NX = N1 * N2;
   const MeshGeom& mg = a.mg;
   const size_t unit = (size_t)mg.S * RG * NX * Q * sizeof(float2);
-  const int nstage = xpass_stages(unit);
+  const size_t work = XpWork<N1, N2, Q>::bytes(mg.S * RG);
+  const int nstage = xpass_stages(unit, work);
   if (nstage < 2) {
     set_error("filter", "fused x-pass unit does not fit twice in shared memory");
     return FD3_EINVAL;
   }
-  const size_t smem = kXpAlignPad + kXpTwBytes + (size_t)nstage * unit;
+  const size_t smem = kXpAlignPad + kXpTwBytes + (size_t)nstage * unit + work;
   static bool attr = false;
   if (!attr) {
     if (cudaFuncSetAttribute(k_xpass<N1, N2, Q, RG, MAXS>, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -163,6 +163,22 @@ def test_module_edges_out_of_range_index_gives_nan(cuda_device):
     assert abs(float(e_ok) * 27.21138505 - float(rec["energy_ev"])) <= E_REL * abs(float(rec["energy_ev"]))
 
 
+def test_fused_stale_cell_gives_nan(cuda_device):
+    """The fused path builds its cell list from the host cell. A device cell that differs (as
+    when a captured graph is replayed after the cell changed) makes every output NaN; the same
+    call with matching cells is finite and matches the reference."""
+    from fourierd3_b200 import D3Model
+
+    rec = gc.load("sio2_648_spme_p5")
+    m = D3Model(rec["numbers"], rec["cell"], precision="fp64", device=cuda_device, **gc.model_kwargs(rec["config"]))
+    pos = torch.tensor(rec["positions"], dtype=torch.float64, device=cuda_device)
+    moved = torch.tensor(rec["cell"] * 1.001, dtype=torch.float64, device=cuda_device)
+    e, f, s = m.engine.energy_forces_stress(pos, rec["cell"], 6.0, cell_dev=moved)
+    assert torch.isnan(e).item() and torch.isnan(f).all().item() and torch.isnan(s).all().item()
+    e, f, s = m.engine.energy_forces_stress(pos, rec["cell"], 6.0)
+    assert abs(float(e) - float(rec["energy_ev"])) <= E_REL * abs(float(rec["energy_ev"]))
+
+
 def test_fused_dense_box_uses_fallback_paths(cuda_device):
     """A dense light-element box overflows the shared-memory bin stage (and records), so the
     CN and its adjoint take the global-memory traversals; results must still match the oracle."""

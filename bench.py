@@ -217,17 +217,39 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def stage_bytes(stage: str, n: int, mesh, C: int, R: int, b: int) -> float:
+def touched_mesh_values(pos, cell, numbers, mesh, order: int, R: int) -> int:
+    """Mesh values (species plane points x R ranks) that some atom's p^3 stencil reaches: what the
+    gather must read at least once (SPME stencil centring: round for odd p, floor for even p)."""
+    n = np.asarray(mesh)
+    u = (np.asarray(pos) @ np.linalg.inv(np.asarray(cell))) * n
+    ref = np.round(u).astype(np.int64) if order % 2 else np.floor(u).astype(np.int64)
+    offs = np.arange(order) - (order // 2 if order % 2 else order // 2 - 1)
+    total = 0
+    z = np.asarray(numbers)
+    for sp in np.unique(z):
+        r = ref[z == sp]
+        X = (r[:, 0, None] + offs) % n[0]
+        Y = (r[:, 1, None] + offs) % n[1]
+        Z = (r[:, 2, None] + offs) % n[2]
+        lin = (X[:, :, None, None] * (n[1] * n[2]) + Y[:, None, :, None] * n[2] + Z[:, None, None, :]).reshape(-1)
+        total += np.unique(lin).size
+    return int(total) * R
+
+
+def stage_bytes(stage: str, n: int, mesh, C: int, R: int, b: int, touched: int = 0) -> float:
     """Algorithmic HBM bytes of one launch of a pipeline stage: mesh terms per mesh point and
-    channel (b bytes real, 2b complex), atom terms per atom."""
+    channel (b bytes real, 2b complex), atom terms per atom. The gather reads only the mesh
+    values the atoms' stencils reach (``touched``, when given)."""
     M = mesh[0] * mesh[1] * mesh[2]
     Mh = mesh[0] * mesh[1] * (mesh[2] // 2 + 1)
     if stage == "spread":
         return C * M * b + n * (24 + 4 + 8 * R)
     if stage == "filter":
-        return 2 * C * Mh * 2 * b + Mh * 4
+        # float64: the float32 SPME window table is read per k-point; the mixed form multiplies
+        # three per-axis factors (L1-resident) instead
+        return 2 * C * Mh * 2 * b + (Mh * 4 if b == 8 else 0)
     if stage == "gather":
-        return C * M * b + n * (24 + 4 + 16 * R + 8 + 24)
+        return (touched if touched else C * M) * b + n * (24 + 4 + 16 * R + 8 + 24)
     if stage in ("fft_r2c", "fft_c2r"):
         return C * M * b + C * Mh * 2 * b
     if stage == "cn_c6":
@@ -702,11 +724,16 @@ def main():
     ours = {k: v for k, v in st_mixed.items() if not k.startswith("fft")}
     dom = max(ours, key=ours.get)
     peak, peak_kind = measured_peaks()
-    dom_bytes = stage_bytes(dom, n, mesh, C, R, b)
+    touched = touched_mesh_values(pos, cell, nums, mesh, 5, R)
+    dom_bytes = stage_bytes(dom, n, mesh, C, R, b, touched)
     achieved = dom_bytes / (ours[dom] * 1e-3) / 1e9
-    # DRAM bytes (read + write) per launch from one ncu capture of each kernel on this
-    # 256^3 x 8-channel mixed mesh; mesh-side traffic does not depend on N. When the autotuner
-    # chose the fused x-pass, its kernel is the "filter" stage.
+    # every own stage against the same peak (algorithmic bytes / CUDA-event stage time)
+    stage_roof = {}
+    for k, ms in ours.items():
+        by = stage_bytes(k, n, mesh, C, R, b, touched)
+        if by > 0 and ms > 0:
+            stage_roof[k] = {"bytes": by, "ms": ms, "gbs": by / (ms * 1e-3) / 1e9,
+                             "frac": by / (ms * 1e-3) / 1e9 / peak}
     # DRAM bytes (read + write) per launch from one-kernel ncu captures on this 256^3 x 8-channel mixed
     # mesh (the mesh-side traffic does not depend on N), for the filter kernel the tuner picked:
     # 3D-path filter, the cp.async pencil x-pass (fft_x 1) or the TMA x-pass (fft_x 2, 4 q x 4 ranks)
@@ -721,7 +748,7 @@ def main():
             "traffic": traffic_by_stage.get(dom) if mesh_match else None,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, 256^3 x 8 channels, mixed"
                               if mesh_match and dom in traffic_by_stage else None,
-            "bytes_per_launch": dom_bytes, "ms_per_launch": ours[dom]}
+            "bytes_per_launch": dom_bytes, "ms_per_launch": ours[dom], "stages": stage_roof}
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1

@@ -296,12 +296,14 @@ def _profiled_stage(batch: "D3Batch", i: int, stage, reps: int = 2) -> float:
     raise KeyError(i)
 
 
-def autotune_filter(batch: "D3Batch", candidates: Sequence[int] = (0, 1, 2, 4, 8, 16), reps: int = 2) -> dict:
-    """Pick the filter k-tile per species-count class from the heaviest structure of each class.
+def autotune_filter(batch: "D3Batch", candidates: Sequence = (0, 1, 2, 4, 8, 16, "tc"), reps: int = 2) -> dict:
+    """Pick the filter per species-count class from the heaviest structure of each class: a
+    CUDA-core k-tile width (0 = per-thread register kernel) or "tc" (mixed precision: the
+    tensor-core filter, where it applies).
 
     Classes: up to 8 species, 9-24, 25-64. Each class is timed on its heaviest structure
-    (profiled eager calls) and its best tile is set on every engine of that class where it
-    is valid. Returns {class: (tile, {tile: ms})}. Drops a captured graph.
+    (profiled eager calls) and its best choice is set on every engine of that class where it
+    is valid. Returns {class: (choice, {choice: ms})}. Drops a captured graph.
     """
     batch._graph = None
     classes: dict = {}
@@ -310,24 +312,29 @@ def autotune_filter(batch: "D3Batch", candidates: Sequence[int] = (0, 1, 2, 4, 8
         c = 0 if s <= 8 else (1 if s <= 24 else 2)
         if c not in classes or batch.costs[i] > batch.costs[classes[c]]:
             classes[c] = i
+
+    def apply(e, choice) -> bool:
+        try:
+            if choice == "tc":
+                e.set_tuning(filter_kt=-1, filter_mma=1)
+                return e.tuning()["filter_mma"] == 1
+            e.set_tuning(filter_mma=0, filter_kt=choice)
+            return True
+        except ValueError:
+            return False
+
     out = {}
     for c, i in sorted(classes.items()):
         eng = batch._engines[batch._keys[i]]
         times = {}
-        for kt in candidates:
-            try:
-                eng.set_tuning(filter_kt=kt)
-            except ValueError:
-                continue
-            times[kt] = _profiled_stage(batch, i, "filter", reps)
+        for choice in candidates:
+            if apply(eng, choice):
+                times[choice] = _profiled_stage(batch, i, "filter", reps)
         best = min(times, key=times.get)
         for key, e in batch._engines.items():
             s = len(key[0])
-            if (0 if s <= 8 else (1 if s <= 24 else 2)) == c:
-                try:
-                    e.set_tuning(filter_kt=best)
-                except ValueError:
-                    e.set_tuning(filter_kt=-1)
+            if (0 if s <= 8 else (1 if s <= 24 else 2)) == c and not apply(e, best):
+                e.set_tuning(filter_kt=-1, filter_mma=-1)
         out[c] = (best, times)
     return out
 

@@ -223,6 +223,7 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
       m.xpencil = -1;
       m.xq = -1;
       m.xranks = -1;
+      m.filter_mma = -1;
       m.fft_x = -1;   // default: off (3D cuFFT around the separate filter measured faster on B200)
       const size_t Mh = (size_t)m.n[0] * m.n[1] * m.nzh;
       m.win_axes = nullptr;
@@ -431,6 +432,14 @@ extern "C" int fd3_plan_set_tuning(fd3_plan* p, int32_t knob, int32_t value) {
     p->mg.xranks = value;
     return FD3_OK;
   }
+  if (knob == FD3_TUNE_FILTER_MMA) {
+    if (value < -1 || value > 1) {
+      set_error("fd3_plan_set_tuning", "tensor-core filter must be -1 (default), 0 (CUDA cores) or 1");
+      return FD3_EINVAL;
+    }
+    p->mg.filter_mma = value;
+    return FD3_OK;
+  }
   if (knob == FD3_TUNE_XPENCIL) {
     if (value != -1 && value != 1 && value != 2 && value != 4) {
       set_error("fd3_plan_set_tuning", "fused x-pass pencil must be -1 (default), 1, 2 or 4 kz values");
@@ -478,6 +487,13 @@ extern "C" int fd3_plan_get_tuning(const fd3_plan* p, int32_t knob, int32_t* val
     xpass_shape(p, &Q, &RG);
     const bool ok = p->has_fft2 && p->precision == FD3_PREC_MIXED && xpass_applies(p->mg, Q, RG);
     *value = ok ? (knob == FD3_TUNE_XQ ? Q : RG) : 0;
+    return FD3_OK;
+  }
+  if (knob == FD3_TUNE_FILTER_MMA) {
+    *value = p->method != FD3_METHOD_EWALD && p->precision == FD3_PREC_MIXED && !xpass_on(p) && !old_xpass_on(p) &&
+                     filter_mma_on(p->mg)
+                 ? 1
+                 : 0;
     return FD3_OK;
   }
   if (knob == FD3_TUNE_XPENCIL) {

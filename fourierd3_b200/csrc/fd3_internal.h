@@ -129,8 +129,9 @@ struct MeshGeom {
   int spread_cap; // staged atoms per column chunk at most (0: as many as shared memory holds)
   int fft_x;      // fused x-pass (2D cuFFT + x FFT/filter kernel): 1 on, 0 off, -1 default
   int xpencil;    // kz values per pencil of the fused x-pass (1, 2, 4), -1 default
-  int xq;         // TMA x-pass: q values per unit (8, 16, 32), -1 default
-  int xranks;     // TMA x-pass: ranks per unit (1, 2), -1 default
+  int xq;         // TMA x-pass: q values per unit (4, 8, 16, 32), -1 default
+  int xranks;     // TMA x-pass: ranks per unit (1, 2, 4), -1 default
+  int filter_mma; // float spectrum: 1 tensor-core (tcgen05) filter where it applies, 0 CUDA cores, -1 default
   const float* win_axes;  // SPME, mixed form: sinc(m/n)^(2p) per axis, [nx | ny | nz/2+1] (null: none)
 };
 // h_expect (optional, host, copied into the launch): the cell the caller's host-side geometry (cell
@@ -170,6 +171,11 @@ bool xpass_applies(const MeshGeom& mg, int Q, int RG);
 int launch_xpass(const MeshGeom& mg, int Q, int RG, const CellInfo* ci, const GreenPairF* gpf, const float4* gtab,
                  const Tables* tab, const float* deconv, int spme, void* spec, double* part, int* n_blocks,
                  cudaStream_t s);
+// tensor-core filter (float spectrum, tcgen05 kind::tf32, at most 64 species and 8 ranks)
+bool filter_mma_applies(const MeshGeom& mg);
+bool filter_mma_on(const MeshGeom& mg);
+int launch_filter_mma(const MeshGeom& mg, const CellInfo* ci, const float4* gtab, const Tables* tab,
+                      const float* deconv, int spme, void* spec, double* part, int* n_blocks, cudaStream_t s);
 // mixed form: per-call table of G and its k-derivatives per species pair (gtab of the filter)
 int launch_green_table(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab, void* table,
                        cudaStream_t s);

@@ -518,6 +518,8 @@ int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, c
   const size_t Mh = (size_t)mg.n[0] * mg.n[1] * mg.nzh;
   const MeshDev g = to_dev(mg);
   C2* sp = reinterpret_cast<C2*>(spec);
+  if (sizeof(T) == 4 && filter_mma_on(mg))
+    return launch_filter_mma(mg, ci, gtab, tab, deconv, spme, spec, part, n_blocks, s);
   const int kt = mg.filter_kt >= 0 ? mg.filter_kt : filter_default_kt(mg.S, mg.R, sizeof(T));
   if (kt == 0 && mg.S <= 8) {
     const int blocks = filter_grid(Mh);

@@ -187,21 +187,24 @@ class Engine:
 
     _KNOBS = {"filter_kt": _native.TUNE_FILTER_KT, "spread_zc": _native.TUNE_SPREAD_ZC,
               "spread_cap": _native.TUNE_SPREAD_CAP, "fft_x": _native.TUNE_FFT_X,
-              "xpencil": _native.TUNE_XPENCIL, "xq": _native.TUNE_XQ, "xranks": _native.TUNE_XRANKS}
+              "xpencil": _native.TUNE_XPENCIL, "xq": _native.TUNE_XQ, "xranks": _native.TUNE_XRANKS,
+              "filter_mma": _native.TUNE_FILTER_MMA}
 
     def set_tuning(self, filter_kt: Optional[int] = None, spread_zc: Optional[int] = None,
                    spread_cap: Optional[int] = None, fft_x: Optional[int] = None,
                    xpencil: Optional[int] = None, xq: Optional[int] = None,
-                   xranks: Optional[int] = None) -> None:
+                   xranks: Optional[int] = None, filter_mma: Optional[int] = None) -> None:
         """Launch-shape knobs (results agree to rounding): ``filter_kt`` = k-points per filter
         tile, ``spread_zc`` = z-tiles per column chunk of the spread, ``spread_cap`` = staged
         atoms per chunk at most, ``fft_x`` = 0 (3D cuFFT around the filter), 1 (2D cuFFT and the
         x FFT / filter / inverse x FFT in one kernel, pencils of ``xpencil`` = 1, 2 or 4 kz values
-        of every channel) or 2 (the same with TMA-moved units of ``xq`` = 8, 16 or 32 flattened
-        (y, kz) values of ``xranks`` = 1 or 2 ranks, mixed precision); -1 (0 for the cap)
-        restores a default."""
+        of every channel) or 2 (the same with TMA-moved units of ``xq`` = 4, 8, 16 or 32
+        flattened (y, kz) values of ``xranks`` = 1, 2 or 4 ranks, mixed precision),
+        ``filter_mma`` = 1 (mixed precision: the per-k-point species products of the separate
+        filter on the tensor cores) or 0 (CUDA cores); -1 (0 for the cap) restores a default."""
         for name, val in (("filter_kt", filter_kt), ("spread_zc", spread_zc), ("spread_cap", spread_cap),
-                          ("fft_x", fft_x), ("xpencil", xpencil), ("xq", xq), ("xranks", xranks)):
+                          ("fft_x", fft_x), ("xpencil", xpencil), ("xq", xq), ("xranks", xranks),
+                          ("filter_mma", filter_mma)):
             if val is not None:
                 _native.check(_native.lib().fd3_plan_set_tuning(self._plan, self._KNOBS[name], int(val)),
                               "fd3_plan_set_tuning")

@@ -98,13 +98,21 @@ FD3_API int fd3_plan_destroy(fd3_plan* plan);
  *                       staging path inside the same CTA).
  *   FD3_TUNE_FFT_X      1 = cuFFT transforms the (y, z) planes and one kernel does the x
  *                       transform, the filter and the inverse x transform per pencil (where
- *                       it applies: at most 4 species and 8 ranks, nx = 64, 128 or 256); 0 =
+ *                       it applies: at most 4 species and 8 ranks, nx = 64, 128 or 256); 2 =
+ *                       the same with units of rank groups moved by TMA (mixed precision); 0 =
  *                       3D cuFFT around a separate filter; -1 = the default (0). Which is
- *                       faster depends on the mesh and precision: time both.
+ *                       faster depends on the mesh and precision: time them.
  *   FD3_TUNE_XPENCIL    kz values per pencil of the fused x-pass: 1, 2 or 4 (used when the
  *                       pencil fits in shared memory), -1 = the default (the widest that
  *                       leaves three CTAs per SM for float, within 100 KB for double);
  *                       the value in effect is 0 where the fused x-pass does not apply.
+ *   FD3_TUNE_XQ         TMA x-pass (FD3_TUNE_FFT_X = 2, mixed precision): flattened (y, kz)
+ *                       values per unit, 4, 8, 16 or 32; -1 = the default (16).
+ *   FD3_TUNE_XRANKS     TMA x-pass: ranks per unit, 1, 2 or 4; -1 = the default (1).
+ *   FD3_TUNE_FILTER_MMA mixed precision, separate filter: 1 = the per-k-point S x S products
+ *                       on the tensor cores (tcgen05.mma kind::tf32, operands split into tf32
+ *                       high and low parts; at most 64 species and 8 ranks, as shared memory
+ *                       allows), 0 or -1 = CUDA cores (the default).
  * fd3_plan_get_tuning returns the value in effect (the default resolved). */
 #define FD3_TUNE_FILTER_KT 0
 #define FD3_TUNE_SPREAD_ZC 1
@@ -113,6 +121,7 @@ FD3_API int fd3_plan_destroy(fd3_plan* plan);
 #define FD3_TUNE_XPENCIL 4
 #define FD3_TUNE_XQ 5
 #define FD3_TUNE_XRANKS 6
+#define FD3_TUNE_FILTER_MMA 7
 FD3_API int fd3_plan_set_tuning(fd3_plan* plan, int32_t knob, int32_t value);
 FD3_API int fd3_plan_get_tuning(const fd3_plan* plan, int32_t knob, int32_t* value);
 

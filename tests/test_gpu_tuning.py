@@ -203,3 +203,43 @@ def test_autotune_fft_x_picks_a_timed_path(cuda_device):
     assert any(k.startswith("2/") for k in fused[0])
     e = b()[0]
     assert torch.allclose(e, e0, rtol=2e-6, atol=0.0)
+
+
+@pytest.mark.parametrize("z_max,n,seed", [(54, 300, 61), (43, 200, 62), (12, 160, 63), (6, 120, 64)])
+def test_tensor_core_filter_agrees(z_max, n, seed, cuda_device):
+    """Mixed form: the tcgen05 filter (tf32 high/low split, three products per k-point) against
+    the CUDA-core filter on the same plan -- energy 2e-6 relative, forces and stress 1e-5 --
+    for 6 to 54 species (ranks 3 to 8, so padded columns of the 16-wide product as well)."""
+    from fourierd3_b200 import D3Model, structures as st
+
+    pos, cell, z = st.random_box(seed, n, z_max=z_max, angles=(75.0, 105.0))
+    m = D3Model(z, cell, precision="mixed", device=cuda_device, **KW)
+    m.engine.set_tuning(filter_mma=0)
+    assert m.engine.tuning()["filter_mma"] == 0
+    e0, f0, s0 = (t.clone() for t in m(pos, cell))
+    m.engine.set_tuning(filter_mma=1)
+    assert m.engine.tuning()["filter_mma"] == 1
+    e, f, s = m(pos, cell)
+    assert torch.isfinite(e).item()
+    assert abs(float(e) - float(e0)) <= 2e-6 * abs(float(e0)), (float(e), float(e0))
+    assert (f - f0).abs().max().item() <= 1e-5
+    assert (s - s0).abs().max().item() <= 1e-5
+    e2, f2, s2 = m(pos, cell)                 # repeat: bitwise equal
+    assert float(e2) == float(e) and torch.equal(f2, f) and torch.equal(s2, s)
+
+
+def test_tensor_core_filter_default_and_bounds(cuda_device):
+    """Default: CUDA cores; the tensor-core filter is in effect only where asked for and where it
+    applies (mixed precision, at most 64 species and 8 ranks); out-of-range values are rejected."""
+    from fourierd3_b200 import D3Model, structures as st
+
+    pos, cell, z = st.random_box(65, 120, z_max=20)
+    m = D3Model(z, cell, precision="mixed", device=cuda_device, **KW)
+    assert m.engine.tuning()["filter_mma"] == 0
+    m.engine.set_tuning(filter_mma=1)
+    assert m.engine.tuning()["filter_mma"] == 1
+    with pytest.raises(ValueError):
+        m.engine.set_tuning(filter_mma=2)
+    m64 = D3Model(z, cell, precision="fp64", device=cuda_device, **KW)
+    m64.engine.set_tuning(filter_mma=1)
+    assert m64.engine.tuning()["filter_mma"] == 0          # float64 stays on CUDA cores

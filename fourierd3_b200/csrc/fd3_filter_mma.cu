@@ -368,8 +368,8 @@ __global__ void __launch_bounds__(kFmThreads, 1) k_filter_mma(MeshDev g, int P, 
 #pragma unroll
       for (int i = 0; i < kFmMaxBlk; ++i) {
         if (prow[i] < 0) continue;
-        float gv = (hb.h00 * ta[i].x + hb.h10 * ta[i].y + hb.h01 * tb4[i].x + hb.h11 * tb4[i].y) * inv_sc;
-        const float dv = (hb.h00 * ta[i].y + hb.h10 * ta[i].z + hb.h01 * tb4[i].y + hb.h11 * tb4[i].z) * dscale;
+        float gv = herm_value(hb, ta[i], tb4[i]) * inv_sc;
+        const float dv = herm_slope(hb, ta[i], tb4[i]) * dscale;
         if (partner) {
           float gpv, dpv;
           green_lookup(gtab + prow[i], ge.pj, ge.pb, inv_h, gpv, dpv);

@@ -124,22 +124,32 @@ __global__ void __launch_bounds__(256) k_green_table(MeshDev g, const CellInfo* 
   const double k = j * h;
   const double s6 = tab->s6, s8 = tab->s8;
   const double A6 = s6 * q.c6pre, A8 = 3.0 * s8 * q.qq * q.c8pre;
-  double G, G1, G2;
+  double G, G1, G2, G3;
   if (k * q.R < 1e-15) {
-    // Taylor limit (pair_pot.py: the kR < thresh branch): G = a - b k^2
-    const double a = s6 * q.c6s1 + 3.0 * s8 * q.qq * q.c8s1, b = s6 * q.c6s2 + 3.0 * s8 * q.qq * q.c8s2;
-    G = a - b * k * k;
-    G1 = -2.0 * b * k;
-    G2 = -2.0 * b;
+    // k = 0: the value of the reference's Taylor branch (pair_pot.py:146, G = a), and the
+    // derivatives of the closed form G = F(kR) / k there, G^(m)(0) = F^(m+1)(0) R^(m+1) / (m+1)
+    // with F'(0) = A6 - sqrt2 sin(pi/8) A8, F''(0) = 0, F'''(0) = -2 A6 + sqrt2 sin(pi/8) A8,
+    // F''''(0) = 3 A6. (The reference's k^2 coefficient of the C6 term, pair_pot.py:96, scales as
+    // R where the expansion of the closed form gives 2 pi^2 / (9 R); it multiplies k^2 = 0 there,
+    // so it never enters its results, but the interpolation between knots needs the true G''.)
+    const double a = s6 * q.c6s1 + 3.0 * s8 * q.qq * q.c8s1;
+    const double r2s8 = 0.54119610014619698440;   // sqrt(2) sin(pi/8)
+    const double R3 = q.R * q.R * q.R;
+    G = a;
+    G1 = 0.0;
+    G2 = (-2.0 * A6 + r2s8 * A8) * R3 / 3.0;
+    G3 = 3.0 * A6 * R3 * q.R / 4.0;
   } else {
-    double n6, d6, e6, n8, d8, e8;
-    green_n(k * q.R, &n6, &d6, &e6, &n8, &d8, &e8);
-    const double F = A6 * n6 + A8 * n8, F1 = A6 * d6 + A8 * d8, F2 = A6 * e6 + A8 * e8;
-    G = F / k;
-    G1 = (q.R * F1 - G) / k;
-    G2 = (q.R * q.R * F2 - 2.0 * G1) / k;
+    double n6[4], n8[4];
+    green_n(k * q.R, n6, n8);
+    double F[4];
+    for (int m = 0; m < 4; ++m) F[m] = A6 * n6[m] + A8 * n8[m];
+    G = F[0] / k;
+    G1 = (q.R * F[1] - G) / k;
+    G2 = (q.R * q.R * F[2] - 2.0 * G1) / k;
+    G3 = (q.R * q.R * q.R * F[3] - 3.0 * G2) / k;
   }
-  out[e] = make_float4((float)G, (float)(h * G1), (float)(h * h * G2), 0.f);
+  out[e] = make_float4((float)G, (float)(h * G1), (float)(h * h * G2), (float)(h * h * h * G3));
 }
 
 int launch_green_table(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const Tables* tab,
@@ -350,8 +360,8 @@ __global__ void __launch_bounds__(kFilterThreads) k_filter_tiled(MeshDev g, int 
           T gv, dv;
           const int pi = row0[X] + (Y - X);
           if constexpr (sizeof(T) == 4) {
-            gv = hb.h00 * ta[y].x + hb.h10 * ta[y].y + hb.h01 * tb[y].x + hb.h11 * tb[y].y;
-            dv = (hb.h00 * ta[y].y + hb.h10 * ta[y].z + hb.h01 * tb[y].y + hb.h11 * tb[y].z) * inv_h;
+            gv = herm_value(hb, ta[y], tb[y]);
+            dv = herm_slope(hb, ta[y], tb[y]) * inv_h;
           } else {
             green_eval<T>(gp[X * S + Y], q.knorm, s6, s8, gv, dv);
           }

@@ -424,9 +424,11 @@ BATCH_WORKLOAD = "batch256_N32-4096_Z1-54_spme_p5_h1.2_E+F+stress"
 
 def run_accuracy(args, ws, rank, local):
     """Precision scaling: the seeded SiO2 box replicated 1^3..6^3 (648..139,968 atoms, jitter
-    N(0, 0.05 A)); plain float64 SPME and the mixed form against the float64 direct pairwise D3
-    lattice sum (committed fixtures, up to 5,184 atoms) and the mixed form against float64 SPME
-    at every size. One JSON line per size; energies in eV, forces eV/A, stress eV/A^3."""
+    N(0, 0.05 A)); plain float64 SPME, the mixed form (3D transforms) and the mixed form as the
+    headline runs it (TMA x-pass) against the float64 direct pairwise D3 lattice sum computed on
+    the device at every size (pairs within 25 A + continuum tail), against the CPU oracle's direct
+    sum where a fixture exists (648, 5,184 atoms), and the mixed forms against float64 SPME. One
+    JSON line per size; energies in eV, forces eV/A, stress eV/A^3."""
     if rank != 0:
         return
     from fourierd3_b200 import structures as st
@@ -435,6 +437,11 @@ def run_accuracy(args, ws, rank, local):
     device = torch.device("cuda", local)
     kw = dict(method="spme", mesh_spacing=1.2, interpolation_nodes=5, c6tol=1.0, r_cut=6.0)
     golden = os.path.join(REPO, "tests", "golden")
+
+    def diff(a, b):
+        return {"energy_rel": abs(a[0] - b[0]) / abs(b[0]), "force_max_ev_a": float(np.abs(a[1] - b[1]).max()),
+                "stress_max_ev_a3": float(np.abs(a[2] - b[2]).max())}
+
     for reps in range(1, 7):
         pos, cell, nums = st.sio2_scaled(reps)
         path = os.path.join(golden, f"direct_sio2_{len(nums)}.npz")
@@ -446,30 +453,36 @@ def run_accuracy(args, ws, rank, local):
             m = D3Model(nums, cell, precision=prec, device=device, **kw)
             e, f, s = m(pos, cell)
             res[prec] = (float(e), f.cpu().numpy(), s.cpu().numpy())
-            if prec == "mixed":
-                # the mixed form as the headline runs it: fused x-pass where it applies
-                m.engine.set_tuning(fft_x=1)
-                if m.engine.tuning()["fft_x"] == 1:
+            if prec == "fp64":
+                torch.cuda.synchronize(device)
+                t0 = time.perf_counter()
+                e, f, s = m.direct(pos, cell, r_direct=25.0)
+                torch.cuda.synchronize(device)
+                res["direct_gpu_s"] = time.perf_counter() - t0
+                res["direct_gpu"] = (float(e), f.cpu().numpy(), s.cpu().numpy())
+            else:
+                # the mixed form as the headline runs it: TMA x-pass where it applies
+                m.engine.set_tuning(fft_x=2, xq=4, xranks=4)
+                if m.engine.tuning()["fft_x"] == 2:
                     e, f, s = m(pos, cell)
-                    res["mixed_fused"] = (float(e), f.cpu().numpy(), s.cpu().numpy())
+                    res["mixed_tma"] = (float(e), f.cpu().numpy(), s.cpu().numpy())
             del m
             torch.cuda.empty_cache()
-        e64, f64, s64 = res["fp64"]
         line = {"workload": "accuracy_sio2_scaling", "n_atoms": len(nums), "reps": reps,
-                "energy_ev_fp64": e64}
-        for form in ("mixed", "mixed_fused"):
+                "energy_ev_fp64": res["fp64"][0], "energy_ev_direct": res["direct_gpu"][0],
+                "direct_gpu_s": res["direct_gpu_s"]}
+        for form in ("mixed", "mixed_tma"):
             if form in res:
-                e32, f32, s32 = res[form]
-                line[f"{form}_vs_fp64"] = {"energy_rel": abs(e32 - e64) / abs(e64),
-                                           "force_max_ev_a": float(np.abs(f32 - f64).max()),
-                                           "stress_max_ev_a3": float(np.abs(s32 - s64).max())}
+                line[f"{form}_vs_fp64"] = diff(res[form], res["fp64"])
+        for form in ("fp64", "mixed", "mixed_tma"):
+            if form in res:
+                line[f"{form}_vs_direct_gpu"] = diff(res[form], res["direct_gpu"])
         if d is not None:
-            for prec in [p for p in ("fp64", "mixed", "mixed_fused") if p in res]:
-                e, f, s = res[prec]
-                line[f"{prec}_vs_direct_sum"] = {
-                    "energy_rel": abs(e - float(d["energy_ev"])) / abs(float(d["energy_ev"])),
-                    "force_max_ev_a": float(np.abs(f - d["forces"]).max()),
-                    "stress_max_ev_a3": float(np.abs(s - d["stress"]).max())}
+            ref = (float(d["energy_ev"]), d["forces"], d["stress"])
+            line["direct_gpu_vs_direct_cpu_oracle"] = diff(res["direct_gpu"], ref)
+            for form in ("fp64", "mixed", "mixed_tma"):
+                if form in res:
+                    line[f"{form}_vs_direct_cpu_oracle"] = diff(res[form], ref)
         print(json.dumps(line), flush=True)
 
 

@@ -61,6 +61,10 @@ _SIGS = {
     "fd3_energy_forces_stress": (ctypes.c_int, [_vp, _c_int64, _vp, _vp, _dp, _vp, _c_double, _vp,
                                                 ctypes.c_size_t, _vp, _vp, _vp, _vp]),
     "fd3_atom_terms": (ctypes.c_int, [_vp, _c_int64, _c_int64, _vp, ctypes.c_size_t, _vp, _vp, _vp]),
+    "fd3_direct_workspace_size": (ctypes.c_int, [_vp, _c_int64, _dp, _c_double, _c_double,
+                                                 ctypes.POINTER(ctypes.c_size_t)]),
+    "fd3_direct_energy_forces_stress": (ctypes.c_int, [_vp, _c_int64, _vp, _vp, _dp, _vp, _c_double, _c_double,
+                                                       _vp, ctypes.c_size_t, _vp, _vp, _vp, _vp]),
     "fd3_neighbor_workspace_size":(ctypes.c_int, [_c_int64, _dp, _c_double, ctypes.POINTER(ctypes.c_size_t)]),
     "fd3_neighbor_count": (ctypes.c_int, [_c_int64, _vp, _dp, _c_double, _vp, ctypes.c_size_t,
                                           ctypes.POINTER(_c_int64), _vp]),
@@ -81,6 +85,35 @@ _lib = None
 
 def lib_path() -> str:
     return _LIB_PATH
+
+
+_TORCH_LIB_PATH = os.path.join(os.path.dirname(_LIB_PATH), "libfd3_torch.so")
+_ops_loaded = False
+
+
+def ops():
+    """``torch.ops.fd3``: the thin operator library over the C ABI (energy_forces_stress,
+    energy_edges; CUDA kernels call libfd3 on the current stream, Meta kernels give shapes).
+    Loaded once, after libfd3.so itself; raises if it has not been built."""
+    global _ops_loaded
+    if not _ops_loaded:
+        lib()
+        with _lock:
+            if not _ops_loaded:
+                if not os.path.exists(_TORCH_LIB_PATH):
+                    raise RuntimeError(f"{_TORCH_LIB_PATH} is missing: build it with `python -m fourierd3_b200.build`")
+                import torch
+
+                torch.ops.load_library(_TORCH_LIB_PATH)
+                _ops_loaded = True
+    import torch
+
+    return torch.ops.fd3
+
+
+def handle(p: ctypes.c_void_p) -> int:
+    """A plan pointer as the integer the operator library takes."""
+    return int(p.value or 0)
 
 
 def lib() -> ctypes.CDLL:

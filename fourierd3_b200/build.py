@@ -75,6 +75,35 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     return LIB
 
 
+TORCH_SRC = os.path.join(HERE, "csrc_torch", "fd3_torch_ops.cpp")
+TORCH_LIB = os.path.join(OUT_DIR, "libfd3_torch.so")
+
+
+def build_torch_ops(force: bool = False, verbose: bool = False) -> str:
+    """The thin torch operator library (torch.ops.fd3.*) over the C ABI: g++ against the
+    installed torch headers and libraries, linked to libfd3.so (found next to it at run time)."""
+    import torch
+
+    deps = [TORCH_SRC, LIB, os.path.join(os.path.dirname(HERE), "include", "fd3.h")]
+    if (not force and os.path.exists(TORCH_LIB)
+            and all(os.path.getmtime(d) <= os.path.getmtime(TORCH_LIB) for d in deps)):
+        return TORCH_LIB
+    tdir = os.path.dirname(torch.__file__)
+    abi = int(torch._C._GLIBCXX_USE_CXX11_ABI)
+    cmd = ["g++", "-O2", "-std=c++17", "-shared", "-fPIC", f"-D_GLIBCXX_USE_CXX11_ABI={abi}",
+           "-I" + os.path.join(tdir, "include"), "-I" + os.path.join(tdir, "include", "torch", "csrc", "api", "include"),
+           "-I" + os.path.join(CUDA_HOME, "include"), "-I" + os.path.join(os.path.dirname(HERE), "include"),
+           TORCH_SRC, "-o", TORCH_LIB + ".tmp",
+           "-L" + OUT_DIR, "-lfd3", "-L" + os.path.join(tdir, "lib"), "-ltorch", "-ltorch_cpu", "-ltorch_cuda",
+           "-lc10", "-lc10_cuda", "-L" + os.path.join(CUDA_HOME, "lib64"), "-lcudart",
+           "-Wl,-rpath,$ORIGIN", "-Wl,-rpath," + os.path.join(tdir, "lib")]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    os.replace(TORCH_LIB + ".tmp", TORCH_LIB)
+    return TORCH_LIB
+
+
 if __name__ == "__main__":
     extra = sys.argv[1:]
     print(build(force=True, verbose=True, extra=extra))

@@ -999,6 +999,105 @@ extern "C" int fd3_energy_forces_stress(fd3_plan* p, int64_t n_atoms, const doub
   return FD3_OK;
 }
 
+// ------------------------------------------------------------------ direct pair sum (accuracy oracle)
+namespace {
+struct DirectWork {
+  CellList cl;        // the bin grid of the pair cutoff r_direct
+  double* dEdc;       // [N R]
+  double* pair_part;  // [blocks 7]
+  double* sp_part;    // [kDirSpBlocks S R]
+  double* A;          // [S R]
+  double* tail;       // [2]
+  double* scratch;    // [S R + 2 S^2]: T, I_XY, phi_XY(Rc)
+};
+constexpr int kDirSpBlocks = 148;
+void carve_direct(const fd3_plan* p, int64_t N, int64_t K2, Carver& c, DirectWork& d) {
+  d.cl.bin_of = c.take<int>(N);
+  d.cl.bin_count = c.take<int>(K2);
+  d.cl.bin_start = c.take<int>(K2 + 1);
+  d.cl.order = c.take<int>(N);
+  d.cl.xs = c.take<double4>(N);
+  d.cl.meta = c.take<int4>(N);
+  d.cl.off = c.take<int4>(N);
+  d.dEdc = c.take<double>((size_t)N * p->R);
+  d.pair_part = c.take<double>((size_t)7 * ((N + 7) / 8));
+  d.sp_part = c.take<double>((size_t)kDirSpBlocks * p->S * p->R);
+  d.A = c.take<double>((size_t)p->S * p->R);
+  d.tail = c.take<double>(2);
+  d.scratch = c.take<double>(direct_scratch_doubles(p->S, p->R));
+}
+int direct_grids(const fd3_plan* p, int64_t N, const double* h_cell, double r_cut, double r_direct, CellGrid& g,
+                 CellGrid& g2, size_t* fused_bytes, size_t* total_bytes) {
+  if (!p || N < 1 || N > (int64_t)1 << 30 || !h_cell || !(r_direct > 0)) return FD3_EINVAL;
+  if (p->cnfunc == FD3_CN_D4) {
+    set_error("fd3_direct_energy_forces_stress", "the direct pair sum takes the smooth-cutoff CN");
+    return FD3_EINVAL;
+  }
+  FD3_TRY(make_cell_grid(h_cell, r_cut, &g));
+  FD3_TRY(make_cell_grid(h_cell, r_direct, &g2));
+  Carver c;
+  Work w;
+  carve(p, N, (int64_t)g.nb[0] * g.nb[1] * g.nb[2], c, w);
+  *fused_bytes = c.off;
+  DirectWork d;
+  carve_direct(p, N, (int64_t)g2.nb[0] * g2.nb[1] * g2.nb[2], c, d);
+  *total_bytes = c.off + 512;
+  return FD3_OK;
+}
+}  // namespace
+
+extern "C" int fd3_direct_workspace_size(const fd3_plan* p, int64_t n_atoms, const double* h_cell_ang,
+                                         double r_cut_ang, double r_direct_ang, size_t* bytes) {
+  if (!bytes) return FD3_EINVAL;
+  CellGrid g, g2;
+  size_t fused = 0;
+  return direct_grids(p, n_atoms, h_cell_ang, r_cut_ang, r_direct_ang, g, g2, &fused, bytes);
+}
+
+extern "C" int fd3_direct_energy_forces_stress(fd3_plan* p, int64_t n_atoms, const double* d_pos_ang,
+                                               const int32_t* d_species, const double* h_cell_ang,
+                                               const double* d_cell_ang, double r_cut_ang, double r_direct_ang,
+                                               void* d_work, size_t work_bytes, double* d_energy, double* d_forces,
+                                               double* d_stress, void* stream) {
+  if (!d_pos_ang || !d_species || !d_cell_ang || !d_energy || !d_forces || !d_stress) return FD3_EINVAL;
+  CellGrid g, g2;
+  size_t fused = 0, total = 0;
+  FD3_TRY(direct_grids(p, n_atoms, h_cell_ang, r_cut_ang, r_direct_ang, g, g2, &fused, &total));
+  if (!d_work || work_bytes < total) {
+    set_error("workspace", "smaller than fd3_direct_workspace_size");
+    return FD3_ENOMEM;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  const int N = (int)n_atoms;
+  Work w;
+  FD3_TRY(check_work(p, N, (int64_t)g.nb[0] * g.nb[1] * g.nb[2], d_work, work_bytes, w));
+  Carver c;   // the direct sum's buffers follow the fused ones
+  c.base = reinterpret_cast<char*>(((uintptr_t)d_work + 255) & ~(uintptr_t)255);
+  {
+    Work skip;
+    carve(p, N, (int64_t)g.nb[0] * g.nb[1] * g.nb[2], c, skip);
+  }
+  DirectWork d;
+  carve_direct(p, N, (int64_t)g2.nb[0] * g2.nb[1] * g2.nb[2], c, d);
+  FD3_TRY(launch_cellinfo(d_cell_ang, kAngToBohr, w.ci, s, h_cell_ang));
+  FD3_TRY(build_cell_list(g, N, d_pos_ang, d_species, w.cl, s));
+  int n_self = 0, n_pair = 0, n_cnv = 0;
+  FD3_TRY(launch_cn_c6_cells(g, N, w.cl, d_pos_ang, d_species, p->d_tab, p->d_eigvecs, p->R, w.cn, w.c6, w.dc6,
+                             w.self_part, &n_self, w.hits, s));
+  FD3_TRY(build_cell_list(g2, N, d_pos_ang, d_species, d.cl, s));
+  // pair gradient (Hartree/Bohr) staged in d_forces, finished by the CN adjoint
+  FD3_TRY(launch_direct_pairs(g2, N, d.cl, w.c6, p->d_tab, p->R, p->S, p->d_green, d.dEdc, d_forces, d.pair_part,
+                              &n_pair, s));
+  FD3_TRY(launch_direct_tail_gcn(N, d_species, w.c6, w.dc6, d.dEdc, p->d_tab, p->d_green, p->S, p->R,
+                                 r_direct_ang * kAngToBohr, w.ci, d.sp_part, kDirSpBlocks, d.A, d.tail, d.scratch,
+                                 w.gcn, s));
+  FD3_TRY(launch_cn_adjoint_cells(g, N, w.cl, d_pos_ang, d_species, p->d_tab, w.gcn, d_forces,
+                                  -kHartreeToEv * kAngToBohr, w.cnv_part, &n_cnv, w.hits, s));
+  FD3_TRY(launch_direct_finalize(d.pair_part, n_pair, d.tail, w.cnv_part, n_cnv, w.ci, d_energy, d_stress, s));
+  FD3_TRY(launch_poison_if_stale(w.ci, N, d_energy, d_forces, d_stress, s));
+  return FD3_OK;
+}
+
 // ------------------------------------------------------------------ per-atom read-back
 extern "C" int fd3_atom_terms(const fd3_plan* p, int64_t n_atoms, int64_t n_bins, const void* d_work,
                               size_t work_bytes, double* d_cn, double* d_c6, void* stream) {

@@ -977,6 +977,103 @@ __global__ void __launch_bounds__(256) k_nbr_fill(GridDev g, int n, const int* _
                   });
 }
 
+// ------------------------------------------------------------------ direct pair sum (float64)
+// The accuracy oracle's lattice sum on the device: over every image pair (i, j, n) closer than
+// the grid's cutoff (r_direct) except i = j at n = 0, with C6_ij = sum_r lambda_r c_ir c_jr
+// (the plan's low-rank factors) and the BJ-damped kernel of src/fourierd3/pair_pot.py:64,
+//   phi(r) = s6 / (r^6 + R0^6) + 3 s8 qq / (r^8 + R0^8),  E = -1/2 sum C6 phi   (Bohr, Hartree).
+// Warp per atom i over the bin-sorted atoms: e_i = sum_j C6 phi, dE/dc_ir = -lambda_r sum_j
+// c_jr phi, dE/dx_i = sum_j C6 (phi'/r) d (d = x_j + n - x_i; each pair is seen from both ends),
+// and per block e = sum_i e_i and the virial -1/2 sum C6 (phi'/r) d_a d_b (6 components).
+__global__ void __launch_bounds__(256) k_direct_pairs(GridDev g, int n, const int* __restrict__ bin_start,
+                                                     const double4* __restrict__ xs, const int4* __restrict__ meta,
+                                                     const int4* __restrict__ off, const double* __restrict__ c6,
+                                                     const Tables* __restrict__ tab, int R, int S,
+                                                     const GreenPair* __restrict__ gp, double* __restrict__ dEdc,
+                                                     double* __restrict__ grad, double* __restrict__ part) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int t = blockIdx.x * kWarpsPerBlock + wid;
+  double acc[7] = {0, 0, 0, 0, 0, 0, 0};   // e, virial xx xy xz yy yz zz
+  if (t < n) {
+    const double4 xi = xs[t];
+    const int i = meta[t].w;
+    const int Xi = (int)xi.w;
+    const double s6 = tab->s6, s8 = tab->s8;
+    double ci[8], gc[8];
+#pragma unroll
+    for (int r = 0; r < 8; ++r) {
+      ci[r] = r < R ? tab->eigs[r] * c6[(size_t)i * R + r] : 0.0;
+      gc[r] = 0.0;
+    }
+    double e = 0.0, g0 = 0.0, g1 = 0.0, g2 = 0.0, v[6] = {0, 0, 0, 0, 0, 0};
+    visit_neighbors(g, bin_start, xs, meta, i, xi.x, xi.y, xi.z, off[i],
+                    [&](bool hit, int u, int j, int, int, int, double d0, double d1, double d2) {
+                      if (!hit) return;
+                      const double b0 = d0 * kAngToBohr, b1 = d1 * kAngToBohr, b2 = d2 * kAngToBohr;
+                      const double r2 = b0 * b0 + b1 * b1 + b2 * b2;
+                      const GreenPair q = gp[Xi * S + (int)xs[u].w];
+                      const double R02 = q.R * q.R, R06 = R02 * R02 * R02, R08 = R06 * R02;
+                      const double r4 = r2 * r2, r6 = r4 * r2, r8 = r6 * r2;
+                      const double den6 = r6 + R06, den8 = r8 + R08;
+                      const double phi = s6 / den6 + 3.0 * s8 * q.qq / den8;
+                      const double dphi_r = -6.0 * s6 * r4 / (den6 * den6) - 24.0 * s8 * q.qq * r6 / (den8 * den8);
+                      double C6 = 0.0;
+#pragma unroll
+                      for (int r = 0; r < 8; ++r)
+                        if (r < R) {
+                          const double cj = c6[(size_t)j * R + r];
+                          C6 += ci[r] * cj;
+                          gc[r] += cj * phi;
+                        }
+                      e += C6 * phi;
+                      const double w = C6 * dphi_r;
+                      g0 += w * b0;
+                      g1 += w * b1;
+                      g2 += w * b2;
+                      v[0] += w * b0 * b0;
+                      v[1] += w * b0 * b1;
+                      v[2] += w * b0 * b2;
+                      v[3] += w * b1 * b1;
+                      v[4] += w * b1 * b2;
+                      v[5] += w * b2 * b2;
+                    });
+    e = warp_sum(e);
+    g0 = warp_sum(g0);
+    g1 = warp_sum(g1);
+    g2 = warp_sum(g2);
+#pragma unroll
+    for (int r = 0; r < 8; ++r) gc[r] = warp_sum(gc[r]);
+#pragma unroll
+    for (int c = 0; c < 6; ++c) v[c] = warp_sum(v[c]);
+    if (lane == 0) {
+      for (int r = 0; r < R; ++r) dEdc[(size_t)i * R + r] = -tab->eigs[r] * gc[r];
+      grad[3 * (size_t)i] = g0;
+      grad[3 * (size_t)i + 1] = g1;
+      grad[3 * (size_t)i + 2] = g2;
+      acc[0] = e;
+#pragma unroll
+      for (int c = 0; c < 6; ++c) acc[1 + c] = -0.5 * v[c];
+    }
+  }
+  block_sum_store<7>(acc, part + 7 * blockIdx.x);
+}
+
+int launch_direct_pairs(const CellGrid& g, int n, const CellList& cl, const double* c6, const Tables* tab, int R,
+                        int S, const GreenPair* gp, double* dEdc, double* grad, double* part, int* n_blocks,
+                        cudaStream_t s) {
+  if (R < 1 || R > 8) {
+    set_error("direct sum", "the direct pair sum takes at most 8 ranks");
+    return FD3_EINVAL;
+  }
+  const int blocks = (n + kWarpsPerBlock - 1) / kWarpsPerBlock;
+  *n_blocks = blocks;
+  if (blocks == 0) return FD3_OK;
+  k_direct_pairs<<<blocks, 32 * kWarpsPerBlock, 0, s>>>(to_dev(g), n, cl.bin_start, cl.xs, cl.meta, cl.off, c6, tab,
+                                                        R, S, gp, dEdc, grad, part);
+  FD3_LAUNCHED();
+  return FD3_OK;
+}
+
 int launch_nbr_count(const CellGrid& g, int n, const CellList& cl, const double* pos_ang, int* counts,
                      cudaStream_t s) {
   (void)pos_ang;

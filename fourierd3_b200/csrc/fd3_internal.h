@@ -84,6 +84,18 @@ int launch_cn_adjoint_cells(const CellGrid& g, int n, const CellList& cl, const 
                             double out_scale, double* vir_part, int* n_blocks, const HitStore& hs,
                             cudaStream_t s);
 
+// direct pairwise lattice sum (float64 accuracy oracle on the device)
+int launch_direct_pairs(const CellGrid& g, int n, const CellList& cl, const double* c6, const Tables* tab, int R,
+                        int S, const GreenPair* gp, double* dEdc, double* grad, double* part, int* n_blocks,
+                        cudaStream_t s);
+size_t direct_scratch_doubles(int S, int R);
+int launch_direct_tail_gcn(int n, const int32_t* species, const double* c6, const double* dc6, const double* dEdc,
+                           const Tables* tab, const GreenPair* gp, int S, int R, double rc_bohr, const CellInfo* ci,
+                           double* sp_part, int sp_blocks, double* A, double* tail, double* T, double* gcn,
+                           cudaStream_t s);
+int launch_direct_finalize(const double* pair_part, int n_pair, const double* tail, const double* cnv_part, int n_cnv,
+                           const CellInfo* ci, double* energy, double* stress, cudaStream_t s);
+
 // edge-list CN path
 // Edges sorted by source and by destination (stable counting sorts of the edge ids): the
 // per-atom segments the fixed-order CN sum and its adjoint walk.

@@ -270,20 +270,13 @@ class Engine:
         sh = shifts_b.detach().to(torch.float64).contiguous()
         ei = edge_index.to(torch.int64).contiguous()
         src, dst = ei[0], ei[1]
-        energy = torch.empty((), dtype=torch.float64, device=self.device)
-        gpos = torch.empty_like(pos) if need_grad else None
-        gsh = torch.empty_like(sh) if need_grad else None
-        gcell = torch.empty((3, 3), dtype=torch.float64, device=self.device) if need_grad else None
         work = self.edge_workspace(n, e)
-
-        def ptr(t):
-            return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else None
-
-        rc = _native.lib().fd3_energy_edges(
-            self._plan, n, ptr(pos), ptr(self.species_tensor()), ptr(cell), e, ptr(src), ptr(dst), ptr(sh),
-            1 if need_grad else 0, ptr(work), work.numel(), ptr(energy), ptr(gpos), ptr(gsh), ptr(gcell),
-            ctypes.c_void_p(_stream_ptr(self.device)))
-        _native.check(rc, "fd3_energy_edges")
+        # torch.ops.fd3.energy_edges: the operator layer over fd3_energy_edges (current stream)
+        energy, gpos, gsh, gcell = _native.ops().energy_edges(
+            _native.handle(self._plan), pos, self.species_tensor(), cell, src.contiguous(), dst.contiguous(), sh,
+            bool(need_grad), work)
+        if not need_grad:
+            return energy, None, None, None
         return energy, gpos, gsh, gcell
 
     def energy_forces_stress(self, pos_ang: torch.Tensor, cell_ang: np.ndarray, r_cut_ang: float,
@@ -302,14 +295,16 @@ class Engine:
             work = self.workspace(n, nb[0] * nb[1] * nb[2])
         if species is None:
             species = self.species_tensor()
+        if out is None:
+            # torch.ops.fd3.energy_forces_stress: the operator layer over fd3_energy_forces_stress
+            return _native.ops().energy_forces_stress(
+                _native.handle(self._plan), pos_ang, species, torch.from_numpy(cell_h.reshape(3, 3).copy()),
+                float(r_cut_ang), work, cell_dev)
+        # caller-owned outputs (the batch runner's packed buffers, fixed across graph replays):
+        # the C ABI directly
         if cell_dev is None:
             cell_dev = torch.as_tensor(cell_h, dtype=torch.float64).to(self.device, non_blocking=False)
-        if out is None:
-            energy = torch.empty((), dtype=torch.float64, device=self.device)
-            forces = torch.empty((n, 3), dtype=torch.float64, device=self.device)
-            stress = torch.empty((3, 3), dtype=torch.float64, device=self.device)
-        else:
-            energy, forces, stress = out
+        energy, forces, stress = out
         rc = _native.lib().fd3_energy_forces_stress(
             self._plan, n, ctypes.c_void_p(pos_ang.data_ptr()), ctypes.c_void_p(species.data_ptr()),
             _native.dptr(cell_h), ctypes.c_void_p(cell_dev.data_ptr()), float(r_cut_ang),
@@ -317,6 +312,33 @@ class Engine:
             ctypes.c_void_p(forces.data_ptr()), ctypes.c_void_p(stress.data_ptr()),
             ctypes.c_void_p(_stream_ptr(self.device)))
         _native.check(rc, "fd3_energy_forces_stress")
+        return energy, forces, stress
+
+    def direct_energy_forces_stress(self, pos_ang: torch.Tensor, cell_ang: np.ndarray, r_cut_ang: float,
+                                    r_direct_ang: float = 25.0):
+        """Direct pairwise D3(BJ) lattice sum in float64 (the accuracy oracle of the mesh methods,
+        on the device): every image pair closer than ``r_direct_ang`` plus the continuum tail,
+        with this plan's CN and C6 factors. Returns (energy [eV], forces [eV/A], stress [eV/A^3])."""
+        n = pos_ang.shape[0]
+        cell_h = np.ascontiguousarray(cell_ang, dtype=np.float64).reshape(9)
+        nbytes = ctypes.c_size_t()
+        _native.check(_native.lib().fd3_direct_workspace_size(self._plan, n, _native.dptr(cell_h), float(r_cut_ang),
+                                                              float(r_direct_ang), ctypes.byref(nbytes)),
+                      "fd3_direct_workspace_size")
+        work = torch.empty(int(nbytes.value), dtype=torch.uint8, device=self.device)
+        species = self.species_tensor()
+        cell_dev = torch.as_tensor(cell_h, dtype=torch.float64).to(self.device)
+        energy = torch.empty((), dtype=torch.float64, device=self.device)
+        forces = torch.empty((n, 3), dtype=torch.float64, device=self.device)
+        stress = torch.empty((3, 3), dtype=torch.float64, device=self.device)
+        pos = pos_ang.to(device=self.device, dtype=torch.float64).contiguous()
+        rc = _native.lib().fd3_direct_energy_forces_stress(
+            self._plan, n, ctypes.c_void_p(pos.data_ptr()), ctypes.c_void_p(species.data_ptr()),
+            _native.dptr(cell_h), ctypes.c_void_p(cell_dev.data_ptr()), float(r_cut_ang), float(r_direct_ang),
+            ctypes.c_void_p(work.data_ptr()), work.numel(), ctypes.c_void_p(energy.data_ptr()),
+            ctypes.c_void_p(forces.data_ptr()), ctypes.c_void_p(stress.data_ptr()),
+            ctypes.c_void_p(_stream_ptr(self.device)))
+        _native.check(rc, "fd3_direct_energy_forces_stress")
         return energy, forces, stress
 
 

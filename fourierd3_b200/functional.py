@@ -48,6 +48,14 @@ class D3Model:
         cell_h = np.asarray(cell.detach().cpu() if torch.is_tensor(cell) else cell, dtype=np.float64)
         return self.engine.energy_forces_stress(pos, cell_h, self.r_cut, out=out)
 
+    def direct(self, positions, cell, r_direct: float = 25.0):
+        """The direct pairwise lattice sum in float64 (pairs within ``r_direct`` A plus the
+        continuum tail) with this model's CN, C6 factors and damping: the accuracy oracle the
+        mesh methods converge to. Returns (E [eV], F [eV/A], stress [eV/A^3])."""
+        pos = torch.as_tensor(positions, dtype=torch.float64).to(self.device).contiguous()
+        cell_h = np.asarray(cell.detach().cpu() if torch.is_tensor(cell) else cell, dtype=np.float64)
+        return self.engine.direct_energy_forces_stress(pos, cell_h, self.r_cut, r_direct)
+
 
 _CACHE: dict = {}
 

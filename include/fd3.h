@@ -183,6 +183,26 @@ FD3_API int fd3_energy_forces_stress(fd3_plan* plan, int64_t n_atoms, const doub
                              double* d_forces, double* d_stress, void* stream);
 
 /*
+ * Direct pairwise D3(BJ) lattice sum in float64: the accuracy oracle of the reciprocal-space
+ * methods (no reference counterpart; the reference checks its mesh methods against its own
+ * Ewald path and torch-dftd, papercode/get_convergence.py). With the plan's smooth-cutoff CN and
+ * low-rank C6 factors (C6_ij = sum_r lambda_r c_ir c_jr, core.py:323-386, 449-543) and the BJ
+ * kernel of pair_pot.py:64:
+ *   E = -1/2 sum'_{i,j,n} C6_ij [s6 / (r^6 + R0^6) + 3 s8 sqrt(Q_i Q_j) / (r^8 + R0^8)]
+ * over every image pair closer than r_direct_ang (i = j at n = 0 excluded), plus the continuum
+ * tail beyond r_direct; forces and stress analytic (pair terms, tail, CN chain). Same units and
+ * output layout as fd3_energy_forces_stress; the plan's cnfunc must be FD3_CN_SMOOTH. Cost
+ * grows as N r_direct^3: meant for accuracy checks, not for the timed path.
+ */
+FD3_API int fd3_direct_workspace_size(const fd3_plan* plan, int64_t n_atoms, const double* h_cell_ang,
+                                      double r_cut_ang, double r_direct_ang, size_t* bytes);
+FD3_API int fd3_direct_energy_forces_stress(fd3_plan* plan, int64_t n_atoms, const double* d_pos_ang,
+                                            const int32_t* d_species, const double* h_cell_ang,
+                                            const double* d_cell_ang, double r_cut_ang, double r_direct_ang,
+                                            void* d_work, size_t work_bytes, double* d_energy,
+                                            double* d_forces, double* d_stress, void* stream);
+
+/*
  * Per-atom intermediates of the last compute call that used this workspace: the coordination
  * numbers after the optional cncorr correction (FourierD3.compute_cn_smooth, core.py:323-386)
  * and the rank-r C6 factors c[i, r] = sum_p w_ip V[Z_i, p, r] (core.py:449-478, 525-532),

@@ -194,3 +194,20 @@ def test_fused_dense_box_uses_fallback_paths(cuda_device):
     assert abs(float(e) - e_ref) <= E_REL * abs(e_ref)
     np.testing.assert_allclose(f.cpu().numpy(), f_ref, rtol=0, atol=F_ABS)
     np.testing.assert_allclose(s.cpu().numpy(), s_ref, rtol=0, atol=S_ABS)
+
+
+def test_operator_layer_matches_c_abi(cuda_device):
+    """torch.ops.fd3.energy_forces_stress (the default call) and the C ABI with caller-owned
+    outputs (the batch runner's path) run the same kernels: bitwise-equal results."""
+    from fourierd3_b200 import D3Model
+
+    rec = gc.load("hcno_240_spme_p6")
+    m = D3Model(rec["numbers"], rec["cell"], precision="fp64", device=cuda_device, **gc.model_kwargs(rec["config"]))
+    pos = torch.tensor(rec["positions"], dtype=torch.float64, device=cuda_device)
+    a = [t.clone() for t in m.engine.energy_forces_stress(pos, rec["cell"], m.r_cut)]
+    out = (torch.empty((), dtype=torch.float64, device=cuda_device),
+           torch.empty((len(rec["numbers"]), 3), dtype=torch.float64, device=cuda_device),
+           torch.empty((3, 3), dtype=torch.float64, device=cuda_device))
+    b = m.engine.energy_forces_stress(pos, rec["cell"], m.r_cut, out=out)
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)

@@ -224,6 +224,7 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
       m.xq = -1;
       m.xranks = -1;
       m.filter_mma = -1;
+      m.gather_tile = -1;
       m.fft_x = -1;   // default: off (3D cuFFT around the separate filter measured faster on B200)
       const size_t Mh = (size_t)m.n[0] * m.n[1] * m.nzh;
       m.win_axes = nullptr;
@@ -448,6 +449,14 @@ extern "C" int fd3_plan_set_tuning(fd3_plan* p, int32_t knob, int32_t value) {
     p->mg.xpencil = value;
     return FD3_OK;
   }
+  if (knob == FD3_TUNE_GATHER_TILE) {
+    if (value < -1 || value > 1) {
+      set_error("fd3_plan_set_tuning", "tile-staged gather must be -1 (default), 0 (per-atom gather) or 1");
+      return FD3_EINVAL;
+    }
+    p->mg.gather_tile = value;
+    return FD3_OK;
+  }
   if (knob == FD3_TUNE_SPREAD_CAP) {
     if (value != 0 && value < 256) {
       set_error("fd3_plan_set_tuning", "spread staging cap must be 0 (shared-memory bound) or >= 256");
@@ -498,6 +507,13 @@ extern "C" int fd3_plan_get_tuning(const fd3_plan* p, int32_t knob, int32_t* val
   }
   if (knob == FD3_TUNE_XPENCIL) {
     *value = p->has_fft2 ? xfilter_pencil(p->mg, p->precision == FD3_PREC_FP64 ? 1 : 0) : 0;
+    return FD3_OK;
+  }
+  if (knob == FD3_TUNE_GATHER_TILE) {
+    *value = p->method != FD3_METHOD_EWALD && p->mg.gather_tile == 1 &&
+                     gather_tile_applies(p->mg, p->precision == FD3_PREC_FP64 ? 8 : 4)
+                 ? 1
+                 : 0;
     return FD3_OK;
   }
   set_error("fd3_plan_get_tuning", "unknown knob");

@@ -4,9 +4,13 @@
 // fence for shared memory.
 #pragma once
 #include <cuda.h>
+#include <cudaTypedefs.h>
 #include <stdint.h>
 
 namespace fd3 {
+
+// cuTensorMapEncodeTiled from the driver (null when the driver does not export it).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder();
 
 constexpr long long kAsyncWaitCycles = 4000000000LL;   // about two seconds at B200 clocks
 

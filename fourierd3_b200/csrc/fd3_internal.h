@@ -144,6 +144,7 @@ struct MeshGeom {
   int xq;         // TMA x-pass: q values per unit (4, 8, 16, 32), -1 default
   int xranks;     // TMA x-pass: ranks per unit (1, 2, 4), -1 default
   int filter_mma; // float spectrum: 1 tensor-core (tcgen05) filter where it applies, 0 CUDA cores, -1 default
+  int gather_tile; // fused-path gather: 1 tile-staged TMA gather where it applies, 0 or -1 (default) per-atom
   const float* win_axes;  // SPME, mixed form: sinc(m/n)^(2p) per axis, [nx | ny | nz/2+1] (null: none)
 };
 // h_expect (optional, host, copied into the launch): the cell the caller's host-side geometry (cell
@@ -163,6 +164,8 @@ struct MeshRecords {
   void* dw;     // [N][3][P] d weight / d local coordinate
   void* c;      // [N][R] rank factors
 };
+// Whether the tile-staged (TMA) gather applies to this mesh for elements of `elem` bytes.
+bool gather_tile_applies(const MeshGeom& mg, size_t elem);
 template <typename T>
 int launch_spread(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
                   const double* c6, const CellInfo* ci, const int* key_start, const int* order,

@@ -728,6 +728,10 @@ int launch_spread(const MeshGeom& mg, int n, const double* pos, double pos_scale
 }
 
 // ------------------------------------------------------------------ gather
+}  // namespace fd3
+#include "fd3_gather_tile.cuh"   // the tile-staged (TMA) gather, on MeshDev / MeshRecords above
+namespace fd3 {
+
 constexpr int kGatherWarps = 8;
 
 template <typename T, int P, bool LAG, int MAXR>
@@ -1007,8 +1011,13 @@ static int gather_r(const MeshGeom& mg, int blocks, int n, const double* pos, do
                     const double* c6, const double* dc6, const CellInfo* ci, const Tables* tab, const int* order,
                     const int* key_start, const MeshRecords& rec, const T* phi, double* gcn, double* gpos,
                     double* mcell, int* n_mcell, cudaStream_t s) {
+  // tile-staged gather (one CTA per (tile, species) key, the key's mesh box staged once by TMA)
+  // for the fused path where its box fits two CTAs per SM, when asked for
+  if (!mcell && mg.gather_tile == 1 && gather_tile_applies(mg, sizeof(T))) {
+    *n_mcell = 0;
+    return launch_gather_tile<T, P>(mg, n, c6, dc6, ci, tab, order, key_start, rec, phi, gcn, gpos, s);
+  }
   const MeshDev g = to_dev(mg);
-  (void)key_start;
   *n_mcell = mcell ? blocks : 0;
   const int tb = 32 * kGatherWarps;
   const int4* rb = rec.b;

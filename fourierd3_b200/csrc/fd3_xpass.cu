@@ -8,8 +8,8 @@
 
 namespace fd3 {
 
-namespace {
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+// cuTensorMapEncodeTiled from the driver (null when the driver does not export it).
+PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   static std::once_flag once;
   std::call_once(once, [] {
@@ -21,7 +21,6 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   });
   return fn;
 }
-}  // namespace
 
 // Whether the TMA x-pass can run this mesh with Q q values and RG ranks per unit: nx a tabulated
 // length, at most 4 species, RG <= R, an even number of values per spectrum row block (the TMA
@@ -48,7 +47,7 @@ int launch_xpass(const MeshGeom& mg, int Q, int RG, const CellInfo* ci, const Gr
     set_error("filter", "the TMA x-pass does not apply to this mesh / pencil");
     return FD3_EINVAL;
   }
-  auto fn = encode_fn();
+  auto fn = tensor_map_encoder();
   if (!fn) {
     set_error("filter", "cuTensorMapEncodeTiled is not available from the driver");
     return FD3_ECUDA;

@@ -188,12 +188,13 @@ class Engine:
     _KNOBS = {"filter_kt": _native.TUNE_FILTER_KT, "spread_zc": _native.TUNE_SPREAD_ZC,
               "spread_cap": _native.TUNE_SPREAD_CAP, "fft_x": _native.TUNE_FFT_X,
               "xpencil": _native.TUNE_XPENCIL, "xq": _native.TUNE_XQ, "xranks": _native.TUNE_XRANKS,
-              "filter_mma": _native.TUNE_FILTER_MMA}
+              "filter_mma": _native.TUNE_FILTER_MMA, "gather_tile": _native.TUNE_GATHER_TILE}
 
     def set_tuning(self, filter_kt: Optional[int] = None, spread_zc: Optional[int] = None,
                    spread_cap: Optional[int] = None, fft_x: Optional[int] = None,
                    xpencil: Optional[int] = None, xq: Optional[int] = None,
-                   xranks: Optional[int] = None, filter_mma: Optional[int] = None) -> None:
+                   xranks: Optional[int] = None, filter_mma: Optional[int] = None,
+                   gather_tile: Optional[int] = None) -> None:
         """Launch-shape knobs (results agree to rounding): ``filter_kt`` = k-points per filter
         tile, ``spread_zc`` = z-tiles per column chunk of the spread, ``spread_cap`` = staged
         atoms per chunk at most, ``fft_x`` = 0 (3D cuFFT around the filter), 1 (2D cuFFT and the
@@ -201,10 +202,12 @@ class Engine:
         of every channel) or 2 (the same with TMA-moved units of ``xq`` = 4, 8, 16 or 32
         flattened (y, kz) values of ``xranks`` = 1, 2 or 4 ranks, mixed precision),
         ``filter_mma`` = 1 (mixed precision: the per-k-point species products of the separate
-        filter on the tensor cores) or 0 (CUDA cores); -1 (0 for the cap) restores a default."""
+        filter on the tensor cores) or 0 (CUDA cores), ``gather_tile`` = 1 (one CTA per mesh
+        tile and species stages the tile's potential box once by TMA) or 0 (warp per atom reading
+        the mesh directly); -1 (0 for the cap) restores a default."""
         for name, val in (("filter_kt", filter_kt), ("spread_zc", spread_zc), ("spread_cap", spread_cap),
                           ("fft_x", fft_x), ("xpencil", xpencil), ("xq", xq), ("xranks", xranks),
-                          ("filter_mma", filter_mma)):
+                          ("filter_mma", filter_mma), ("gather_tile", gather_tile)):
             if val is not None:
                 _native.check(_native.lib().fd3_plan_set_tuning(self._plan, self._KNOBS[name], int(val)),
                               "fd3_plan_set_tuning")

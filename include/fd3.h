@@ -113,6 +113,10 @@ FD3_API int fd3_plan_destroy(fd3_plan* plan);
  *                       on the tensor cores (tcgen05.mma kind::tf32, operands split into tf32
  *                       high and low parts; at most 64 species and 8 ranks, as shared memory
  *                       allows), 0 or -1 = CUDA cores (the default).
+ *   FD3_TUNE_GATHER_TILE fused-path gather: 1 = one CTA per (mesh tile, species) that stages
+ *                       the tile's potential box once by TMA (at most 8 ranks, the box within
+ *                       113 KB of shared memory); 0 or -1 (the default) = warp per atom reading
+ *                       the mesh directly (faster unless a tile holds many atoms per species).
  * fd3_plan_get_tuning returns the value in effect (the default resolved). */
 #define FD3_TUNE_FILTER_KT 0
 #define FD3_TUNE_SPREAD_ZC 1
@@ -122,6 +126,7 @@ FD3_API int fd3_plan_destroy(fd3_plan* plan);
 #define FD3_TUNE_XQ 5
 #define FD3_TUNE_XRANKS 6
 #define FD3_TUNE_FILTER_MMA 7
+#define FD3_TUNE_GATHER_TILE 8
 FD3_API int fd3_plan_set_tuning(fd3_plan* plan, int32_t knob, int32_t value);
 FD3_API int fd3_plan_get_tuning(const fd3_plan* plan, int32_t knob, int32_t* value);
 

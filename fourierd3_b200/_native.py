@@ -24,6 +24,7 @@ TUNE_XQ = 5
 TUNE_XRANKS = 6
 TUNE_FILTER_MMA = 7
 TUNE_GATHER_TILE = 8
+TUNE_FFT_YZ = 9
 
 _c_int32 = ctypes.c_int32
 _c_int64 = ctypes.c_int64

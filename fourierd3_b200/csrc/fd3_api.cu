@@ -225,6 +225,7 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
       m.xranks = -1;
       m.filter_mma = -1;
       m.gather_tile = -1;
+      m.fft_yz = -1;
       m.fft_x = -1;   // default: off (3D cuFFT around the separate filter measured faster on B200)
       const size_t Mh = (size_t)m.n[0] * m.n[1] * m.nzh;
       m.win_axes = nullptr;
@@ -384,6 +385,11 @@ static bool xpass_on(const fd3_plan* p) {
   return p->method != FD3_METHOD_EWALD && p->has_fft2 && p->precision == FD3_PREC_MIXED && p->mg.fft_x == 2 &&
          xpass_applies(p->mg, Q, RG);
 }
+// fused (y, z) transforms in effect: float mesh on a 2D-transform path, ny = nz = 256, asked for
+static bool fft_yz_on(const fd3_plan* p) {
+  return p->precision == FD3_PREC_MIXED && p->method != FD3_METHOD_EWALD && p->mg.fft_yz >= 1 &&
+         yzfft_applies(p->mg);
+}
 static bool old_xpass_on(const fd3_plan* p) {
   return p->method != FD3_METHOD_EWALD && p->has_fft2 && p->mg.fft_x == 1 &&
          xfilter_pencil(p->mg, p->precision == FD3_PREC_FP64 ? 1 : 0) > 0;
@@ -449,6 +455,14 @@ extern "C" int fd3_plan_set_tuning(fd3_plan* p, int32_t knob, int32_t value) {
     p->mg.xpencil = value;
     return FD3_OK;
   }
+  if (knob == FD3_TUNE_FFT_YZ) {
+    if (value < -1 || value > 2) {
+      set_error("fd3_plan_set_tuning", "fused (y, z) transforms must be -1 (default), 0 (cuFFT), 1 or 2");
+      return FD3_EINVAL;
+    }
+    p->mg.fft_yz = value;
+    return FD3_OK;
+  }
   if (knob == FD3_TUNE_GATHER_TILE) {
     if (value < -1 || value > 1) {
       set_error("fd3_plan_set_tuning", "tile-staged gather must be -1 (default), 0 (per-atom gather) or 1");
@@ -507,6 +521,10 @@ extern "C" int fd3_plan_get_tuning(const fd3_plan* p, int32_t knob, int32_t* val
   }
   if (knob == FD3_TUNE_XPENCIL) {
     *value = p->has_fft2 ? xfilter_pencil(p->mg, p->precision == FD3_PREC_FP64 ? 1 : 0) : 0;
+    return FD3_OK;
+  }
+  if (knob == FD3_TUNE_FFT_YZ) {
+    *value = (xpass_on(p) || old_xpass_on(p)) && fft_yz_on(p) ? p->mg.fft_yz : 0;
     return FD3_OK;
   }
   if (knob == FD3_TUNE_GATHER_TILE) {
@@ -742,13 +760,19 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
   prof_mark(p, s, "spread");
   const bool tma_x = sizeof(T) == 4 && xpass_on(p);
   if (tma_x || old_xpass_on(p)) {
-    // (y, z) transforms by cuFFT; x transform, filter and inverse x transform in one kernel
-    FD3_CUFFT(cufftSetStream(p->fwd2, s));
-    FD3_CUFFT(cufftSetWorkArea(p->fwd2, w.fftw));
-    if (sizeof(T) == 8)
-      FD3_CUFFT(cufftExecD2Z(p->fwd2, (cufftDoubleReal*)w.rho, (cufftDoubleComplex*)w.spec));
-    else
-      FD3_CUFFT(cufftExecR2C(p->fwd2, (cufftReal*)w.rho, (cufftComplex*)w.spec));
+    // (y, z) transforms by the fused cluster kernels or cuFFT; x transform, filter and inverse x
+    // transform in one kernel
+    const bool yz = sizeof(T) == 4 && fft_yz_on(p);
+    if (yz) {
+      FD3_TRY(launch_yz_forward(mg, p->S * p->R, mg.fft_yz, (const float*)w.rho, w.spec, s));
+    } else {
+      FD3_CUFFT(cufftSetStream(p->fwd2, s));
+      FD3_CUFFT(cufftSetWorkArea(p->fwd2, w.fftw));
+      if (sizeof(T) == 8)
+        FD3_CUFFT(cufftExecD2Z(p->fwd2, (cufftDoubleReal*)w.rho, (cufftDoubleComplex*)w.spec));
+      else
+        FD3_CUFFT(cufftExecR2C(p->fwd2, (cufftReal*)w.rho, (cufftComplex*)w.spec));
+    }
     prof_mark(p, s, "fft_r2c");
     if (sizeof(T) == 4) FD3_TRY(launch_green_table(mg, w.ci, p->d_green, p->d_tab, w.gtab, s));
     if (tma_x) {
@@ -763,12 +787,16 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
     prof_mark(p, s, "filter");
     *n_mcell = 0;
     if (!need_grad) return FD3_OK;
-    FD3_CUFFT(cufftSetStream(p->inv2, s));
-    FD3_CUFFT(cufftSetWorkArea(p->inv2, w.fftw));
-    if (sizeof(T) == 8)
-      FD3_CUFFT(cufftExecZ2D(p->inv2, (cufftDoubleComplex*)w.spec, (cufftDoubleReal*)w.rho));
-    else
-      FD3_CUFFT(cufftExecC2R(p->inv2, (cufftComplex*)w.spec, (cufftReal*)w.rho));
+    if (yz) {
+      FD3_TRY(launch_yz_inverse(mg, p->S * p->R, mg.fft_yz, w.spec, (float*)w.rho, s));
+    } else {
+      FD3_CUFFT(cufftSetStream(p->inv2, s));
+      FD3_CUFFT(cufftSetWorkArea(p->inv2, w.fftw));
+      if (sizeof(T) == 8)
+        FD3_CUFFT(cufftExecZ2D(p->inv2, (cufftDoubleComplex*)w.spec, (cufftDoubleReal*)w.rho));
+      else
+        FD3_CUFFT(cufftExecC2R(p->inv2, (cufftComplex*)w.spec, (cufftReal*)w.rho));
+    }
     prof_mark(p, s, "fft_c2r");
     FD3_TRY(launch_gather<T>(mg, N, pos, ps, species, w.c6, w.dc6, w.ci, p->d_tab, w.morder, w.mstart, w.rec,
                              (const T*)w.rho, w.gcn, gpos, mcell, n_mcell, s));

@@ -188,13 +188,14 @@ class Engine:
     _KNOBS = {"filter_kt": _native.TUNE_FILTER_KT, "spread_zc": _native.TUNE_SPREAD_ZC,
               "spread_cap": _native.TUNE_SPREAD_CAP, "fft_x": _native.TUNE_FFT_X,
               "xpencil": _native.TUNE_XPENCIL, "xq": _native.TUNE_XQ, "xranks": _native.TUNE_XRANKS,
-              "filter_mma": _native.TUNE_FILTER_MMA, "gather_tile": _native.TUNE_GATHER_TILE}
+              "filter_mma": _native.TUNE_FILTER_MMA, "gather_tile": _native.TUNE_GATHER_TILE,
+              "fft_yz": _native.TUNE_FFT_YZ}
 
     def set_tuning(self, filter_kt: Optional[int] = None, spread_zc: Optional[int] = None,
                    spread_cap: Optional[int] = None, fft_x: Optional[int] = None,
                    xpencil: Optional[int] = None, xq: Optional[int] = None,
                    xranks: Optional[int] = None, filter_mma: Optional[int] = None,
-                   gather_tile: Optional[int] = None) -> None:
+                   gather_tile: Optional[int] = None, fft_yz: Optional[int] = None) -> None:
         """Launch-shape knobs (results agree to rounding): ``filter_kt`` = k-points per filter
         tile, ``spread_zc`` = z-tiles per column chunk of the spread, ``spread_cap`` = staged
         atoms per chunk at most, ``fft_x`` = 0 (3D cuFFT around the filter), 1 (2D cuFFT and the
@@ -204,10 +205,12 @@ class Engine:
         ``filter_mma`` = 1 (mixed precision: the per-k-point species products of the separate
         filter on the tensor cores) or 0 (CUDA cores), ``gather_tile`` = 1 (one CTA per mesh
         tile and species stages the tile's potential box once by TMA) or 0 (warp per atom reading
-        the mesh directly); -1 (0 for the cap) restores a default."""
+        the mesh directly), ``fft_yz`` = 1 or 2 (mixed precision, x-pass paths, ny = nz = 256:
+        the (y, z) plane transforms by this library's cluster kernels, one pass each way, on
+        clusters of 2 or 4 CTAs) or 0 (cuFFT); -1 (0 for the cap) restores a default."""
         for name, val in (("filter_kt", filter_kt), ("spread_zc", spread_zc), ("spread_cap", spread_cap),
                           ("fft_x", fft_x), ("xpencil", xpencil), ("xq", xq), ("xranks", xranks),
-                          ("filter_mma", filter_mma), ("gather_tile", gather_tile)):
+                          ("filter_mma", filter_mma), ("gather_tile", gather_tile), ("fft_yz", fft_yz)):
             if val is not None:
                 _native.check(_native.lib().fd3_plan_set_tuning(self._plan, self._KNOBS[name], int(val)),
                               "fd3_plan_set_tuning")

@@ -117,6 +117,11 @@ FD3_API int fd3_plan_destroy(fd3_plan* plan);
  *                       the tile's potential box once by TMA (at most 8 ranks, the box within
  *                       113 KB of shared memory); 0 or -1 (the default) = warp per atom reading
  *                       the mesh directly (faster unless a tile holds many atoms per species).
+ *   FD3_TUNE_FFT_YZ     mixed precision with the fused x-pass (FD3_TUNE_FFT_X = 1 or 2) and
+ *                       ny = nz = 256: 1 or 2 = the (y, z) plane transforms by this library's
+ *                       cluster kernels (one pass over the mesh each way instead of cuFFT's
+ *                       two; 1: clusters of 2 CTAs, one per SM; 2: clusters of 4, two per SM);
+ *                       0 = cuFFT; -1 = the default (0).
  * fd3_plan_get_tuning returns the value in effect (the default resolved). */
 #define FD3_TUNE_FILTER_KT 0
 #define FD3_TUNE_SPREAD_ZC 1
@@ -127,6 +132,7 @@ FD3_API int fd3_plan_destroy(fd3_plan* plan);
 #define FD3_TUNE_XRANKS 6
 #define FD3_TUNE_FILTER_MMA 7
 #define FD3_TUNE_GATHER_TILE 8
+#define FD3_TUNE_FFT_YZ 9
 FD3_API int fd3_plan_set_tuning(fd3_plan* plan, int32_t knob, int32_t value);
 FD3_API int fd3_plan_get_tuning(const fd3_plan* plan, int32_t knob, int32_t* value);
 

@@ -301,3 +301,45 @@ def test_tile_gather_knob_bounds(cuda_device):
     assert m.engine.tuning()["gather_tile"] == 0
     with pytest.raises(ValueError):
         m.engine.set_tuning(gather_tile=2)
+
+
+@pytest.mark.parametrize("fft_x,variant", [(2, 1), (2, 2), (1, 2)])
+def test_fused_yz_transforms_agree_with_cufft(fft_x, variant, cuda_device):
+    """The fused (y, z) plane transforms (clusters of 2 or 4 CTAs sharing each 256 x 256 plane
+    through distributed shared memory, one pass over the mesh each way) give cuFFT's energy,
+    forces and stress to float rounding, under the TMA x-pass (fft_x=2, the benchmarked knobs)
+    and the cp.async x-pass (fft_x=1): the 41,472-atom SiO2 replica, 256^3 mesh, mixed precision.
+    The energy is checked against the float64 form as well, at the mixed form's tolerance."""
+    from fourierd3_b200 import D3Model, structures as st
+
+    pos, cell, z = st.sio2_scaled(4)
+    m = D3Model(z, cell, precision="mixed", device=cuda_device, **KW)
+    knobs = dict(fft_x=2, xq=4, xranks=4) if fft_x == 2 else dict(fft_x=1)
+    m.engine.set_tuning(fft_yz=0, **knobs)
+    assert m.engine.tuning()["fft_yz"] == 0
+    e0, f0, s0 = (t.clone() for t in m(pos, cell))
+    m.engine.set_tuning(fft_yz=variant)
+    assert m.engine.tuning()["fft_yz"] == variant
+    e, f, s = m(pos, cell)
+    assert abs(float(e) - float(e0)) <= 2e-7 * abs(float(e0)), (float(e), float(e0))
+    assert (f - f0).abs().max().item() <= 5e-6
+    assert (s - s0).abs().max().item() <= 5e-8
+    m64 = D3Model(z, cell, precision="fp64", device=cuda_device, **KW)
+    e64, f64, s64 = m64(pos, cell)
+    assert abs(float(e) - float(e64)) <= 1e-6 * abs(float(e64))
+    assert (f - f64).abs().max().item() <= 1e-4
+    # deterministic: no atomics in either transform
+    e2, f2, s2 = m(pos, cell)
+    assert float(e2) == float(e) and torch.equal(f2, f) and torch.equal(s2, s)
+
+
+def test_fused_yz_transforms_where_they_apply(cuda_device):
+    """In effect only with the x-pass, mixed precision and a 256 x 256 (y, z) plane."""
+    from fourierd3_b200 import D3Model, structures as st
+
+    pos, cell, z = st.sio2_box(0)                      # 64^3 mesh
+    m = D3Model(z, cell, precision="mixed", device=cuda_device, **KW)
+    m.engine.set_tuning(fft_yz=1, fft_x=2)
+    assert m.engine.tuning()["fft_yz"] == 0
+    with pytest.raises(ValueError):
+        m.engine.set_tuning(fft_yz=3)

@@ -370,8 +370,10 @@ def autotune_fft_x(batch: "D3Batch", pencils: Sequence[int] = (1, 2, 4), reps: i
     ``pencils`` kz values of every channel ("1/<kz>"), or TMA-moved units of (q values, ranks)
     from ``tma_units`` ("2/<q>/<ranks>", mixed precision), by the summed time of the forward
     transform, filter and inverse transform stages of the plan's heaviest structure. Plans where
-    no fused path applies keep "0". Returns {plan index: (choice, {choice: ms})}. Drops a
-    captured graph."""
+    no fused path applies keep "0". On an x-pass path with 256 x 256 (y, z) planes it then times
+    the (y, z) transforms as cluster kernels on pairs (the default), with the forward on quads
+    ("<choice>/yz2") and by cuFFT ("<choice>/yz0"), and keeps the fastest. Returns
+    {plan index: (choice, {choice: ms})}. Drops a captured graph."""
     batch._graph = None
     heaviest: dict = {}
     for i, key in enumerate(batch._keys):
@@ -403,6 +405,15 @@ def autotune_fft_x(batch: "D3Batch", pencils: Sequence[int] = (1, 2, 4), reps: i
             eng.set_tuning(fft_x=1, xpencil=int(parts[1]))
         else:
             eng.set_tuning(fft_x=2, xq=int(parts[1]), xranks=int(parts[2]))
+        if best != "0" and eng.tuning()["fft_yz"] > 0:
+            # the (y, z) transforms of the chosen x-pass path: cluster kernels (pairs, the
+            # default; the forward on quads) or cuFFT
+            yz_times = {1: times[best]}
+            for v in (2, 0):
+                eng.set_tuning(fft_yz=v)
+                yz_times[v] = _profiled_stage(batch, i, stages, reps)
+                times[f"{best}/yz{v}"] = yz_times[v]
+            eng.set_tuning(fft_yz=min(yz_times, key=yz_times.get))
         out[n] = (best, times)
     return out
 

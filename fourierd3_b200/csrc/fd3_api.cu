@@ -387,9 +387,11 @@ static bool xpass_on(const fd3_plan* p) {
 }
 // fused (y, z) transforms in effect: float mesh on a 2D-transform path, ny = nz = 256, asked for
 static bool fft_yz_on(const fd3_plan* p) {
-  return p->precision == FD3_PREC_MIXED && p->method != FD3_METHOD_EWALD && p->mg.fft_yz >= 1 &&
+  return p->precision == FD3_PREC_MIXED && p->method != FD3_METHOD_EWALD && p->mg.fft_yz != 0 &&
          yzfft_applies(p->mg);
 }
+// cluster shape of the fused (y, z) forward transform: the knob, or pairs by default
+static int yz_variant(const fd3_plan* p) { return p->mg.fft_yz > 0 ? p->mg.fft_yz : 1; }
 static bool old_xpass_on(const fd3_plan* p) {
   return p->method != FD3_METHOD_EWALD && p->has_fft2 && p->mg.fft_x == 1 &&
          xfilter_pencil(p->mg, p->precision == FD3_PREC_FP64 ? 1 : 0) > 0;
@@ -524,7 +526,7 @@ extern "C" int fd3_plan_get_tuning(const fd3_plan* p, int32_t knob, int32_t* val
     return FD3_OK;
   }
   if (knob == FD3_TUNE_FFT_YZ) {
-    *value = (xpass_on(p) || old_xpass_on(p)) && fft_yz_on(p) ? p->mg.fft_yz : 0;
+    *value = (xpass_on(p) || old_xpass_on(p)) && fft_yz_on(p) ? yz_variant(p) : 0;
     return FD3_OK;
   }
   if (knob == FD3_TUNE_GATHER_TILE) {
@@ -764,7 +766,7 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
     // transform in one kernel
     const bool yz = sizeof(T) == 4 && fft_yz_on(p);
     if (yz) {
-      FD3_TRY(launch_yz_forward(mg, p->S * p->R, mg.fft_yz, (const float*)w.rho, w.spec, s));
+      FD3_TRY(launch_yz_forward(mg, p->S * p->R, yz_variant(p), (const float*)w.rho, w.spec, s));
     } else {
       FD3_CUFFT(cufftSetStream(p->fwd2, s));
       FD3_CUFFT(cufftSetWorkArea(p->fwd2, w.fftw));
@@ -788,7 +790,7 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
     *n_mcell = 0;
     if (!need_grad) return FD3_OK;
     if (yz) {
-      FD3_TRY(launch_yz_inverse(mg, p->S * p->R, mg.fft_yz, w.spec, (float*)w.rho, s));
+      FD3_TRY(launch_yz_inverse(mg, p->S * p->R, yz_variant(p), w.spec, (float*)w.rho, s));
     } else {
       FD3_CUFFT(cufftSetStream(p->inv2, s));
       FD3_CUFFT(cufftSetWorkArea(p->inv2, w.fftw));

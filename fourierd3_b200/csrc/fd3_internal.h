@@ -145,7 +145,7 @@ struct MeshGeom {
   int xranks;     // TMA x-pass: ranks per unit (1, 2, 4), -1 default
   int filter_mma; // float spectrum: 1 tensor-core (tcgen05) filter where it applies, 0 CUDA cores, -1 default
   int gather_tile; // fused-path gather: 1 tile-staged TMA gather where it applies, 0 or -1 (default) per-atom
-  int fft_yz;      // float mesh, 2D-transform paths: fused (y, z) cluster kernels (1 pairs, 2 quads), 0 cuFFT, -1 default
+  int fft_yz;      // float mesh, 2D-transform paths: fused (y, z) cluster kernels (1 pairs, 2 quad forward), 0 cuFFT, -1 default (1)
   const float* win_axes;  // SPME, mixed form: sinc(m/n)^(2p) per axis, [nx | ny | nz/2+1] (null: none)
 };
 // h_expect (optional, host, copied into the launch): the cell the caller's host-side geometry (cell
@@ -168,7 +168,8 @@ struct MeshRecords {
 // Fused (y, z) plane transforms of the float mesh (ny = nz = 256; planes = nchannels x nx, the
 // layouts of the batched 2D cuFFT R2C / C2R they replace).
 bool yzfft_applies(const MeshGeom& mg);
-// variant 1: clusters of 2 CTAs (one per SM); 2: clusters of 4 (two per SM).
+// variant 1: clusters of 2 CTAs (one per SM); 2: the forward on clusters of 4 (two per SM), the
+// inverse on pairs.
 int launch_yz_forward(const MeshGeom& mg, int nchannels, int variant, const float* rho, void* spec,
                       cudaStream_t s);
 int launch_yz_inverse(const MeshGeom& mg, int nchannels, int variant, const void* spec, float* rho,

@@ -449,8 +449,8 @@ __global__ void __launch_bounds__(YzCfg<CL>::kThreads, YzCfg<CL>::kMinBlocks)
 }
 
 template <int CL>
-int launch_yz(const void* kern, int which, void** args, int nplanes, cudaStream_t s, const char* what) {
-  const size_t smem = sizeof(YzSmem<CL>) + 128;
+int launch_yz(const void* kern, int which, int threads, size_t smem, void** args, int nplanes, cudaStream_t s,
+              const char* what) {
   static unsigned attr_set[2] = {0, 0};   // per kernel, one bit per device (set every call past 32)
   int dev = 0;
   cudaGetDevice(&dev);
@@ -468,7 +468,7 @@ int launch_yz(const void* kern, int which, void** args, int nplanes, cudaStream_
   attr[0].val.clusterDim.x = CL;
   attr[0].val.clusterDim.y = 1;
   attr[0].val.clusterDim.z = 1;
-  cfg.blockDim = dim3(YzCfg<CL>::kThreads);
+  cfg.blockDim = dim3(threads);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cfg.attrs = attr;
@@ -494,7 +494,8 @@ int launch_yz(const void* kern, int which, void** args, int nplanes, cudaStream_
 
 bool yzfft_applies(const MeshGeom& mg) { return mg.n[1] == kYzN && mg.n[2] == kYzN; }
 
-// variant: 1 = clusters of 2 CTAs (one per SM), 2 = clusters of 4 (two per SM)
+// variant: 1 = clusters of 2 CTAs (one per SM), 2 = clusters of 4 (two per SM) for the forward
+// transform; the inverse always runs on pairs
 int launch_yz_forward(const MeshGeom& mg, int nchannels, int variant, const float* rho, void* spec,
                       cudaStream_t s) {
   if (!yzfft_applies(mg) || nchannels < 1 || (variant != 1 && variant != 2)) return FD3_EINVAL;
@@ -504,8 +505,11 @@ int launch_yz_forward(const MeshGeom& mg, int nchannels, int variant, const floa
   float2* out = reinterpret_cast<float2*>(spec);
   int n = (int)np;
   void* args[3] = {&in, &out, &n};
-  if (variant == 1) return launch_yz<2>(reinterpret_cast<const void*>(k_yz_forward<2>), 0, args, n, s, "fft_r2c");
-  return launch_yz<4>(reinterpret_cast<const void*>(k_yz_forward<4>), 0, args, n, s, "fft_r2c");
+  if (variant == 1)
+    return launch_yz<2>(reinterpret_cast<const void*>(k_yz_forward<2>), 0, YzCfg<2>::kThreads,
+                        sizeof(YzSmem<2>) + 128, args, n, s, "fft_r2c");
+  return launch_yz<4>(reinterpret_cast<const void*>(k_yz_forward<4>), 0, YzCfg<4>::kThreads, sizeof(YzSmem<4>) + 128,
+                      args, n, s, "fft_r2c");
 }
 
 int launch_yz_inverse(const MeshGeom& mg, int nchannels, int variant, const void* spec, float* rho,
@@ -517,8 +521,9 @@ int launch_yz_inverse(const MeshGeom& mg, int nchannels, int variant, const void
   float* out = rho;
   int n = (int)np;
   void* args[3] = {&in, &out, &n};
-  if (variant == 1) return launch_yz<2>(reinterpret_cast<const void*>(k_yz_inverse<2>), 1, args, n, s, "fft_c2r");
-  return launch_yz<4>(reinterpret_cast<const void*>(k_yz_inverse<4>), 1, args, n, s, "fft_c2r");
+  (void)variant;   // the inverse runs on pairs for both variants (quads measured slower)
+  return launch_yz<2>(reinterpret_cast<const void*>(k_yz_inverse<2>), 1, YzCfg<2>::kThreads, sizeof(YzSmem<2>) + 128,
+                      args, n, s, "fft_c2r");
 }
 
 }  // namespace fd3

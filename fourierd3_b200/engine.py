@@ -206,8 +206,9 @@ class Engine:
         filter on the tensor cores) or 0 (CUDA cores), ``gather_tile`` = 1 (one CTA per mesh
         tile and species stages the tile's potential box once by TMA) or 0 (warp per atom reading
         the mesh directly), ``fft_yz`` = 1 or 2 (mixed precision, x-pass paths, ny = nz = 256:
-        the (y, z) plane transforms by this library's cluster kernels, one pass each way, on
-        clusters of 2 or 4 CTAs) or 0 (cuFFT); -1 (0 for the cap) restores a default."""
+        the (y, z) plane transforms by this library's cluster kernels, one pass each way, the
+        forward on clusters of 2 or 4 CTAs; the default) or 0 (cuFFT); -1 (0 for the cap)
+        restores a default."""
         for name, val in (("filter_kt", filter_kt), ("spread_zc", spread_zc), ("spread_cap", spread_cap),
                           ("fft_x", fft_x), ("xpencil", xpencil), ("xq", xq), ("xranks", xranks),
                           ("filter_mma", filter_mma), ("gather_tile", gather_tile), ("fft_yz", fft_yz)):

@@ -120,8 +120,8 @@ FD3_API int fd3_plan_destroy(fd3_plan* plan);
  *   FD3_TUNE_FFT_YZ     mixed precision with the fused x-pass (FD3_TUNE_FFT_X = 1 or 2) and
  *                       ny = nz = 256: 1 or 2 = the (y, z) plane transforms by this library's
  *                       cluster kernels (one pass over the mesh each way instead of cuFFT's
- *                       two; 1: clusters of 2 CTAs, one per SM; 2: clusters of 4, two per SM);
- *                       0 = cuFFT; -1 = the default (0).
+ *                       two; 1: clusters of 2 CTAs, one per SM; 2: the forward transform on
+ *                       clusters of 4, two per SM); 0 = cuFFT; -1 = the default (1).
  * fd3_plan_get_tuning returns the value in effect (the default resolved). */
 #define FD3_TUNE_FILTER_KT 0
 #define FD3_TUNE_SPREAD_ZC 1

@@ -315,7 +315,9 @@ def test_fused_yz_transforms_agree_with_cufft(fft_x, variant, cuda_device):
     pos, cell, z = st.sio2_scaled(4)
     m = D3Model(z, cell, precision="mixed", device=cuda_device, **KW)
     knobs = dict(fft_x=2, xq=4, xranks=4) if fft_x == 2 else dict(fft_x=1)
-    m.engine.set_tuning(fft_yz=0, **knobs)
+    m.engine.set_tuning(**knobs)
+    assert m.engine.tuning()["fft_yz"] == 1            # the default where it applies
+    m.engine.set_tuning(fft_yz=0)
     assert m.engine.tuning()["fft_yz"] == 0
     e0, f0, s0 = (t.clone() for t in m(pos, cell))
     m.engine.set_tuning(fft_yz=variant)

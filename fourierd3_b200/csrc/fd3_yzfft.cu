@@ -105,6 +105,10 @@ __device__ __forceinline__ void cluster_sync_all() {
 __device__ __forceinline__ void cluster_sync_exec() {
   asm volatile("barrier.cluster.arrive.relaxed;\nbarrier.cluster.wait;\n" ::: "memory");
 }
+// Bring `bytes` of global memory into L2 ahead of use (no data returned to the SM).
+__device__ __forceinline__ void prefetch_l2(const void* src, uint32_t bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;\n" ::"l"(src), "r"(bytes) : "memory");
+}
 __device__ __forceinline__ void group_bar(int g, int nthreads) {   // one half of the CTA
   asm volatile("bar.sync %0, %1;\n" ::"r"(g + 1), "r"(nthreads) : "memory");
 }
@@ -252,8 +256,13 @@ __global__ void __launch_bounds__(YzCfg<CL>::kThreads, YzCfg<CL>::kMinBlocks)
   // Z[128 - k] for this lane's Z[k] (k1 = 0 and 4 pair within the lane)
   const int r2 = lane >> 3, k1 = lane & 7;
   const int partner = (lane & ~7) | ((8 - k1) & 7);
+  constexpr uint32_t kShare = (uint32_t)(C::kRows * kYzN * 4);   // this CTA's rows of a plane
   for (int i = 0; i < nmine; ++i) {
     const int plane = cid + i * ncl;
+    // the next plane's rows into L2 while this one is transformed (its first chunks follow by
+    // bulk copy as soon as this plane's last ones are consumed)
+    if (tid == 0 && i + 1 < nmine)
+      prefetch_l2(rho + ((size_t)(plane + ncl) * kYzN + C::kRows * q) * kYzN, kShare);
     // ---- z transforms of this CTA's rows, scattered to the column owners
     for (int sub = g; sub < 4; sub += 2) {
       const int j = 4 * i + sub, s = j & 1;
@@ -364,8 +373,15 @@ __global__ void __launch_bounds__(YzCfg<CL>::kThreads, YzCfg<CL>::kMinBlocks)
   auto xaddr = [&](int kz, uint32_t yr) {
     return map_rank(b_local, (uint32_t)(kz >> C::kLogCols)) + (yr + (uint32_t)(kz & (C::kCols - 1))) * 8u;
   };
+  // each CTA's share of a plane's spectrum (a multiple of 16 bytes: 256 129 8 / CL)
+  constexpr uint32_t kShare = (uint32_t)(kYzN * kYzH * 8 / CL);
+  if (tid == 0 && nmine > 0)
+    prefetch_l2(reinterpret_cast<const char*>(spec + (size_t)cid * kYzN * kYzH) + q * kShare, kShare);
   for (int i = 0; i < nmine; ++i) {
     const int plane = cid + i * ncl;
+    // the next plane's spectrum into L2 while this one is transformed
+    if (tid == 0 && i + 1 < nmine)
+      prefetch_l2(reinterpret_cast<const char*>(spec + (size_t)(plane + ncl) * kYzN * kYzH) + q * kShare, kShare);
     // ---- inverse y transforms of this CTA's columns, pass 1 straight from the spectrum
     const float2* in = spec + (size_t)plane * kYzN * kYzH;
     for (int it = tid; it < C::kCols * 16; it += C::kThreads) {

@@ -385,10 +385,13 @@ struct BinStage {
 
 // Returns the number of staged candidates, or -1 when the neighbourhood does not fit; org is the
 // origin subtracted from the staged positions (zero for double4).
+// rcov: when given, the staged w component is the candidate's covalent radius rcov[species]
+// (the CN kernel's only use of the species) instead of the species index.
 template <typename P4>
 __device__ int stage_bin(const GridDev& g, int b, const int* __restrict__ bin_start,
                          const double4* __restrict__ xs, const int4* __restrict__ meta, BinStage<P4>& st,
-                         double* __restrict__ s_g, const double* __restrict__ gcn, double (&org)[3]) {
+                         double* __restrict__ s_g, const double* __restrict__ gcn, double (&org)[3],
+                         const double* __restrict__ rcov = nullptr) {
   const int nx = 2 * g.reach[0] + 1, ny = 2 * g.reach[1] + 1, nz = 2 * g.reach[2] + 1;
   const int nnb = nx * ny * nz;
   if (nnb > kMaxNbrBins) return -1;
@@ -412,7 +415,18 @@ __device__ int stage_bin(const GridDev& g, int b, const int* __restrict__ bin_st
     st.img[e][2] = sz;
   }
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (nnb <= 32) {   // one warp scans the bin sizes (27 bins at reach 1)
+    if (threadIdx.x < 32) {
+      int v = threadIdx.x < nnb ? st.pref[threadIdx.x + 1] : 0;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int u = __shfl_up_sync(0xffffffffu, v, o);
+        if ((int)threadIdx.x >= o) v += u;
+      }
+      if ((int)threadIdx.x < nnb) st.pref[threadIdx.x + 1] = v;
+      if (threadIdx.x == 0) st.pref[0] = 0;
+    }
+  } else if (threadIdx.x == 0) {
     st.pref[0] = 0;
     for (int e = 0; e < nnb; ++e) st.pref[e + 1] += st.pref[e];
   }
@@ -432,10 +446,11 @@ __device__ int stage_bin(const GridDev& g, int b, const int* __restrict__ bin_st
     const double px = xj.x + S0 * g.cell[0] + S1 * g.cell[3] + S2 * g.cell[6];
     const double py = xj.y + S0 * g.cell[1] + S1 * g.cell[4] + S2 * g.cell[7];
     const double pz = xj.z + S0 * g.cell[2] + S1 * g.cell[5] + S2 * g.cell[8];
+    const double wv = rcov ? rcov[(int)xj.w] : xj.w;
     if constexpr (sizeof(P4) == sizeof(double4))
-      st.p[c] = make_double4(px, py, pz, xj.w);
+      st.p[c] = make_double4(px, py, pz, wv);
     else
-      st.p[c] = make_float4((float)(px - org[0]), (float)(py - org[1]), (float)(pz - org[2]), (float)xj.w);
+      st.p[c] = make_float4((float)(px - org[0]), (float)(py - org[1]), (float)(pz - org[2]), (float)wv);
     st.j[c] = mj.w;
     if (s_g) s_g[c] = gcn[mj.w];
   }
@@ -491,7 +506,7 @@ __device__ __forceinline__ void cn_hit(const BinStage<typename StagePos<TC>::typ
   const TC r2 = v0 * v0 + v1 * v1 + v2 * v2;
   TC f = TC(0), a = TC(0);
   if (r2 > TC(1e-12)) {
-    cn_pair<TC>(r2, rci + (TC)tab->rcov[(int)pj.w], rc, f, a);
+    cn_pair<TC>(r2, rci + (TC)pj.w, rc, f, a);   // pj.w: the neighbour's covalent radius
     acc += f;
   }
   if (h < hl.cap) {
@@ -511,7 +526,7 @@ __global__ void __launch_bounds__(256) k_cn_bins(GridDev g, const int* __restric
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int b = blockIdx.x;
   double org[3];
-  const int total = stage_bin<P4>(g, b, bin_start, xs, meta, st, nullptr, nullptr, org);
+  const int total = stage_bin<P4>(g, b, bin_start, xs, meta, st, nullptr, nullptr, org, tab->rcov);
   const int s0 = bin_start[b], s1 = bin_start[b + 1];
   if (total < 0) {
     for (int t = s0 + threadIdx.x; t < s1; t += blockDim.x) hl.n[t] = -2;

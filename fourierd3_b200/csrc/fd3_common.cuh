@@ -153,7 +153,14 @@ __device__ __forceinline__ void sincospi_t(float x, float* s, float* c) {
   *s = (q & 2) ? -so : so;
   *c = ((q + 1) & 2) ? -co : co;
 }
-__device__ __forceinline__ float rcp_t(float x) { return __frcp_rn(x); }
+// float: the hardware reciprocal (rcp.approx, at most 1 ulp from the correctly rounded value;
+// callers pass normal, positive arguments) -- the mixed form's CN pair function takes two per
+// pair, where the correctly rounded reciprocal costs an instruction sequence each
+__device__ __forceinline__ float rcp_t(float x) {
+  float r;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
 
 // The same CN edge function from the squared distance r2 > 1e-12 Bohr^2 (the reference zeroes
 // r <= 1e-6): f and a = f'(r) / r with one reciprocal square root and two reciprocals.

@@ -99,6 +99,7 @@ class D3Batch:
         self.n_struct = len(structures)
         self._engines: dict = {}
         self._graph = None
+        self._graph_host = None
         counts, cells, species, setups, keys, costs = [], [], [], [], [], []
         for pos, cell, numbers in structures:
             pos = np.asarray(pos, dtype=np.float64)
@@ -134,9 +135,14 @@ class D3Batch:
         self.species = torch.from_numpy(np.concatenate(species).astype(np.int32)).to(dev)
         self.cells_host = np.stack(cells)
         self.cells = torch.from_numpy(self.cells_host.reshape(-1, 9).copy()).to(dev)
-        self.energy = torch.zeros((self.n_struct,), dtype=torch.float64, device=dev)
-        self.forces = torch.zeros((total, 3), dtype=torch.float64, device=dev)
-        self.stress = torch.zeros((self.n_struct, 3, 3), dtype=torch.float64, device=dev)
+        # one flat output buffer [energy (B) | stress (B, 3, 3) | forces (N, 3)] so that a host
+        # read of every result is a single copy
+        B = self.n_struct
+        self._out = torch.zeros(10 * B + 3 * total, dtype=torch.float64, device=dev)
+        self.energy = self._out[:B]
+        self.stress = self._out[B:10 * B].view(B, 3, 3)
+        self.forces = self._out[10 * B:].view(total, 3)
+        self._host = None   # pinned host buffers of the host-I/O graph (positions, outputs)
         self._keys = keys
         self._need = [self._engines[k].workspace_bytes(counts[i], cells[i], self.r_cut)
                       for i, k in enumerate(keys)]
@@ -150,6 +156,7 @@ class D3Batch:
         if lanes == self.lanes:
             return
         self._graph = None
+        self._graph_host = None
         self._work = None
         torch.cuda.synchronize(self.device)
         split = lpt_split(self.costs, lanes)
@@ -193,8 +200,14 @@ class D3Batch:
             main.wait_event(ev)
 
     # ------------------------------------------------------------------ graph
-    def capture(self) -> None:
-        """Record the whole batch (all lanes) as one CUDA graph; later calls replay it."""
+    def capture(self, host_io: bool = False) -> None:
+        """Record the whole batch (all lanes) as one CUDA graph; later calls replay it.
+
+        host_io: record a second graph (replayed by ``run_host``) that also copies the positions in from the pinned host buffer of
+        ``host_buffers()`` and every result out to it (one copy each way), so that one replay
+        (``run_host``) is a whole evaluation from host memory to host memory."""
+        if host_io:
+            self.host_buffers()
         side = torch.cuda.Stream(self.device)
         side.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(side):
@@ -203,9 +216,40 @@ class D3Batch:
         torch.cuda.synchronize(self.device)
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
+            if host_io:
+                self.positions.copy_(self._host["pos"], non_blocking=True)
             self._launch_all()
+            if host_io:
+                self._host["out"].copy_(self._out, non_blocking=True)
         torch.cuda.synchronize(self.device)
-        self._graph = g
+        if host_io:
+            self._graph_host = g
+        else:
+            self._graph = g
+
+    def host_buffers(self) -> dict:
+        """Pinned host buffers for host-to-host evaluation: ``positions`` (sum N, 3) read by the
+        host-I/O graph, and ``energy`` (B,), ``stress`` (B, 3, 3), ``forces`` (sum N, 3) that it
+        writes (views of one pinned buffer)."""
+        if self._host is None:
+            pos = torch.empty(tuple(self.positions.shape), dtype=torch.float64).pin_memory()
+            pos.copy_(self.positions.cpu())
+            out = torch.zeros(self._out.shape, dtype=torch.float64).pin_memory()
+            B, total = self.n_struct, int(self.positions.shape[0])
+            self._host = {"pos": pos, "out": out, "positions": pos, "energy": out[:B],
+                          "stress": out[B:10 * B].view(B, 3, 3), "forces": out[10 * B:].view(total, 3)}
+        return self._host
+
+    def run_host(self):
+        """One evaluation from the pinned host positions to the pinned host results (a single
+        graph replay with both copies inside; captures with host_io=True first if needed). The
+        results are valid once the current stream has been synchronised. Returns the host
+        (energy, forces, stress) views."""
+        if getattr(self, "_graph_host", None) is None:
+            self.capture(host_io=True)
+        self._graph_host.replay()
+        h = self._host
+        return h["energy"], h["forces"], h["stress"]
 
     @property
     def captured(self) -> bool:
@@ -306,6 +350,7 @@ def autotune_filter(batch: "D3Batch", candidates: Sequence = (0, 1, 2, 4, 8, 16,
     is valid. Returns {class: (choice, {choice: ms})}. Drops a captured graph.
     """
     batch._graph = None
+    batch._graph_host = None
     classes: dict = {}
     for i, key in enumerate(batch._keys):
         s = len(key[0])
@@ -344,6 +389,7 @@ def autotune_spread(batch: "D3Batch", candidates: Sequence[int] = (0, 2, 4, 8, 1
     plan: every candidate is timed (profiled eager calls) and the fastest is set on that plan.
     Returns {plan index: (chunk, {chunk: ms})}. Drops a captured graph."""
     batch._graph = None
+    batch._graph_host = None
     heaviest: dict = {}
     for i, key in enumerate(batch._keys):
         if key not in heaviest or batch.costs[i] > batch.costs[heaviest[key]]:
@@ -375,6 +421,7 @@ def autotune_fft_x(batch: "D3Batch", pencils: Sequence[int] = (1, 2, 4), reps: i
     ("<choice>/yz2") and by cuFFT ("<choice>/yz0"), and keeps the fastest. Returns
     {plan index: (choice, {choice: ms})}. Drops a captured graph."""
     batch._graph = None
+    batch._graph_host = None
     heaviest: dict = {}
     for i, key in enumerate(batch._keys):
         if key not in heaviest or batch.costs[i] > batch.costs[heaviest[key]]:

@@ -6,6 +6,8 @@
 * one structure of the batch matches the float64 oracle (energy 1e-10 relative, forces
   1e-8 eV/A, stress 1e-10 eV/A^3), so the batch path inherits the drop-in parity;
 * positions updated in place are picked up by a graph replay;
+* the host-I/O graph (run_host: positions copied in and results out inside one replay) equals
+  the device path bit for bit;
 * the lane autotuner picks one of its candidates and writes its cache.
 """
 import json
@@ -89,6 +91,37 @@ def test_replay_sees_new_positions(cuda_device):
         assert torch.equal(e[i], e1)
         assert torch.equal(b.split_forces()[i], f1)
         assert torch.equal(s[i], s1)
+
+
+def test_run_host_matches_device_call(cuda_device):
+    """run_host (one graph replay with the host positions copied in and every result copied out)
+    gives the device-path results bit for bit, picks up new host positions, and leaves the
+    device-I/O graph (__call__) reading the device positions."""
+    from fourierd3_b200.batch import D3Batch
+
+    structs = _structures(n=5)
+    b = D3Batch(structs, precision="mixed", lanes=2, device=cuda_device, **KW)
+    b.capture()
+    e0, f0, s0 = (t.clone() for t in b())
+    h = b.host_buffers()
+    assert h["positions"].is_pinned() and h["forces"].is_pinned()
+    e, f, s = b.run_host()
+    torch.cuda.synchronize()
+    assert torch.equal(e, e0.cpu()) and torch.equal(f, f0.cpu()) and torch.equal(s, s0.cpu())
+    rng = np.random.default_rng(5)
+    moved = np.concatenate([p + rng.normal(0.0, 0.02, p.shape) for p, _, _ in structs])
+    h["positions"].copy_(torch.from_numpy(moved))
+    e2, f2, s2 = b.run_host()
+    torch.cuda.synchronize()
+    ed, fd, sd = (t.cpu() for t in b(torch.from_numpy(moved)))
+    torch.cuda.synchronize()
+    assert torch.equal(e2, ed) and torch.equal(f2, fd) and torch.equal(s2, sd)
+    assert not torch.equal(e2, e0.cpu())
+    # the device-I/O graph still follows the device positions
+    back = torch.from_numpy(np.concatenate([p for p, _, _ in structs]))
+    e3, _, _ = b(back)
+    torch.cuda.synchronize()
+    assert torch.equal(e3, e0)
 
 
 def test_autotune_lanes_caches(tmp_path, cuda_device):

@@ -226,6 +226,7 @@ extern "C" int fd3_plan_create(const fd3_plan_desc* d, fd3_plan** out) {
       m.filter_mma = -1;
       m.gather_tile = -1;
       m.fft_yz = -1;
+      m.qpitch = 0;
       m.fft_x = -1;   // default: off (3D cuFFT around the separate filter measured faster on B200)
       const size_t Mh = (size_t)m.n[0] * m.n[1] * m.nzh;
       m.win_axes = nullptr;
@@ -658,7 +659,10 @@ void carve(const fd3_plan* p, int64_t N, int64_t K_in, Carver& c, Work& w, int64
   w.hits.ovf = c.take<int>(1);
   const size_t C = (size_t)p->S * p->R;
   w.rho = c.take<char>(mesh ? C * M * es : 1);
-  w.spec = c.take<char>(mesh ? C * Mh * 2 * es : 1);
+  // the mixed form's spectrum may carry one pad slot per ky row (16-byte rows for the fused
+  // (y, z) transforms under the TMA x-pass)
+  const size_t Mh_spec = p->precision == FD3_PREC_MIXED ? Mh + (size_t)p->mg.n[0] * p->mg.n[1] : Mh;
+  w.spec = c.take<char>(mesh ? C * Mh_spec * 2 * es : 1);
   w.fftw = c.take<char>(p->fft_ws);
   w.gtab = c.take<char>(mesh && p->precision == FD3_PREC_MIXED ? green_table_bytes(p->S) : 1);
   // D4 k-space CN: density / sigma / psi, phi, the density spectrum (kept for the adjoint), the
@@ -762,11 +766,15 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
   prof_mark(p, s, "spread");
   const bool tma_x = sizeof(T) == 4 && xpass_on(p);
   if (tma_x || old_xpass_on(p)) {
+    // the TMA x-pass between the fused (y, z) transforms: ky rows of nzh + 1 values (a zero pad
+    // slot), so that the inverse transform can fetch its columns by TMA
+    MeshGeom mgq = mg;
+    mgq.qpitch = tma_x && sizeof(T) == 4 && fft_yz_on(p) && mg.nzh == 129 ? mg.nzh + 1 : mg.nzh;
     // (y, z) transforms by the fused cluster kernels or cuFFT; x transform, filter and inverse x
     // transform in one kernel
     const bool yz = sizeof(T) == 4 && fft_yz_on(p);
     if (yz) {
-      FD3_TRY(launch_yz_forward(mg, p->S * p->R, yz_variant(p), (const float*)w.rho, w.spec, s));
+      FD3_TRY(launch_yz_forward(mgq, p->S * p->R, yz_variant(p), (const float*)w.rho, w.spec, s));
     } else {
       FD3_CUFFT(cufftSetStream(p->fwd2, s));
       FD3_CUFFT(cufftSetWorkArea(p->fwd2, w.fftw));
@@ -780,7 +788,7 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
     if (tma_x) {
       int Q, RG;
       xpass_shape(p, &Q, &RG);
-      FD3_TRY(launch_xpass(mg, Q, RG, w.ci, p->d_green_f, (const float4*)w.gtab, p->d_tab, p->d_deconv,
+      FD3_TRY(launch_xpass(mgq, Q, RG, w.ci, p->d_green_f, (const float4*)w.gtab, p->d_tab, p->d_deconv,
                            p->method == FD3_METHOD_SPME, w.spec, w.kspc_part, n_kspc, s));
     } else {
       FD3_TRY(launch_xfilter<T>(mg, w.ci, p->d_green, p->d_green_f, (const float4*)w.gtab, p->d_tab, p->d_deconv,
@@ -790,7 +798,7 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
     *n_mcell = 0;
     if (!need_grad) return FD3_OK;
     if (yz) {
-      FD3_TRY(launch_yz_inverse(mg, p->S * p->R, yz_variant(p), w.spec, (float*)w.rho, s));
+      FD3_TRY(launch_yz_inverse(mgq, p->S * p->R, yz_variant(p), w.spec, (float*)w.rho, s));
     } else {
       FD3_CUFFT(cufftSetStream(p->inv2, s));
       FD3_CUFFT(cufftSetWorkArea(p->inv2, w.fftw));

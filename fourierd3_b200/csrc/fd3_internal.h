@@ -146,6 +146,8 @@ struct MeshGeom {
   int filter_mma; // float spectrum: 1 tensor-core (tcgen05) filter where it applies, 0 CUDA cores, -1 default
   int gather_tile; // fused-path gather: 1 tile-staged TMA gather where it applies, 0 or -1 (default) per-atom
   int fft_yz;      // float mesh, 2D-transform paths: fused (y, z) cluster kernels (1 pairs, 2 quad forward), 0 cuFFT, -1 default (1)
+  int qpitch;      // complex values per ky row of the half spectrum: nzh, or nzh + 1 (16-byte rows) when the
+                   // TMA x-pass and the fused (y, z) transforms share it; 0 = nzh
   const float* win_axes;  // SPME, mixed form: sinc(m/n)^(2p) per axis, [nx | ny | nz/2+1] (null: none)
 };
 // h_expect (optional, host, copied into the launch): the cell the caller's host-side geometry (cell

@@ -21,7 +21,8 @@ namespace fd3 {
 
 struct MeshDev {
   int n[3], nzh, t[3], nt[3], ns[3], S, R;
-  FastDiv div_nzh, div_ny;
+  int qpitch;   // complex values per ky row of the half spectrum (nzh or nzh + 1)
+  FastDiv div_nzh, div_ny, div_qpitch;
   const float* win_axes;
 };
 static inline MeshDev to_dev(const MeshGeom& g) {
@@ -36,6 +37,8 @@ static inline MeshDev to_dev(const MeshGeom& g) {
   d.S = g.S;
   d.R = g.R;
   d.div_nzh = make_fastdiv((uint32_t)g.nzh);
+  d.qpitch = g.qpitch > 0 ? g.qpitch : g.nzh;
+  d.div_qpitch = make_fastdiv((uint32_t)d.qpitch);
   d.div_ny = make_fastdiv((uint32_t)g.n[1]);
   d.win_axes = g.win_axes;
   return d;

@@ -29,7 +29,8 @@ bool xpass_applies(const MeshGeom& mg, int Q, int RG) {
   if (mg.n[0] != 64 && mg.n[0] != 128 && mg.n[0] != 256) return false;
   if (mg.S > 4 || RG > mg.R || (RG != 1 && RG != 2 && RG != 4)) return false;
   if (Q != 4 && Q != 8 && Q != 16 && Q != 32) return false;
-  if ((((long long)mg.n[1] * mg.nzh) & 1) != 0) return false;
+  const int qp = mg.qpitch > 0 ? mg.qpitch : mg.nzh;
+  if ((((long long)mg.n[1] * qp) & 1) != 0) return false;
   if (mg.n[0] + mg.n[1] + mg.nzh > 1024) return false;   // the per-axis window's shared-memory slot
   // the x transform as N1 x N2 register DFTs (64: 8 x 8, 128: 8 x 16, 256: 16 x 16) and the
   // padded working copy of XpWork
@@ -38,8 +39,8 @@ bool xpass_applies(const MeshGeom& mg, int Q, int RG) {
   return xpass_stages((size_t)mg.S * RG * mg.n[0] * Q * sizeof(float2), work) >= 2;
 }
 
-// Spectrum (float2, layout (S, R, nx, ny, nz/2+1)) as a 4-D float tensor
-// {2 ny (nz/2+1), nx, R, S}; box {2Q, nx, RG, S}: one unit of the x-pass.
+// Spectrum (float2, layout (S, R, nx, ny, P), P = qpitch values per ky row) as a 4-D float
+// tensor {2 ny P, nx, R, S}; box {2Q, nx, RG, S}: one unit of the x-pass.
 int launch_xpass(const MeshGeom& mg, int Q, int RG, const CellInfo* ci, const GreenPairF* gpf, const float4* gtab,
                  const Tables* tab, const float* deconv, int spme, void* spec, double* part, int* n_blocks,
                  cudaStream_t s) {
@@ -52,7 +53,7 @@ int launch_xpass(const MeshGeom& mg, int Q, int RG, const CellInfo* ci, const Gr
     set_error("filter", "cuTensorMapEncodeTiled is not available from the driver");
     return FD3_ECUDA;
   }
-  const cuuint64_t inner = 2ull * mg.n[1] * mg.nzh;
+  const cuuint64_t inner = 2ull * mg.n[1] * (mg.qpitch > 0 ? mg.qpitch : mg.nzh);
   const cuuint64_t dims[4] = {inner, (cuuint64_t)mg.n[0], (cuuint64_t)mg.R, (cuuint64_t)mg.S};
   const cuuint64_t strides[3] = {inner * 4, inner * 4 * mg.n[0], inner * 4 * mg.n[0] * mg.R};
   const cuuint32_t box[4] = {(cuuint32_t)(2 * Q), (cuuint32_t)mg.n[0], (cuuint32_t)RG, (cuuint32_t)mg.S};

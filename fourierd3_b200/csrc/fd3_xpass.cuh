@@ -2,7 +2,9 @@
 // filter, inverse FFT along x, on the float spectrum of the (y, z) 2D transforms.
 //
 // Spectrum layout (the reference's channel-major mesh, kspace_filter_d3.py:55): channel
-// c = X R + r (species X, rank r), then x, then the flattened (y, kz) index q = y (nz/2+1) + kz.
+// c = X R + r (species X, rank r), then x, then the flattened (y, kz) index q = y P + kz, with P
+// = nz/2+1 values per ky row, or nz/2+2 (a zero pad slot, 16-byte rows) when the fused (y, z)
+// transforms write it.
 // For fixed (c, x) every q is contiguous, so a pencil of Q consecutive q values across all x is
 // nx contiguous runs of Q complex values (Q = 16: one 128-byte line per run), one stride apart.
 //
@@ -244,8 +246,8 @@ __global__ void __launch_bounds__(kXpThreads, 1)
     const float inv_h = green_inv_h(g, ci);
     MeshDev gs = g;
     if (g.win_axes) gs.win_axes = s_win;
-    const int n1 = g.n[1], nzh = g.nzh;
-    const int nq = n1 * nzh;
+    const int n1 = g.n[1], nzh = g.nzh, qp = g.qpitch;
+    const int nq = n1 * qp;   // flattened (y, kz) slots per x-row, pad slots included
     for (int k = 0;; ++k) {
       const int u = blockIdx.x + k * gridDim.x;
       if (u >= nunits) break;
@@ -268,8 +270,9 @@ __global__ void __launch_bounds__(kXpThreads, 1)
         const int qq = pt & (Q - 1), slot = pt >> LQ;
         const int qf = qb * Q + qq;
         if (qf >= nq) continue;
-        const int y = (int)fdiv((uint32_t)qf, g.div_nzh);
-        const int iz = qf - y * nzh;
+        const int y = (int)fdiv((uint32_t)qf, g.div_qpitch);
+        const int iz = qf - y * qp;
+        if (iz >= nzh) continue;   // the pad slot of a 16-byte spectrum row: zero, left as it is
         const int ix = (slot >> LN2) + N1 * (slot & (N2 - 1));
         const size_t kflat = ((size_t)ix * n1 + y) * nzh + iz;
         const KPoint<float> q = kpoint_idx<float>(gs, ix, y, iz, kflat, rc, deconv, spme, P);

@@ -57,7 +57,7 @@ int launch_xpass_t(const XpassArgs& a) {
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
-  const long long nq = (long long)mg.n[1] * mg.nzh;
+  const long long nq = (long long)mg.n[1] * (mg.qpitch > 0 ? mg.qpitch : mg.nzh);
   const int nqb = (int)((nq + Q - 1) / Q);
   const int ngrp = (mg.R + RG - 1) / RG;
   const long long nunits = (long long)nqb * ngrp;

@@ -218,7 +218,7 @@ __device__ __forceinline__ int yrow(int k) { return 16 * (k & 15) + (k >> 4); }
 // ------------------------------------------------------------------ forward
 template <int CL>
 __global__ void __launch_bounds__(YzCfg<CL>::kThreads, YzCfg<CL>::kMinBlocks)
-    k_yz_forward(const float* __restrict__ rho, float2* __restrict__ spec, int nplanes) {
+    k_yz_forward(const float* __restrict__ rho, float2* __restrict__ spec, int nplanes, int qp) {
   using C = YzCfg<CL>;
   constexpr int LDB = C::kLDB;
   extern __shared__ __align__(128) unsigned char yz_raw[];
@@ -320,7 +320,7 @@ __global__ void __launch_bounds__(YzCfg<CL>::kThreads, YzCfg<CL>::kMinBlocks)
     __syncthreads();
     const bool bad = *(volatile int*)&sm.fail;
     const float nanf_ = __int_as_float(0x7fc00000);
-    float2* out = spec + (size_t)plane * kYzN * kYzH;
+    float2* out = spec + (size_t)plane * kYzN * qp;   // qp = 129, or 130 with a zero pad slot
     for (int it = tid; it < C::kCols * 16; it += C::kThreads) {
       const int kk1 = it >> C::kLogCols, col = it & (C::kCols - 1);
       float re[16], im[16];
@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(YzCfg<CL>::kThreads, YzCfg<CL>::kMinBlocks)
         const int kz = q * C::kCols + col;
 #pragma unroll
         for (int k2 = 0; k2 < 16; ++k2)
-          out[(size_t)(kk1 + 16 * k2) * kYzH + kz] = bad ? float2{nanf_, 0.f} : float2{re[k2], im[k2]};
+          out[(size_t)(kk1 + 16 * k2) * qp + kz] = bad ? float2{nanf_, 0.f} : float2{re[k2], im[k2]};
       }
     }
     if (q == 0) {
@@ -343,8 +343,9 @@ __global__ void __launch_bounds__(YzCfg<CL>::kThreads, YzCfg<CL>::kMinBlocks)
         const float2 c = sm.B[yrow(ky) * LDB], cm = sm.B[yrow((kYzN - ky) & (kYzN - 1)) * LDB];
         const float2 y0{0.5f * (c.x + cm.x), 0.5f * (c.y - cm.y)};
         const float2 y128{0.5f * (c.y + cm.y), 0.5f * (cm.x - c.x)};
-        out[(size_t)ky * kYzH] = bad ? float2{nanf_, 0.f} : y0;
-        out[(size_t)ky * kYzH + 128] = bad ? float2{nanf_, 0.f} : y128;
+        out[(size_t)ky * qp] = bad ? float2{nanf_, 0.f} : y0;
+        out[(size_t)ky * qp + 128] = bad ? float2{nanf_, 0.f} : y128;
+        if (qp > kYzH) out[(size_t)ky * qp + kYzH] = float2{0.f, 0.f};
       }
     }
     cluster_sync_exec();   // every CTA has read its columns: the next plane may scatter
@@ -464,10 +465,170 @@ __global__ void __launch_bounds__(YzCfg<CL>::kThreads, YzCfg<CL>::kMinBlocks)
   cluster_sync_all();
 }
 
+// ------------------------------------------------------------------ inverse, TMA-fed (16-byte rows)
+// The inverse on CTA pairs for a half spectrum whose ky rows carry a pad slot (130 values, 1,040
+// bytes): each CTA's 64 columns of a plane arrive by one 2-D TMA load (rank 0 also loads the
+// kz = 128 column), instead of 8-byte loads whose latency the y pass waits on.
+struct YzInvT {
+  static constexpr int kThreads = 512;
+  static constexpr int kCols = 64;
+  static constexpr int kLDB = 64;   // the TMA box lands dense
+  static constexpr int kRows = 128;
+};
+struct YzInvTSmem {
+  float2 B[kYzN * YzInvT::kLDB];      // the CTA's columns, rows in ky, then the y transform in place
+  float4 h128[kYzN];                  // rank 0: (H[ky][128], pad) per ky
+  float2 ring[2][32 * 128];           // 16 warps x 4 row buffers of the z stage
+  float2 tw128[8 * 16];
+  float2 tw256[16 * 16];
+  float2 wk[kYzH + 1];
+  uint64_t full;
+  int fail;
+};
+
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int c0, int c1, uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(c0), "r"(c1), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__global__ void __launch_bounds__(YzInvT::kThreads, 1)
+    k_yz_inverse_tma(const __grid_constant__ CUtensorMap tcols, const __grid_constant__ CUtensorMap tnyq,
+                     const float2* __restrict__ spec, float* __restrict__ rho, int nplanes) {
+  constexpr int CL = 2, LDB = YzInvT::kLDB, QP = kYzH + 1;
+  extern __shared__ __align__(128) unsigned char yz_raw[];
+  YzInvTSmem& sm = *reinterpret_cast<YzInvTSmem*>(yz_raw + ((128u - (smem_u32(yz_raw) & 127u)) & 127u));
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int q = (int)cluster_rank();
+  const int cid = blockIdx.x / CL, ncl = gridDim.x / CL;
+  const int nmine = cid < nplanes ? (nplanes - cid + ncl - 1) / ncl : 0;
+  if (tid == 0) {
+    mbar_init(&sm.full, 1);
+    sm.fail = 0;
+    mbar_fence_init();
+  }
+  for (int m = tid; m < 128 + 256 + kYzH; m += blockDim.x) {
+    double sn, cs;
+    if (m < 128) {
+      sincospi(-2.0 * (((m >> 4) * (m & 15)) % 128) / 128.0, &sn, &cs);
+      sm.tw128[m] = float2{(float)cs, (float)sn};
+    } else if (m < 384) {
+      const int j = m - 128;
+      sincospi(-2.0 * (((j >> 4) * (j & 15)) % 256) / 256.0, &sn, &cs);
+      sm.tw256[j] = float2{(float)cs, (float)sn};
+    } else {
+      sincospi(-2.0 * (m - 384) / 256.0, &sn, &cs);
+      sm.wk[m - 384] = float2{(float)cs, (float)sn};
+    }
+  }
+  __syncthreads();
+  cluster_sync_all();
+  const uint32_t b_local = smem_u32(sm.B);
+  float2* wbuf = &sm.ring[0][0] + warp * 4 * 128;
+  auto xaddr = [&](int kz, uint32_t yr) {
+    return map_rank(b_local, (uint32_t)(kz >> 6)) + (yr + (uint32_t)(kz & 63)) * 8u;
+  };
+  constexpr uint32_t kShare = (uint32_t)(kYzN * QP * 8 / CL);   // this CTA's half of a plane's rows
+  constexpr uint32_t kColBytes = kYzN * YzInvT::kCols * 8;
+  constexpr uint32_t kNyqBytes = kYzN * 16;
+  if (tid == 0 && nmine > 0)
+    prefetch_l2(reinterpret_cast<const char*>(spec + (size_t)cid * kYzN * QP) + q * kShare, kShare);
+  const float nanf_ = __int_as_float(0x7fc00000);
+  for (int i = 0; i < nmine; ++i) {
+    const int plane = cid + i * ncl;
+    if (tid == 0) {
+      if (i + 1 < nmine)
+        prefetch_l2(reinterpret_cast<const char*>(spec + (size_t)(plane + ncl) * kYzN * QP) + q * kShare, kShare);
+      if (!sm.fail) {
+        fence_proxy_async_smem();   // the previous plane's reads of B are done (cluster barrier)
+        mbar_arrive_expect_tx(&sm.full, q == 0 ? kColBytes + kNyqBytes : kColBytes);
+        tma_load_2d(sm.B, &tcols, 128 * q, plane * kYzN, &sm.full);
+        if (q == 0) tma_load_2d(sm.h128, &tnyq, 256, plane * kYzN, &sm.full);
+      }
+    }
+    if (!*(volatile int*)&sm.fail && !mbar_wait(&sm.full, (uint32_t)i & 1u)) sm.fail = 1;
+    __syncthreads();
+    const bool bad = *(volatile int*)&sm.fail;
+    // ---- inverse y transforms of this CTA's 64 columns
+    for (int it = tid; it < YzInvT::kCols * 16; it += YzInvT::kThreads) {
+      const int n2 = it >> 6, col = it & 63;
+      const bool packed = q == 0 && col == 0;
+      float re[16], im[16];
+#pragma unroll
+      for (int n1 = 0; n1 < 16; ++n1) {
+        const int ky = 16 * n1 + n2;
+        float2 v = sm.B[ky * LDB + col];
+        if (packed) {   // H[ky][0] + i H[ky][128]: one transform gives both real columns
+          const float4 h = sm.h128[ky];
+          v = float2{v.x - h.y, v.y + h.x};
+        }
+        re[n1] = v.x;
+        im[n1] = v.y;
+      }
+      ypass1_store<1, LDB>(re, im, n2, col, sm.B, sm.tw256);
+    }
+    __syncthreads();
+    for (int it = tid; it < YzInvT::kCols * 16; it += YzInvT::kThreads) {
+      const int kk1 = it >> 6, col = it & 63;
+      float re[16], im[16];
+      ypass2_load<1, LDB>(re, im, kk1, col, sm.B);
+#pragma unroll
+      for (int k2 = 0; k2 < 16; ++k2) sm.B[(16 * kk1 + k2) * LDB + col] = float2{re[k2], im[k2]};
+    }
+    cluster_sync_all();   // both CTAs' columns transformed: rows may be read across the pair
+    // ---- per row y: half-complex -> complex packing, inverse 128-point FFT, real row out
+    for (int round = 0; round < 2; ++round) {
+      const int ybase = YzInvT::kRows * q + 64 * round + 4 * warp;
+#pragma unroll
+      for (int it = lane; it < 4 * 64; it += 32) {
+        const int r = it >> 6, k = it & 63;
+        const uint32_t yr = (uint32_t)(yrow(ybase + r) * LDB);
+        float2* row = wbuf + r * 128;
+        const float2 p0 = ld_cluster(xaddr(k, yr));
+        float2 a, c;
+        if (k == 0) {
+          a = float2{p0.x, 0.f};
+          c = float2{p0.y, 0.f};
+        } else {
+          a = p0;
+          c = ld_cluster(xaddr(128 - k, yr));
+        }
+        {
+          const float2 w = sm.wk[k];
+          const float sx = a.x + c.x, sy = a.y - c.y, dx = a.x - c.x, dy = a.y + c.y;
+          row[k] = float2{sx - w.x * dy + w.y * dx, sy + w.x * dx + w.y * dy};
+        }
+        if (k == 0) {   // Z[64] from X[64] alone
+          const float2 x = ld_cluster(xaddr(64, yr));
+          const float2 w = sm.wk[64];
+          const float dy = 2.f * x.y;
+          row[64] = float2{2.f * x.x - w.x * dy, w.y * dy};
+        } else {
+          const float2 w = sm.wk[128 - k];
+          const float sx = c.x + a.x, sy = c.y - a.y, dx = c.x - a.x, dy = c.y + a.y;
+          row[128 - k] = float2{sx - w.x * dy + w.y * dx, sy + w.x * dx + w.y * dy};
+        }
+      }
+      __syncwarp();
+      float re[16], im[16];
+      fft128_rows<1>(wbuf, sm.tw128, lane, re, im);
+      const int r2 = lane >> 3, k1 = lane & 7;
+      float2* dst = reinterpret_cast<float2*>(rho + ((size_t)plane * kYzN + ybase + r2) * kYzN);
+#pragma unroll
+      for (int k2 = 0; k2 < 16; ++k2) dst[k1 + 8 * k2] = bad ? float2{nanf_, nanf_} : float2{re[k2], im[k2]};
+      __syncwarp();
+    }
+    cluster_sync_exec();   // both CTAs have read the pair's columns: the next plane may load
+  }
+  cluster_sync_all();
+}
+
 template <int CL>
 int launch_yz(const void* kern, int which, int threads, size_t smem, void** args, int nplanes, cudaStream_t s,
               const char* what) {
-  static unsigned attr_set[2] = {0, 0};   // per kernel, one bit per device (set every call past 32)
+  static unsigned attr_set[3] = {0, 0, 0};   // per kernel, one bit per device (set every call past 32)
   int dev = 0;
   cudaGetDevice(&dev);
   const unsigned bit = dev < 32 ? 1u << dev : 0u;
@@ -520,7 +681,9 @@ int launch_yz_forward(const MeshGeom& mg, int nchannels, int variant, const floa
   const float* in = rho;
   float2* out = reinterpret_cast<float2*>(spec);
   int n = (int)np;
-  void* args[3] = {&in, &out, &n};
+  int qp = mg.qpitch > 0 ? mg.qpitch : kYzH;
+  if (qp != kYzH && qp != kYzH + 1) return FD3_EINVAL;
+  void* args[4] = {&in, &out, &n, &qp};
   if (variant == 1)
     return launch_yz<2>(reinterpret_cast<const void*>(k_yz_forward<2>), 0, YzCfg<2>::kThreads,
                         sizeof(YzSmem<2>) + 128, args, n, s, "fft_r2c");
@@ -531,14 +694,43 @@ int launch_yz_forward(const MeshGeom& mg, int nchannels, int variant, const floa
 int launch_yz_inverse(const MeshGeom& mg, int nchannels, int variant, const void* spec, float* rho,
                       cudaStream_t s) {
   if (!yzfft_applies(mg) || nchannels < 1 || (variant != 1 && variant != 2)) return FD3_EINVAL;
+  (void)variant;   // the inverse runs on pairs for both variants (quads measured slower)
   const long long np = (long long)nchannels * mg.n[0];
-  if (np > (1LL << 30)) return FD3_EINVAL;
+  if (np > (1LL << 30) / kYzN) return FD3_EINVAL;
+  const int qp = mg.qpitch > 0 ? mg.qpitch : kYzH;
   const float2* in = reinterpret_cast<const float2*>(spec);
   float* out = rho;
   int n = (int)np;
-  void* args[3] = {&in, &out, &n};
-  (void)variant;   // the inverse runs on pairs for both variants (quads measured slower)
-  return launch_yz<2>(reinterpret_cast<const void*>(k_yz_inverse<2>), 1, YzCfg<2>::kThreads, sizeof(YzSmem<2>) + 128,
+  if (qp == kYzH) {
+    void* args[3] = {&in, &out, &n};
+    return launch_yz<2>(reinterpret_cast<const void*>(k_yz_inverse<2>), 1, YzCfg<2>::kThreads,
+                        sizeof(YzSmem<2>) + 128, args, n, s, "fft_c2r");
+  }
+  if (qp != kYzH + 1) return FD3_EINVAL;
+  // 16-byte spectrum rows: the columns come by TMA (a 2-D map over (floats of a row, rows))
+  auto fn = tensor_map_encoder();
+  if (!fn) {
+    set_error("fft_c2r", "cuTensorMapEncodeTiled is not available from the driver");
+    return FD3_ECUDA;
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)(2 * qp), (cuuint64_t)np * kYzN};
+  const cuuint64_t strides[1] = {(cuuint64_t)(2 * qp) * 4};
+  const cuuint32_t estr[2] = {1, 1};
+  const cuuint32_t box_cols[2] = {2 * YzInvT::kCols, kYzN};
+  const cuuint32_t box_nyq[2] = {4, kYzN};
+  CUtensorMap tcols, tnyq;
+  for (int m = 0; m < 2; ++m) {
+    const CUresult r = fn(m == 0 ? &tcols : &tnyq, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<void*>(spec), dims,
+                          strides, m == 0 ? box_cols : box_nyq, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                          CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+      set_error("fft_c2r", "cuTensorMapEncodeTiled rejected the spectrum's tensor map");
+      return FD3_ECUDA;
+    }
+  }
+  void* args[5] = {&tcols, &tnyq, &in, &out, &n};
+  return launch_yz<2>(reinterpret_cast<const void*>(k_yz_inverse_tma), 2, YzInvT::kThreads, sizeof(YzInvTSmem) + 128,
                       args, n, s, "fft_c2r");
 }
 

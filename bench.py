@@ -76,6 +76,49 @@ def dist_setup(args):
     return ws, rank, local
 
 
+def gpu_local_cpus(dev_idx: int):
+    """The host CPUs NVML reports as closest to the GPU (its NUMA node), or None."""
+    try:
+        import pynvml
+
+        pynvml.nvmlInit()
+        try:
+            pr = torch.cuda.get_device_properties(dev_idx)
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(
+                f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0")
+        except Exception:
+            h = pynvml.nvmlDeviceGetHandleByIndex(dev_idx)
+        ncpu = os.cpu_count() or 1
+        words = pynvml.nvmlDeviceGetCpuAffinity(h, (ncpu + 63) // 64)
+        cpus = {64 * w + b for w, m in enumerate(words) for b in range(64) if (int(m) >> b) & 1}
+        cpus &= set(range(ncpu))
+        return cpus or None
+    except Exception:
+        return None
+
+
+def host_buffers_local(batch):
+    """batch.host_buffers(), allocated and first written by this thread bound to the GPU's
+    NUMA-local CPUs (so the pinned pages sit next to the GPU); returns (buffers, cpus or None)."""
+    cpus = gpu_local_cpus(torch.cuda.current_device())
+    old = os.sched_getaffinity(0) if hasattr(os, "sched_getaffinity") else None
+    bound = False
+    if cpus and old is not None and (cpus & old):
+        try:
+            os.sched_setaffinity(0, cpus & old)
+            bound = True
+        except OSError:
+            bound = False
+    try:
+        h = batch.host_buffers()
+        h["out"].zero_()
+        h["positions"].copy_(batch.positions.cpu())
+    finally:
+        if bound:
+            os.sched_setaffinity(0, old)
+    return h, (cpus & old if bound else None)
+
+
 def barrier(ws):
     if ws > 1:
         import torch.distributed as dist
@@ -540,7 +583,7 @@ def run_batch(args, ws, rank, local):
             eng.profile(False)
             break
     # end to end: one graph replay that copies the host positions in and E/F/stress out
-    b.host_buffers()
+    host_buffers_local(b)
 
     def e2e():
         b.run_host()
@@ -711,7 +754,9 @@ def main():
     # that copies the positions in from pinned host memory, evaluates, and copies energy, stress
     # and forces back out (one copy each way)
     gb = graphs[head]
-    hbuf = gb.host_buffers()
+    # the pinned host buffers on the GPU's own NUMA node (allocated and first written by a thread
+    # bound to the CPUs NVML lists for the GPU; the binding is undone afterwards)
+    hbuf, local_cpus = host_buffers_local(gb)
     hbuf["positions"].copy_(torch.tensor(pos, dtype=torch.float64))
     h2d_bytes = int(hbuf["pos"].numel() * 8)
     d2h_bytes = int(hbuf["out"].numel() * 8)
@@ -812,7 +857,10 @@ def main():
         "e2e": ({"value": ws * n / (e2e_ms * 1e-3), "unit": "atoms/s", "ms_per_step": e2e_ms,
                  "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
                  "path": "D3Batch.run_host: one graph replay that copies the pinned host positions in, "
-                         "evaluates, and copies energy, stress and forces out to pinned host memory"}
+                         "evaluates, and copies energy, stress and forces out to pinned host memory",
+                 "host_buffers": ("pinned on the GPU's NUMA node (allocated from a thread bound to the "
+                                  f"{len(local_cpus)} CPUs NVML lists for the GPU)" if local_cpus
+                                  else "pinned (NVML CPU affinity unavailable)")}
                 if e2e_ms is not None else None),
         "gpu_launches": int(launches) * args.steps,
         "clocks": clocks,

@@ -755,14 +755,28 @@ static int mesh_sort(fd3_plan* p, int N, const double* pos, double ps, const int
   return counting_sort(w.mkeys, N, Kmesh, w.mcount, w.mstart, w.morder, s);
 }
 
+// The position-only preparation of the mesh stage that can run beside the cell list and the CN
+// stage: the stencil records' nodes and weights, and the mixed form's Green table.
+static int mesh_side_prep(fd3_plan* p, int N, const double* pos, double ps, const int32_t* species, Work& w,
+                          cudaStream_t s) {
+  const MeshGeom& mg = p->mg;
+  if (p->precision == FD3_PREC_FP64)
+    return launch_spread<double>(mg, N, pos, ps, species, nullptr, w.ci, w.mstart, w.morder, w.rec, (double*)w.rho,
+                                 s, kSpreadRecordsOnly);
+  FD3_TRY(launch_spread<float>(mg, N, pos, ps, species, nullptr, w.ci, w.mstart, w.morder, w.rec, (float*)w.rho, s,
+                               kSpreadRecordsOnly));
+  return launch_green_table(mg, w.ci, p->d_green, p->d_tab, w.gtab, s);
+}
+
 template <typename T>
 static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const int32_t* species, Work& w,
                          bool need_grad, double* gpos, double* mcell, int* n_kspc, int* n_mcell, bool presorted,
-                         cudaStream_t s) {
+                         cudaStream_t s, bool side_prep = false) {
   const MeshGeom& mg = p->mg;
   if (!presorted) FD3_TRY(mesh_sort(p, N, pos, ps, species, w, s));
   prof_mark(p, s, "mesh_sort");
-  FD3_TRY(launch_spread<T>(mg, N, pos, ps, species, w.c6, w.ci, w.mstart, w.morder, w.rec, (T*)w.rho, s));
+  FD3_TRY(launch_spread<T>(mg, N, pos, ps, species, w.c6, w.ci, w.mstart, w.morder, w.rec, (T*)w.rho, s,
+                           side_prep ? 1 : 0));
   prof_mark(p, s, "spread");
   const bool tma_x = sizeof(T) == 4 && xpass_on(p);
   if (tma_x || old_xpass_on(p)) {
@@ -784,7 +798,7 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
         FD3_CUFFT(cufftExecR2C(p->fwd2, (cufftReal*)w.rho, (cufftComplex*)w.spec));
     }
     prof_mark(p, s, "fft_r2c");
-    if (sizeof(T) == 4) FD3_TRY(launch_green_table(mg, w.ci, p->d_green, p->d_tab, w.gtab, s));
+    if (sizeof(T) == 4 && !side_prep) FD3_TRY(launch_green_table(mg, w.ci, p->d_green, p->d_tab, w.gtab, s));
     if (tma_x) {
       int Q, RG;
       xpass_shape(p, &Q, &RG);
@@ -821,7 +835,7 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
     FD3_CUFFT(cufftExecR2C(p->fwd, (cufftReal*)w.rho, (cufftComplex*)w.spec));
   prof_mark(p, s, "fft_r2c");
   void* hspec = w.spec;   // the filter overwrites the spectrum with H in place
-  if (sizeof(T) == 4) FD3_TRY(launch_green_table(mg, w.ci, p->d_green, p->d_tab, w.gtab, s));
+  if (sizeof(T) == 4 && !side_prep) FD3_TRY(launch_green_table(mg, w.ci, p->d_green, p->d_tab, w.gtab, s));
   FD3_TRY(launch_filter<T>(mg, w.ci, p->d_green, p->d_green_f, (const float4*)w.gtab, p->d_tab, p->d_deconv, p->method == FD3_METHOD_SPME, w.spec,
                            w.kspc_part, n_kspc, s));
   prof_mark(p, s, "filter");
@@ -842,7 +856,7 @@ static int mesh_pipeline(fd3_plan* p, int N, const double* pos, double ps, const
 
 static int run_mesh(fd3_plan* p, int N, const double* pos, double ps, const int32_t* species, Work& w,
                     bool need_grad, double* gpos, double* mcell, int* n_kspc, int* n_mcell, cudaStream_t s,
-                    bool presorted = false) {
+                    bool presorted = false, bool side_prep = false) {
   if (p->method == FD3_METHOD_EWALD) {
     EwaldGeom eg{{p->ens[0], p->ens[1], p->ens[2]}, p->S, p->R};
     int rc;
@@ -856,8 +870,10 @@ static int run_mesh(fd3_plan* p, int N, const double* pos, double ps, const int3
     return rc;
   }
   if (p->precision == FD3_PREC_FP64)
-    return mesh_pipeline<double>(p, N, pos, ps, species, w, need_grad, gpos, mcell, n_kspc, n_mcell, presorted, s);
-  return mesh_pipeline<float>(p, N, pos, ps, species, w, need_grad, gpos, mcell, n_kspc, n_mcell, presorted, s);
+    return mesh_pipeline<double>(p, N, pos, ps, species, w, need_grad, gpos, mcell, n_kspc, n_mcell, presorted, s,
+                                 side_prep);
+  return mesh_pipeline<float>(p, N, pos, ps, species, w, need_grad, gpos, mcell, n_kspc, n_mcell, presorted, s,
+                              side_prep);
 }
 
 // ------------------------------------------------------------------ D4 k-space CN stages
@@ -1027,10 +1043,11 @@ extern "C" int fd3_energy_forces_stress(fd3_plan* p, int64_t n_atoms, const doub
     return FD3_OK;
   }
   const bool fork = p->side != nullptr && p->method != FD3_METHOD_EWALD;
-  if (fork) {   // mesh sort on the side stream, beside the cell list and the CN stage
+  if (fork) {   // mesh sort, stencil records and Green table on the side stream, beside the cell list and CN
     FD3_CUDA(cudaEventRecord(p->ev_fork, s));
     FD3_CUDA(cudaStreamWaitEvent(p->side, p->ev_fork, 0));
     FD3_TRY(mesh_sort(p, N, d_pos_ang, kAngToBohr, d_species, w, p->side));
+    FD3_TRY(mesh_side_prep(p, N, d_pos_ang, kAngToBohr, d_species, w, p->side));
     FD3_CUDA(cudaEventRecord(p->ev_join, p->side));
   }
   FD3_TRY(build_cell_list(g, N, d_pos_ang, d_species, w.cl, s));
@@ -1042,7 +1059,7 @@ extern "C" int fd3_energy_forces_stress(fd3_plan* p, int64_t n_atoms, const doub
   if (fork) FD3_CUDA(cudaStreamWaitEvent(s, p->ev_join, 0));
   // the mesh gradient (Hartree/Bohr) is staged in d_forces, then finished by the CN adjoint
   FD3_TRY(run_mesh(p, N, d_pos_ang, kAngToBohr, d_species, w, true, d_forces, nullptr, &n_kspc, &n_mcell, s,
-                   fork));
+                   fork, fork));
   FD3_TRY(launch_cn_adjoint_cells(g, N, w.cl, d_pos_ang, d_species, p->d_tab, w.gcn, d_forces,
                                   -kHartreeToEv * kAngToBohr, w.cnv_part, &n_cnv, w.hits, s));
   prof_mark(p, s, "cn_adjoint");

@@ -178,10 +178,15 @@ int launch_yz_inverse(const MeshGeom& mg, int nchannels, int variant, const void
                       cudaStream_t s);
 // Whether the tile-staged (TMA) gather applies to this mesh for elements of `elem` bytes.
 bool gather_tile_applies(const MeshGeom& mg, size_t elem);
+// records: 0 = write the stencil records (with the rank factors) and spread; 1 = the records'
+// nodes and weights are written already (kSpreadRecordsOnly on another stream): write the rank
+// factors and spread; 2 (kSpreadRecordsOnly) = write the records' nodes and weights only (they
+// need the positions and the mesh sort, not C6).
+constexpr int kSpreadRecordsOnly = 2;
 template <typename T>
 int launch_spread(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
                   const double* c6, const CellInfo* ci, const int* key_start, const int* order,
-                  const MeshRecords& rec, T* rho, cudaStream_t s);
+                  const MeshRecords& rec, T* rho, cudaStream_t s, int records = 0);
 template <typename T>
 int launch_filter(const MeshGeom& mg, const CellInfo* ci, const GreenPair* gp, const GreenPairF* gpf,
                   const float4* gtab, const Tables* tab, const float* deconv, int spme, void* spec, double* part,

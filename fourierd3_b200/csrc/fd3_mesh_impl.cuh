@@ -96,6 +96,8 @@ __global__ void __launch_bounds__(256) k_mesh_records(MeshDev g, int n, const do
   T xl[3];
   mesh_locate<T>(pos, atom, ps, ci, g.n[0], g.n[1], g.n[2], P, base, xl);
   rb[t] = make_int4(base[0], base[1], base[2], species[atom]);
+  if (c6)
+    for (int r = 0; r < g.R; ++r) rc[(size_t)t * g.R + r] = (T)c6[(size_t)atom * g.R + r];
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     T w[P], dw[P];
@@ -106,7 +108,16 @@ __global__ void __launch_bounds__(256) k_mesh_records(MeshDev g, int n, const do
       rdw[((size_t)t * 3 + a) * P + k] = dw[k];
     }
   }
-  for (int r = 0; r < g.R; ++r) rc[(size_t)t * g.R + r] = (T)c6[(size_t)atom * g.R + r];
+}
+
+// The records' rank factors alone (sorted order), when the nodes and weights were written earlier.
+template <typename T>
+__global__ void __launch_bounds__(256) k_rank_factors(int n, int R, const double* __restrict__ c6,
+                                                      const int* __restrict__ order, T* __restrict__ rc) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  const int atom = order[t];
+  for (int r = 0; r < R; ++r) rc[(size_t)t * R + r] = (T)c6[(size_t)atom * R + r];
 }
 
 // ------------------------------------------------------------------ spread
@@ -667,13 +678,19 @@ inline int spread_zc(const MeshGeom& mg) {
 template <typename T, int P, bool LAG>
 static int spread_r(const MeshGeom& mg, dim3 grid, int n, const double* pos, double ps, const int32_t* species,
                     const double* c6, const CellInfo* ci, const int* ks, const int* order, const MeshRecords& rec,
-                    T* rho, cudaStream_t s) {
+                    T* rho, cudaStream_t s, int records) {
   const MeshDev g = to_dev(mg);
   if (n > 0) {
-    k_mesh_records<T, P, LAG><<<(n + 255) / 256, 256, 0, s>>>(g, n, pos, ps, species, c6, ci, order, rec.b, (T*)rec.w,
-                                                              (T*)rec.dw, (T*)rec.c);
+    if (records == 1) {
+      k_rank_factors<T><<<(n + 255) / 256, 256, 0, s>>>(n, mg.R, c6, order, (T*)rec.c);
+    } else {
+      k_mesh_records<T, P, LAG><<<(n + 255) / 256, 256, 0, s>>>(g, n, pos, ps, species,
+                                                                records == kSpreadRecordsOnly ? nullptr : c6, ci,
+                                                                order, rec.b, (T*)rec.w, (T*)rec.dw, (T*)rec.c);
+    }
     FD3_LAUNCHED();
   }
+  if (records == kSpreadRecordsOnly) return FD3_OK;
   const int zc = spread_zc(mg);
   if (zc > 0) {
     // staged atoms per chunk: as many as let 3 (float) or 2 (double) CTAs share an SM
@@ -705,7 +722,7 @@ static int spread_r(const MeshGeom& mg, dim3 grid, int n, const double* pos, dou
 template <typename T>
 int launch_spread(const MeshGeom& mg, int n, const double* pos, double pos_scale, const int32_t* species,
                   const double* c6, const CellInfo* ci, const int* key_start, const int* order,
-                  const MeshRecords& rec, T* rho, cudaStream_t s) {
+                  const MeshRecords& rec, T* rho, cudaStream_t s, int records) {
   if (mg.R > FD3_MAX_RANK || mg.order < 1 || mg.order > FD3_MAX_ORDER) return FD3_EINVAL;
   if (mg.t[0] > kSpTX || mg.t[1] > kSpTY || mg.t[2] > kSpTZ || mg.ns[0] * mg.ns[1] * mg.ns[2] > 125)
     return FD3_EINVAL;
@@ -713,9 +730,9 @@ int launch_spread(const MeshGeom& mg, int n, const double* pos, double pos_scale
 #define FD3_SPREAD_CASE(PP)                                                                                  \
   case PP:                                                                                                   \
     return mg.lagrange ? spread_r<T, PP, true>(mg, grid, n, pos, pos_scale, species, c6, ci, key_start, order, rec, \
-                                               rho, s)                                                       \
+                                               rho, s, records)                                              \
                        : spread_r<T, PP, false>(mg, grid, n, pos, pos_scale, species, c6, ci, key_start, order, rec, \
-                                                rho, s);
+                                                rho, s, records);
   switch (mg.order) {
     FD3_SPREAD_CASE(1)
     FD3_SPREAD_CASE(2)

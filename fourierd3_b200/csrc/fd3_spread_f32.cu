@@ -3,5 +3,6 @@
 
 namespace fd3 {
 template int launch_spread<float>(const MeshGeom&, int, const double*, double, const int32_t*, const double*,
-                                  const CellInfo*, const int*, const int*, const MeshRecords&, float*, cudaStream_t);
+                                  const CellInfo*, const int*, const int*, const MeshRecords&, float*, cudaStream_t,
+                                  int);
 }  // namespace fd3

@@ -3,5 +3,6 @@
 
 namespace fd3 {
 template int launch_spread<double>(const MeshGeom&, int, const double*, double, const int32_t*, const double*,
-                                  const CellInfo*, const int*, const int*, const MeshRecords&, double*, cudaStream_t);
+                                  const CellInfo*, const int*, const int*, const MeshRecords&, double*, cudaStream_t,
+                                  int);
 }  // namespace fd3

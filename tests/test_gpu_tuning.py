@@ -335,6 +335,36 @@ def test_fused_yz_transforms_agree_with_cufft(fft_x, variant, cuda_device):
     assert float(e2) == float(e) and torch.equal(f2, f) and torch.equal(s2, s)
 
 
+def test_fused_yz_transforms_non_cubic_mesh(cuda_device):
+    """A 50 x 80 x 80 A box at h = 1.2 A: a 128 x 256 x 256 mesh (nx = 128 planes of 256 x 256,
+    the nx = 128 TMA x-pass on the padded spectrum), 3,000 random atoms of 4 elements, mixed
+    precision: the fused (y, z) transforms against cuFFT's, and against the float64 form."""
+    from fourierd3_b200 import D3Model
+
+    rng = np.random.default_rng(11)
+    cell = np.diag([50.0, 80.0, 80.0])
+    n = 3000
+    frac = rng.random((n, 3))
+    pos = frac @ cell
+    z = rng.choice([1, 6, 7, 8], size=n)
+    m = D3Model(z, cell, precision="mixed", device=cuda_device, **KW)
+    assert tuple(m.mesh) == (128, 256, 256)
+    m.engine.set_tuning(fft_x=2, xq=4, xranks=min(4, m.setup.n_rank) if m.setup.n_rank in (1, 2, 4) else 1)
+    for variant in (1, 2):
+        m.engine.set_tuning(fft_yz=0)
+        e0, f0, s0 = (t.clone() for t in m(pos, cell))
+        m.engine.set_tuning(fft_yz=variant)
+        assert m.engine.tuning()["fft_yz"] == variant, m.engine.tuning()
+        e, f, s = m(pos, cell)
+        assert abs(float(e) - float(e0)) <= 2e-7 * abs(float(e0)), (variant, float(e), float(e0))
+        assert (f - f0).abs().max().item() <= 5e-6
+        assert (s - s0).abs().max().item() <= 5e-8
+    m64 = D3Model(z, cell, precision="fp64", device=cuda_device, **KW)
+    e64, f64, _ = m64(pos, cell)
+    assert abs(float(e) - float(e64)) <= 1e-6 * abs(float(e64))
+    assert (f - f64).abs().max().item() <= 1e-4
+
+
 def test_fused_yz_transforms_where_they_apply(cuda_device):
     """In effect only with the x-pass, mixed precision and a 256 x 256 (y, z) plane."""
     from fourierd3_b200 import D3Model, structures as st

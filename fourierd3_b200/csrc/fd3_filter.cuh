@@ -39,6 +39,11 @@ __device__ __forceinline__ double sinc_pi(double x) { return x == 0.0 ? 1.0 : si
 // k-vector, |k|, the SPME window, the Hermitian weight (1 on the first and last z-plane,
 // pair_pot.py:213-218) and, on the self-conjugate planes, the |k| of the stored conjugate
 // partner when it differs. The reciprocal rows are hoisted into registers by the caller.
+// |k| from |k|^2: float64 sqrt, or in float the hardware reciprocal square root times |k|^2
+// (a few ulp; the mixed form's tolerance is orders of magnitude wider)
+__device__ __forceinline__ double knorm_of(double k2) { return sqrt(k2); }
+__device__ __forceinline__ float knorm_of(float k2) { return k2 > 0.f ? k2 * rsqrtf(k2) : 0.f; }
+
 template <typename T>
 struct KPoint {
   T kv[3], knorm, inv_sc, wk, kpart;
@@ -54,15 +59,15 @@ __device__ __forceinline__ KPoint<T> kpoint_idx(const MeshDev& g, int ix, int iy
   const int mz = iz;
 #pragma unroll
   for (int c = 0; c < 3; ++c) q.kv[c] = T(mx) * rc[c] + T(my) * rc[3 + c] + T(mz) * rc[6 + c];
-  q.knorm = sqrt(q.kv[0] * q.kv[0] + q.kv[1] * q.kv[1] + q.kv[2] * q.kv[2]);
+  q.knorm = knorm_of(q.kv[0] * q.kv[0] + q.kv[1] * q.kv[1] + q.kv[2] * q.kv[2]);
   if (sizeof(T) == 4 && spme && g.win_axes) {
     // mixed form: the window is separable, sinc(mx/nx)^2p sinc(my/ny)^2p sinc(mz/nz)^2p (clamped
     // at 1e-10 like the table); three per-axis values that stay in L1 instead of one table read
     const float* wa = g.win_axes;
     const float w = wa[ix] * wa[g.n[0] + iy] * wa[g.n[0] + g.n[1] + iz];
-    q.inv_sc = T(__frcp_rn(w < 1e-10f ? 1e-10f : w));
+    q.inv_sc = T(rcp_t(w < 1e-10f ? 1e-10f : w));
   } else if (sizeof(T) == 4 && spme && deconv) {
-    q.inv_sc = T(__frcp_rn(deconv[k]));   // mixed form: the float32 window inverted (correctly rounded)
+    q.inv_sc = T(rcp_t(deconv[k]));   // mixed form: the float32 window inverted (hardware reciprocal)
   } else {
     double sc = 1.0;
     if (spme) {
@@ -93,7 +98,7 @@ __device__ __forceinline__ KPoint<T> kpoint_idx(const MeshDev& g, int ix, int iy
       T kp[3];
 #pragma unroll
       for (int c = 0; c < 3; ++c) kp[c] = T(qx) * rc[c] + T(qy) * rc[3 + c] + T(mz) * rc[6 + c];
-      q.kpart = sqrt(kp[0] * kp[0] + kp[1] * kp[1] + kp[2] * kp[2]);
+      q.kpart = knorm_of(kp[0] * kp[0] + kp[1] * kp[1] + kp[2] * kp[2]);
       q.partner = q.kpart != q.knorm;
     }
   }
@@ -121,8 +126,8 @@ __device__ __forceinline__ void load_recip(const CellInfo* __restrict__ ci, T (&
 template <typename T>
 __device__ __forceinline__ void virial_acc(const KPoint<T>& q, T dq, double* acc) {
   if (q.knorm > T(0)) {
-    // float: one correctly rounded reciprocal instead of a division (the mixed form's virial)
-    const T f = sizeof(T) == 4 ? T(q.wk * dq * __frcp_rn((float)q.knorm)) : q.wk * dq / q.knorm;
+    // float: one hardware reciprocal instead of a division (the mixed form's virial)
+    const T f = sizeof(T) == 4 ? T(q.wk * dq * rcp_t((float)q.knorm)) : q.wk * dq / q.knorm;
     acc[1] += (double)(f * q.kv[0] * q.kv[0]);
     acc[2] += (double)(f * q.kv[1] * q.kv[1]);
     acc[3] += (double)(f * q.kv[2] * q.kv[2]);

@@ -527,9 +527,6 @@ __global__ void __launch_bounds__(YzInvT::kThreads, 1)
   cluster_sync_all();
   const uint32_t b_local = smem_u32(sm.B);
   float2* wbuf = &sm.ring[0][0] + warp * 4 * 128;
-  auto xaddr = [&](int kz, uint32_t yr) {
-    return map_rank(b_local, (uint32_t)(kz >> 6)) + (yr + (uint32_t)(kz & 63)) * 8u;
-  };
   constexpr uint32_t kShare = (uint32_t)(kYzN * QP * 8 / CL);   // this CTA's half of a plane's rows
   constexpr uint32_t kColBytes = kYzN * YzInvT::kCols * 8;
   constexpr uint32_t kNyqBytes = kYzN * 16;
@@ -578,22 +575,33 @@ __global__ void __launch_bounds__(YzInvT::kThreads, 1)
       for (int k2 = 0; k2 < 16; ++k2) sm.B[(16 * kk1 + k2) * LDB + col] = float2{re[k2], im[k2]};
     }
     cluster_sync_all();   // both CTAs' columns transformed: rows may be read across the pair
-    // ---- per row y: half-complex -> complex packing, inverse 128-point FFT, real row out
+    // ---- per row y: half-complex -> complex packing, inverse 128-point FFT, real row out.
+    // Lane item j (0..7) of a round is row j / 2, k = lane + 32 (j % 2); its two cross-CTA reads
+    // are X[k] and X[128 - k] (X[64] for k = 0): all 16 are issued before any is used.
+    const uint32_t bq0 = map_rank(b_local, 0u), bq1 = map_rank(b_local, 1u);
     for (int round = 0; round < 2; ++round) {
       const int ybase = YzInvT::kRows * q + 64 * round + 4 * warp;
+      float2 va[8], vc[8];
 #pragma unroll
-      for (int it = lane; it < 4 * 64; it += 32) {
-        const int r = it >> 6, k = it & 63;
-        const uint32_t yr = (uint32_t)(yrow(ybase + r) * LDB);
-        float2* row = wbuf + r * 128;
-        const float2 p0 = ld_cluster(xaddr(k, yr));
+      for (int j = 0; j < 8; ++j) {
+        const int k = lane + 32 * (j & 1);   // 0..63: rank 0's columns
+        const uint32_t yr = (uint32_t)(yrow(ybase + (j >> 1)) * LDB);
+        const int k2 = k == 0 ? 64 : 128 - k;   // 64..128 -> rank 1 (X[128]: the packed column's imaginary part)
+        va[j] = ld_cluster(bq0 + (yr + (uint32_t)k) * 8u);
+        vc[j] = ld_cluster(bq1 + (yr + (uint32_t)(k2 & 63)) * 8u);
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int k = lane + 32 * (j & 1);
+        float2* row = wbuf + (j >> 1) * 128;
+        const float2 p0 = va[j];
         float2 a, c;
         if (k == 0) {
           a = float2{p0.x, 0.f};
           c = float2{p0.y, 0.f};
         } else {
           a = p0;
-          c = ld_cluster(xaddr(128 - k, yr));
+          c = vc[j];
         }
         {
           const float2 w = sm.wk[k];
@@ -601,7 +609,7 @@ __global__ void __launch_bounds__(YzInvT::kThreads, 1)
           row[k] = float2{sx - w.x * dy + w.y * dx, sy + w.x * dx + w.y * dy};
         }
         if (k == 0) {   // Z[64] from X[64] alone
-          const float2 x = ld_cluster(xaddr(64, yr));
+          const float2 x = vc[j];
           const float2 w = sm.wk[64];
           const float dy = 2.f * x.y;
           row[64] = float2{2.f * x.x - w.x * dy, w.y * dy};

@@ -5,8 +5,9 @@
 // two passes over the mesh each way (z, then y), these kernels make one.
 //
 // Layouts (as cuFFT's batched 2D transforms over (y, z) leave them): plane p = (channel, x) of
-// the real mesh at rho + p 256 256, of the half spectrum at spec + p 256 129 (ky rows of the
-// 129 kz values).
+// the real mesh at rho + p 256 256, of the half spectrum at spec + p 256 P (ky rows of the 129
+// kz values, P = 129; or P = 130 with a zero pad slot when the TMA x-pass shares the spectrum,
+// so that every row starts on a 16-byte boundary).
 //
 // Columns: kz = 1..127 are complex; kz = 0 and kz = 128 come out of the z transform real, so
 // they travel as one packed complex column X[y][0] + i X[y][128] (one y FFT gives both, split by
@@ -26,14 +27,15 @@
 //      or another's, st.shared::cluster);
 //   4. after a cluster barrier, each CTA runs the 256-point y FFTs of its columns in place
 //      (16 x 16 register DFTs, two passes) and writes them to the spectrum from registers.
-// Inverse: the mirror image (the y pass reads the spectrum from global memory, cluster barrier,
+// Inverse, always on pairs: the mirror image (each CTA's 64 columns of a plane arrive by one 2-D
+// TMA load when the rows are padded, by plain loads otherwise; inverse y FFTs; cluster barrier;
 // per row the half-complex-to-real packing Z[k] = (X[k] + X*[128-k]) + i W256^-k (X[k] - X*[128-k])
-// read across the cluster, an inverse 128-point FFT, the real row written from registers). Both are
-// unnormalised, as cuFFT.
+// read across the cluster, an inverse 128-point FFT, the real row written from registers). Both
+// are unnormalised, as cuFFT. Both prefetch the next plane into L2 while they work on this one.
 //
-// The forward kernel's mbarrier waits are bounded; a wait that runs out stops its loads and marks
-// the plane's spectrum NaN so the result cannot pass for a valid one (the inverse waits on
-// nothing but barriers). Every CTA of a cluster always takes the same barriers.
+// The mbarrier waits are bounded; a wait that runs out stops the kernel's loads and marks its
+// output NaN so the result cannot pass for a valid one. Every CTA of a cluster always takes the
+// same barriers.
 #include <cuda.h>
 
 #include "fd3_async.cuh"

@@ -631,39 +631,74 @@ int launch_cn_c6_cells(const CellGrid& g, int n, const CellList& cl, const doubl
 // strain virial W_ab = sum_i g_i sum_(j,S) f'(r) d_a d_b / r  (Bohr, Hartree). The force written
 // is out_scale * (mesh gradient already in grad + CN gradient). One warp per atom streams the
 // atom's recorded pairs; atoms without a record (n < 0) are left to k_cn_adjoint_global.
+// The kernel is bound by the latency of its dependent loads (count -> atom -> records -> g_j), so
+// a warp fetches the next atom's count and index while it works on this one, issues all of a
+// batch of 96 records' loads before the g_j loads that depend on them, and reads the atom's mesh
+// gradient at the start. Lane l still sums the records l, l + 32, ... in that order.
 template <typename TE>
-__global__ void __launch_bounds__(256) k_cn_adjoint_hits(int n, const int4* __restrict__ meta,
+__global__ void __launch_bounds__(256, 4) k_cn_adjoint_hits(int n, const int4* __restrict__ meta,
                                                         const double* __restrict__ gcn, double* __restrict__ grad,
                                                         double out_scale, double* __restrict__ vir_part,
                                                         HitList<TE> hl) {
+  using V4 = typename Vec4<TE>::type;
+  constexpr int kU = 3;   // records per lane per batch
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int stride = gridDim.x * kWarpsPerBlock;
   double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  int t = blockIdx.x * kWarpsPerBlock + wid;
+  int nh_next = t < n ? hl.n[t] : -1;
+  int i_next = t < n ? meta[t].w : 0;
   // grid-stride over atoms: the block's virial is reduced once, after all its atoms
-  for (int t = blockIdx.x * kWarpsPerBlock + wid; t < n; t += gridDim.x * kWarpsPerBlock) {
-    const int nh = hl.n[t];
+  for (; t < n; t += stride) {
+    const int nh = nh_next, i = i_next;
+    if (t + stride < n) {
+      nh_next = hl.n[t + stride];
+      i_next = meta[t + stride].w;
+    }
     if (nh >= 0) {
-      const int i = meta[t].w;
-      double f0 = 0, f1 = 0, f2 = 0;
       const double gi = gcn[i];
+      const double gq = lane < 3 ? grad[3 * i + lane] : 0.0;
+      double f0 = 0, f1 = 0, f2 = 0;
       const size_t hb = (size_t)t * hl.cap;
-      for (int e = lane; e < nh; e += 32) {
-        const typename Vec4<TE>::type r4 = hl.ad[hb + e];
-        const double a = (double)r4.x, v0 = (double)r4.y, v1 = (double)r4.z, v2 = (double)r4.w;
-        const double w = (gi + gcn[hl.j[hb + e]]) * a;
-        f0 -= w * v0;
-        f1 -= w * v1;
-        f2 -= w * v2;
-        const double bb = gi * a;
-        v[0] += bb * v0 * v0; v[1] += bb * v0 * v1; v[2] += bb * v0 * v2;
-        v[4] += bb * v1 * v1; v[5] += bb * v1 * v2; v[8] += bb * v2 * v2;
+      for (int e0 = 0; e0 < nh; e0 += 32 * kU) {
+        V4 r4[kU];
+        int jj[kU];
+        double gj[kU];
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          const int e = e0 + 32 * u + lane;
+          if (e < nh) {
+            r4[u] = hl.ad[hb + e];
+            jj[u] = hl.j[hb + e];
+          } else {
+            r4[u] = V4{0, 0, 0, 0};
+            jj[u] = -1;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < kU; ++u) gj[u] = jj[u] >= 0 ? gcn[jj[u]] : 0.0;
+#pragma unroll
+        for (int u = 0; u < kU; ++u) {
+          if (jj[u] < 0) continue;
+          const double a = (double)r4[u].x, v0 = (double)r4[u].y, v1 = (double)r4[u].z, v2 = (double)r4[u].w;
+          const double w = (gi + gj[u]) * a;
+          f0 -= w * v0;
+          f1 -= w * v1;
+          f2 -= w * v2;
+          const double bb = gi * a;
+          v[0] += bb * v0 * v0; v[1] += bb * v0 * v1; v[2] += bb * v0 * v2;
+          v[4] += bb * v1 * v1; v[5] += bb * v1 * v2; v[8] += bb * v2 * v2;
+        }
       }
       f0 = warp_sum(f0);
       f1 = warp_sum(f1);
       f2 = warp_sum(f2);
+      const double q0 = __shfl_sync(0xffffffffu, gq, 0), q1 = __shfl_sync(0xffffffffu, gq, 1),
+                   q2 = __shfl_sync(0xffffffffu, gq, 2);
       if (lane == 0) {
-        grad[3 * i] = out_scale * (grad[3 * i] + f0);
-        grad[3 * i + 1] = out_scale * (grad[3 * i + 1] + f1);
-        grad[3 * i + 2] = out_scale * (grad[3 * i + 2] + f2);
+        grad[3 * i] = out_scale * (q0 + f0);
+        grad[3 * i + 1] = out_scale * (q1 + f1);
+        grad[3 * i + 2] = out_scale * (q2 + f2);
       }
     }
   }

@@ -97,9 +97,9 @@ def gpu_local_cpus(dev_idx: int):
         return None
 
 
-def host_buffers_local(batch):
-    """batch.host_buffers(), allocated and first written by this thread bound to the GPU's
-    NUMA-local CPUs (so the pinned pages sit next to the GPU); returns (buffers, cpus or None)."""
+def on_local_cpus(fn):
+    """fn() run by this thread bound to the GPU's NUMA-local CPUs (so that pinned pages it
+    allocates and first writes sit next to the GPU); returns (fn's result, cpus or None)."""
     cpus = gpu_local_cpus(torch.cuda.current_device())
     old = os.sched_getaffinity(0) if hasattr(os, "sched_getaffinity") else None
     bound = False
@@ -110,13 +110,47 @@ def host_buffers_local(batch):
         except OSError:
             bound = False
     try:
-        h = batch.host_buffers()
-        h["out"].zero_()
-        h["positions"].copy_(batch.positions.cpu())
+        r = fn()
     finally:
         if bound:
             os.sched_setaffinity(0, old)
-    return h, (cpus & old if bound else None)
+    return r, (cpus & old if bound else None)
+
+
+def host_buffers_local(batch):
+    """batch.host_buffers() on the GPU's NUMA-local CPUs; returns (buffers, cpus or None)."""
+    def make():
+        h = batch.host_buffers()
+        h["out"].zero_()
+        h["positions"].copy_(batch.positions.cpu())
+        return h
+    return on_local_cpus(make)
+
+
+def time_pipeline(pipe, steps, warmup, ws, device):
+    """Milliseconds per evaluation of a two-slot host pipeline (HostPipeline): W untimed
+    submissions, then K bracketed by a barrier and a device synchronisation on both sides; the
+    events sit on the submitting stream, the first before the first host-to-device copy (the copy
+    streams are ordered after it) and the last after the last device-to-host copy."""
+    for k in range(warmup):
+        pipe.wait(k % 2)
+        pipe.submit(k % 2)
+    pipe.wait(0)
+    pipe.wait(1)
+    barrier(ws)
+    torch.cuda.synchronize(device)
+    a = torch.cuda.Event(enable_timing=True)
+    b = torch.cuda.Event(enable_timing=True)
+    a.record()
+    pipe.fence()
+    for k in range(steps):
+        pipe.wait(k % 2)
+        pipe.submit(k % 2)
+    pipe.join()
+    b.record()
+    torch.cuda.synchronize(device)
+    barrier(ws)
+    return a.elapsed_time(b) / steps
 
 
 def barrier(ws):
@@ -764,9 +798,21 @@ def main():
     def e2e_step():
         gb.run_host()
 
-    e2e_ms = None
+    # the same evaluations through the two-slot pipeline (HostPipeline): each evaluation still
+    # copies its positions in and its results out, on copy streams, beside the other's compute
+    def make_pipe():
+        pp = gb.host_pipeline()
+        for h in pp.host:
+            h["out"].zero_()
+            h["positions"].copy_(torch.tensor(pos, dtype=torch.float64))
+        return pp
+
+    e2e_ms = e2e_seq_ms = None
     if not args.no_e2e:
-        e2e_ms = max_over_ranks(time_steps(e2e_step, args.steps, args.warmup, ws, device), ws, device)
+        e2e_seq_ms = max_over_ranks(time_steps(e2e_step, args.steps, args.warmup, ws, device), ws, device)
+        pipe, _ = on_local_cpus(make_pipe)
+        assert pipe.h2d_bytes == h2d_bytes and pipe.d2h_bytes == d2h_bytes
+        e2e_ms = max_over_ranks(time_pipeline(pipe, args.steps, args.warmup, ws, device), ws, device)
 
     b = 4 if head == "mixed" else 8
     st_mixed = stages[head]
@@ -856,8 +902,13 @@ def main():
         "cpu_baseline": cpu,
         "e2e": ({"value": ws * n / (e2e_ms * 1e-3), "unit": "atoms/s", "ms_per_step": e2e_ms,
                  "h2d_bytes_per_step": h2d_bytes, "d2h_bytes_per_step": d2h_bytes,
-                 "path": "D3Batch.run_host: one graph replay that copies the pinned host positions in, "
-                         "evaluates, and copies energy, stress and forces out to pinned host memory",
+                 "path": "D3Batch.host_pipeline: every evaluation copies the pinned host positions in "
+                         "and energy, stress and forces out to pinned host memory, on copy streams, "
+                         "two evaluations in flight (K evaluations timed from the first copy in to "
+                         "the last copy out)",
+                 "sequential": {"value": ws * n / (e2e_seq_ms * 1e-3), "ms_per_step": e2e_seq_ms,
+                                "path": "D3Batch.run_host: one graph replay with both copies inside, "
+                                        "one evaluation at a time (median step)"},
                  "host_buffers": ("pinned on the GPU's NUMA node (allocated from a thread bound to the "
                                   f"{len(local_cpus)} CPUs NVML lists for the GPU)" if local_cpus
                                   else "pinned (NVML CPU affinity unavailable)")}

@@ -23,12 +23,18 @@ Layout on the device:
 over the lane streams), after which a call is a single graph replay. The cells are fixed
 for the life of a capture (they set the cell-list grid and the mesh).
 
+From host memory to host memory: ``run_host`` replays one graph with the copy of the
+positions in and of the results out inside it (one evaluation at a time);
+``host_pipeline()`` keeps two evaluations in flight, each slot with its own pinned and
+device buffers and graph, so the copies of one run on copy streams beside the other's compute.
+
 ``autotune_filter`` and ``autotune_spread`` time the filter k-tile and the spread z-chunk on
 the heaviest structures; ``autotune_lanes`` times candidate lane counts under graph replay and
 caches the winner in a JSON file keyed by the batch's shape signature.
 """
 from __future__ import annotations
 
+import gc
 import hashlib
 import json
 import os
@@ -100,6 +106,7 @@ class D3Batch:
         self._engines: dict = {}
         self._graph = None
         self._graph_host = None
+        self._pipe = None
         counts, cells, species, setups, keys, costs = [], [], [], [], [], []
         for pos, cell, numbers in structures:
             pos = np.asarray(pos, dtype=np.float64)
@@ -155,8 +162,7 @@ class D3Batch:
         lanes = max(1, min(int(lanes), self.n_struct))
         if lanes == self.lanes:
             return
-        self._graph = None
-        self._graph_host = None
+        self.drop_captures()
         self._work = None
         torch.cuda.synchronize(self.device)
         split = lpt_split(self.costs, lanes)
@@ -167,27 +173,40 @@ class D3Batch:
         self.workspace_bytes = int(sum(-(-s // _ALIGN) * _ALIGN for s in sizes))
         self._work = torch.empty(max(self.workspace_bytes, 1), dtype=torch.uint8, device=self.device)
         self._streams = [torch.cuda.Stream(self.device) for _ in range(lanes)]
-        self._lane_calls = []
+        self._lane_items = []
         base = 0
         for q, items in enumerate(split):
             wsl = self._work[base: base + sizes[q]]
             base += -(-sizes[q] // _ALIGN) * _ALIGN
-            calls = []
             # heaviest first inside a lane as well: the long mesh stages start early
-            for i in sorted(items, key=lambda k: (-self.costs[k], k)):
-                a, b = int(self.offsets[i]), int(self.offsets[i + 1])
-                calls.append((self._engines[self._keys[i]], self.positions[a:b], self.cells_host[i],
-                              self.cells[i], (self.energy[i], self.forces[a:b], self.stress[i]),
-                              self.species[a:b], wsl))
-            self._lane_calls.append(calls)
+            self._lane_items.append((sorted(items, key=lambda k: (-self.costs[k], k)), wsl))
+        self._lane_calls = self._make_lane_calls(self.positions, self._out)
+        self._pipe = None
         self.lanes = lanes
 
-    def _launch_all(self) -> None:
+    def _make_lane_calls(self, positions: torch.Tensor, out: torch.Tensor) -> list:
+        """Per lane, the engine calls of its structures reading ``positions`` (sum N, 3) and
+        writing the packed result buffer ``out`` [energy (B) | stress (B, 3, 3) | forces (sum N, 3)]."""
+        B = self.n_struct
+        energy, stress = out[:B], out[B:10 * B].view(B, 3, 3)
+        forces = out[10 * B:].view(-1, 3)
+        lane_calls = []
+        for items, wsl in self._lane_items:
+            calls = []
+            for i in items:
+                a, b = int(self.offsets[i]), int(self.offsets[i + 1])
+                calls.append((self._engines[self._keys[i]], positions[a:b], self.cells_host[i],
+                              self.cells[i], (energy[i], forces[a:b], stress[i]),
+                              self.species[a:b], wsl))
+            lane_calls.append(calls)
+        return lane_calls
+
+    def _launch_all(self, lane_calls: Optional[list] = None) -> None:
         main = torch.cuda.current_stream(self.device)
         fork = torch.cuda.Event()
         fork.record(main)
         joins = []
-        for st, calls in zip(self._streams, self._lane_calls):
+        for st, calls in zip(self._streams, self._lane_calls if lane_calls is None else lane_calls):
             st.wait_event(fork)
             with torch.cuda.stream(st):
                 for eng, pos, cell_h, cell_d, out, spc, wsl in calls:
@@ -208,37 +227,49 @@ class D3Batch:
         (``run_host``) is a whole evaluation from host memory to host memory."""
         if host_io:
             self.host_buffers()
+            g = self._record(None, copy_in=(self.positions, self._host["pos"]),
+                             copy_out=(self._host["out"], self._out))
+            self._graph_host = g
+        else:
+            self._graph = self._record(None)
+
+    def _record(self, lane_calls: Optional[list], copy_in=None, copy_out=None) -> torch.cuda.CUDAGraph:
+        """One CUDA graph of ``lane_calls`` (default: the batch's own buffers), optionally with a
+        copy (dst, src) before and after the launches."""
         side = torch.cuda.Stream(self.device)
         side.wait_stream(torch.cuda.current_stream(self.device))
         with torch.cuda.stream(side):
-            self._launch_all()  # warm-up outside the capture: cuFFT and module loading
+            self._launch_all(lane_calls)  # warm-up outside the capture: cuFFT and module loading
         torch.cuda.current_stream(self.device).wait_stream(side)
         torch.cuda.synchronize(self.device)
+        # a graph that dies in an unreachable cycle must not be freed by the cycle collector while
+        # this capture runs (destroying a graph during a capture invalidates the capture)
+        gc.collect()
         g = torch.cuda.CUDAGraph()
         with torch.cuda.graph(g):
-            if host_io:
-                self.positions.copy_(self._host["pos"], non_blocking=True)
-            self._launch_all()
-            if host_io:
-                self._host["out"].copy_(self._out, non_blocking=True)
+            if copy_in is not None:
+                copy_in[0].copy_(copy_in[1], non_blocking=True)
+            self._launch_all(lane_calls)
+            if copy_out is not None:
+                copy_out[0].copy_(copy_out[1], non_blocking=True)
         torch.cuda.synchronize(self.device)
-        if host_io:
-            self._graph_host = g
-        else:
-            self._graph = g
+        return g
 
     def host_buffers(self) -> dict:
         """Pinned host buffers for host-to-host evaluation: ``positions`` (sum N, 3) read by the
         host-I/O graph, and ``energy`` (B,), ``stress`` (B, 3, 3), ``forces`` (sum N, 3) that it
         writes (views of one pinned buffer)."""
         if self._host is None:
-            pos = torch.empty(tuple(self.positions.shape), dtype=torch.float64).pin_memory()
-            pos.copy_(self.positions.cpu())
-            out = torch.zeros(self._out.shape, dtype=torch.float64).pin_memory()
-            B, total = self.n_struct, int(self.positions.shape[0])
-            self._host = {"pos": pos, "out": out, "positions": pos, "energy": out[:B],
-                          "stress": out[B:10 * B].view(B, 3, 3), "forces": out[10 * B:].view(total, 3)}
+            self._host = self._pinned_io()
         return self._host
+
+    def _pinned_io(self) -> dict:
+        pos = torch.empty(tuple(self.positions.shape), dtype=torch.float64).pin_memory()
+        pos.copy_(self.positions.cpu())
+        out = torch.zeros(self._out.shape, dtype=torch.float64).pin_memory()
+        B, total = self.n_struct, int(self.positions.shape[0])
+        return {"pos": pos, "out": out, "positions": pos, "energy": out[:B],
+                "stress": out[B:10 * B].view(B, 3, 3), "forces": out[10 * B:].view(total, 3)}
 
     def run_host(self):
         """One evaluation from the pinned host positions to the pinned host results (a single
@@ -250,6 +281,18 @@ class D3Batch:
         self._graph_host.replay()
         h = self._host
         return h["energy"], h["forces"], h["stress"]
+
+    def host_pipeline(self) -> "HostPipeline":
+        """The batch's two-slot host-to-host pipeline (created on first use; see ``HostPipeline``)."""
+        if self._pipe is None:
+            self._pipe = HostPipeline(self)
+        return self._pipe
+
+    def drop_captures(self) -> None:
+        """Forget every captured graph (after a change of lanes or launch knobs)."""
+        self._graph = None
+        self._graph_host = None
+        self._pipe = None
 
     @property
     def captured(self) -> bool:
@@ -321,6 +364,86 @@ class D3Batch:
         return float(np.median(times))
 
 
+class HostPipeline:
+    """Host-to-host evaluations of a ``D3Batch`` with two in flight, so that the PCIe copies of
+    one evaluation overlap the compute of the other (the copy engines and the SMs work at once).
+
+    Slot s (0 or 1) owns pinned host buffers ``host[s]`` (``positions`` (sum N, 3) read;
+    ``energy`` (B,), ``stress`` (B, 3, 3), ``forces`` (sum N, 3) written), device copies of the
+    positions and of the packed results, and a CUDA graph of the whole batch on those device
+    buffers. Both graphs share the batch's workspace, so the evaluations themselves run one after
+    another on the submitting stream; only the copies run beside them, on two copy streams.
+
+    ``submit(s)`` enqueues the host-to-device copy of slot s's positions, the slot's graph and the
+    device-to-host copy of its results, and returns at once. ``wait(s)`` blocks until the results
+    of slot s's last submission are in host memory; after it the caller may read them and write
+    the slot's next positions. A stream of evaluations alternates the slots::
+
+        for k, positions in enumerate(stream):
+            s = k % 2
+            pipe.wait(s)             # results of evaluation k - 2 are now in pipe.host[s]
+            pipe.host[s]["positions"].copy_(positions)
+            pipe.submit(s)
+
+    Cells, species, lanes and launch knobs are the batch's; changing any of them drops the
+    pipeline with the batch's other captures.
+    """
+
+    def __init__(self, batch: D3Batch):
+        # no reference back to the batch: a batch <-> pipeline cycle would leave the graphs to
+        # the cycle collector, which may free them in the middle of a later capture
+        self.device = dev = batch.device
+        self.host = [batch._pinned_io() for _ in range(2)]
+        self.dev_pos = [batch.positions.clone() for _ in range(2)]
+        self.dev_out = [torch.zeros_like(batch._out) for _ in range(2)]
+        self.h2d_bytes = int(batch.positions.numel()) * 8
+        self.d2h_bytes = int(batch._out.numel()) * 8
+        self.graphs = [batch._record(batch._make_lane_calls(self.dev_pos[s], self.dev_out[s]))
+                       for s in range(2)]
+        self.h2d = torch.cuda.Stream(dev)
+        self.d2h = torch.cuda.Stream(dev)
+        self._in_done = [torch.cuda.Event() for _ in range(2)]
+        self._computed = [torch.cuda.Event() for _ in range(2)]
+        self._out_done = [torch.cuda.Event() for _ in range(2)]
+
+    def submit(self, s: int) -> None:
+        """Enqueue one evaluation of slot ``s`` from ``host[s]["positions"]`` to ``host[s]``'s results."""
+        main = torch.cuda.current_stream(self.device)
+        # the slot's device positions are rewritten only once its previous evaluation has read them
+        self.h2d.wait_event(self._computed[s])
+        with torch.cuda.stream(self.h2d):
+            self.dev_pos[s].copy_(self.host[s]["pos"], non_blocking=True)
+        self._in_done[s].record(self.h2d)
+        main.wait_event(self._in_done[s])
+        # ... and its device results only once the previous copy out of them has finished
+        main.wait_event(self._out_done[s])
+        self.graphs[s].replay()
+        self._computed[s].record(main)
+        self.d2h.wait_event(self._computed[s])
+        with torch.cuda.stream(self.d2h):
+            self.host[s]["out"].copy_(self.dev_out[s], non_blocking=True)
+        self._out_done[s].record(self.d2h)
+
+    def wait(self, s: int) -> dict:
+        """Block until slot ``s``'s last results are in host memory; returns ``host[s]``."""
+        self._out_done[s].synchronize()
+        return self.host[s]
+
+    def fence(self) -> None:
+        """Order both copy streams after the work enqueued so far on the current stream (for
+        instance a timing event recorded before the first ``submit``)."""
+        main = torch.cuda.current_stream(self.device)
+        self.h2d.wait_stream(main)
+        self.d2h.wait_stream(main)
+
+    def join(self) -> None:
+        """Order the current stream after every copy enqueued so far (for instance before a timing
+        event recorded after the last ``submit``)."""
+        main = torch.cuda.current_stream(self.device)
+        main.wait_stream(self.h2d)
+        main.wait_stream(self.d2h)
+
+
 def _profiled_stage(batch: "D3Batch", i: int, stage, reps: int = 2) -> float:
     """Milliseconds of one pipeline stage of structure ``i``, or the summed milliseconds of a
     tuple of stages (eager, profiled calls; the fastest of ``reps`` after one warm-up call)."""
@@ -349,8 +472,7 @@ def autotune_filter(batch: "D3Batch", candidates: Sequence = (0, 1, 2, 4, 8, 16,
     (profiled eager calls) and its best choice is set on every engine of that class where it
     is valid. Returns {class: (choice, {choice: ms})}. Drops a captured graph.
     """
-    batch._graph = None
-    batch._graph_host = None
+    batch.drop_captures()
     classes: dict = {}
     for i, key in enumerate(batch._keys):
         s = len(key[0])
@@ -388,8 +510,7 @@ def autotune_spread(batch: "D3Batch", candidates: Sequence[int] = (0, 2, 4, 8, 1
     """Pick the spread's z-chunk length (0 = per-tile kernel) from the heaviest structure of each
     plan: every candidate is timed (profiled eager calls) and the fastest is set on that plan.
     Returns {plan index: (chunk, {chunk: ms})}. Drops a captured graph."""
-    batch._graph = None
-    batch._graph_host = None
+    batch.drop_captures()
     heaviest: dict = {}
     for i, key in enumerate(batch._keys):
         if key not in heaviest or batch.costs[i] > batch.costs[heaviest[key]]:
@@ -420,8 +541,7 @@ def autotune_fft_x(batch: "D3Batch", pencils: Sequence[int] = (1, 2, 4), reps: i
     the (y, z) transforms as cluster kernels on pairs (the default), with the forward on quads
     ("<choice>/yz2") and by cuFFT ("<choice>/yz0"), and keeps the fastest. Returns
     {plan index: (choice, {choice: ms})}. Drops a captured graph."""
-    batch._graph = None
-    batch._graph_host = None
+    batch.drop_captures()
     heaviest: dict = {}
     for i, key in enumerate(batch._keys):
         if key not in heaviest or batch.costs[i] > batch.costs[heaviest[key]]:

@@ -7,7 +7,7 @@
   1e-8 eV/A, stress 1e-10 eV/A^3), so the batch path inherits the drop-in parity;
 * positions updated in place are picked up by a graph replay;
 * the host-I/O graph (run_host: positions copied in and results out inside one replay) equals
-  the device path bit for bit;
+  the device path bit for bit, and so does every evaluation of the two-slot host pipeline;
 * the lane autotuner picks one of its candidates and writes its cache.
 """
 import json
@@ -122,6 +122,50 @@ def test_run_host_matches_device_call(cuda_device):
     e3, _, _ = b(back)
     torch.cuda.synchronize()
     assert torch.equal(e3, e0)
+
+
+def test_host_pipeline_matches_device_calls(cuda_device):
+    """The two-slot host pipeline (copies of one evaluation beside the other's compute) gives,
+    for every evaluation of a stream of different positions, the device-path results bit for
+    bit, each in its own slot's host buffers."""
+    from fourierd3_b200.batch import D3Batch
+
+    structs = _structures(n=5)
+    b = D3Batch(structs, precision="mixed", lanes=2, device=cuda_device, **KW)
+    b.capture()
+    rng = np.random.default_rng(11)
+    base = np.concatenate([p for p, _, _ in structs])
+    stream = [base + rng.normal(0.0, 0.02, base.shape) for _ in range(5)]
+    expect = []
+    for p in stream:
+        e, f, s = b(torch.from_numpy(p))
+        expect.append((e.cpu(), f.cpu(), s.cpu()))
+    torch.cuda.synchronize()
+    pipe = b.host_pipeline()
+    assert pipe.host[0]["positions"].is_pinned() and pipe.host[1]["forces"].is_pinned()
+    got = [None] * len(stream)
+
+    def collect(k):
+        h = pipe.wait(k % 2)
+        got[k] = (h["energy"].clone(), h["forces"].clone(), h["stress"].clone())
+
+    for k, p in enumerate(stream):
+        s = k % 2
+        if k >= 2:
+            collect(k - 2)
+        else:
+            pipe.wait(s)
+        pipe.host[s]["positions"].copy_(torch.from_numpy(p))
+        pipe.submit(s)
+    collect(len(stream) - 2)
+    collect(len(stream) - 1)
+    for (e, f, s), (ed, fd, sd) in zip(got, expect):
+        assert torch.equal(e, ed) and torch.equal(f, fd) and torch.equal(s, sd)
+    assert not torch.equal(got[0][0], got[1][0])
+    # the batch's own graph still reads the batch's device positions
+    e3, _, _ = b(torch.from_numpy(stream[2]))
+    torch.cuda.synchronize()
+    assert torch.equal(e3.cpu(), expect[2][0])
 
 
 def test_autotune_lanes_caches(tmp_path, cuda_device):

@@ -490,7 +490,10 @@ struct HitList {
 // indices of the pairs inside are compacted in order into a per-warp ring of 64, and whenever 32
 // are waiting all lanes evaluate the CN function for them and write their records contiguously. The CN function and the record stores thus run on full warps
 // instead of on the ~15 % of lanes that hit in a given candidate batch.
+// A bin holds ~17 atoms at r_cut 6 A (SiO2 density): 4 warps per CTA leave fewer idle warps
+// waiting for a bin's last atom than 8 do, and more CTAs (bins) fit per SM.
 constexpr int kCnRing = 64;
+constexpr int kCnWarps = 4;
 
 template <typename TC> struct StagePos { using type = double4; };
 template <> struct StagePos<float> { using type = float4; };
@@ -516,13 +519,13 @@ __device__ __forceinline__ void cn_hit(const BinStage<typename StagePos<TC>::typ
 }
 
 template <typename TE, typename TC>
-__global__ void __launch_bounds__(256) k_cn_bins(GridDev g, const int* __restrict__ bin_start,
+__global__ void __launch_bounds__(32 * kCnWarps) k_cn_bins(GridDev g, const int* __restrict__ bin_start,
                                                 const double4* __restrict__ xs, const int4* __restrict__ meta,
                                                 const Tables* __restrict__ tab, double* __restrict__ cn,
                                                 HitList<TE> hl, int* __restrict__ ovf) {
   using P4 = typename StagePos<TC>::type;
   __shared__ BinStage<P4> st;
-  __shared__ int ring[kWarpsPerBlock][kCnRing];
+  __shared__ int ring[kCnWarps][kCnRing];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   const int b = blockIdx.x;
   double org[3];
@@ -537,7 +540,7 @@ __global__ void __launch_bounds__(256) k_cn_bins(GridDev g, const int* __restric
   const TC rc = (TC)tab->r_cut;
   const TC rc2 = (TC)g.rc2;
   int* rg = ring[wid];
-  for (int t = s0 + wid; t < s1; t += kWarpsPerBlock) {
+  for (int t = s0 + wid; t < s1; t += kCnWarps) {
     const double4 xi = xs[t];
     const int4 mi = meta[t];
     double wd0, wd1, wd2;
@@ -609,11 +612,11 @@ int launch_cn_c6_cells(const CellGrid& g, int n, const CellList& cl, const doubl
   const int K = g.nb[0] * g.nb[1] * g.nb[2];
   FD3_CUDA(cudaMemsetAsync(hs.ovf, 0, sizeof(int), s));
   if (hs.is_double)
-    k_cn_bins<double, double><<<K, 32 * kWarpsPerBlock, 0, s>>>(
+    k_cn_bins<double, double><<<K, 32 * kCnWarps, 0, s>>>(
         to_dev(g), cl.bin_start, cl.xs, cl.meta, tab, cn,
         HitList<double>{hs.j, (double4*)hs.ad, hs.n, hs.cap}, hs.ovf);
   else
-    k_cn_bins<float, float><<<K, 32 * kWarpsPerBlock, 0, s>>>(
+    k_cn_bins<float, float><<<K, 32 * kCnWarps, 0, s>>>(
         to_dev(g), cl.bin_start, cl.xs, cl.meta, tab, cn,
         HitList<float>{hs.j, (float4*)hs.ad, hs.n, hs.cap}, hs.ovf);
   FD3_LAUNCHED();

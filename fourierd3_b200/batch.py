@@ -408,6 +408,8 @@ class HostPipeline:
 
     def submit(self, s: int) -> None:
         """Enqueue one evaluation of slot ``s`` from ``host[s]["positions"]`` to ``host[s]``'s results."""
+        if s not in (0, 1):
+            raise ValueError("slot must be 0 or 1")
         main = torch.cuda.current_stream(self.device)
         # the slot's device positions are rewritten only once its previous evaluation has read them
         self.h2d.wait_event(self._computed[s])
@@ -426,6 +428,8 @@ class HostPipeline:
 
     def wait(self, s: int) -> dict:
         """Block until slot ``s``'s last results are in host memory; returns ``host[s]``."""
+        if s not in (0, 1):
+            raise ValueError("slot must be 0 or 1")
         self._out_done[s].synchronize()
         return self.host[s]
 

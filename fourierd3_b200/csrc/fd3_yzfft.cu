@@ -460,7 +460,7 @@ __global__ void __launch_bounds__(YzCfg<CL>::kThreads, YzCfg<CL>::kMinBlocks)
       float2* dst = reinterpret_cast<float2*>(rho + ((size_t)plane * kYzN + ybase + r2) * kYzN);
 #pragma unroll
       for (int k2 = 0; k2 < 16; ++k2) dst[k1 + 8 * k2] = float2{re[k2], im[k2]};
-      __syncwarp();   // the row buffers are rewritten in the next round
+      __syncwarp();   // the row buffers are rewritten in the next iteration
     }
     cluster_sync_exec();   // every CTA has read the cluster's columns: the next plane may load
   }

@@ -490,7 +490,7 @@ struct HitList {
 // indices of the pairs inside are compacted in order into a per-warp ring of 64, and whenever 32
 // are waiting all lanes evaluate the CN function for them and write their records contiguously. The CN function and the record stores thus run on full warps
 // instead of on the ~15 % of lanes that hit in a given candidate batch.
-// A bin holds ~17 atoms at r_cut 6 A (SiO2 density): 4 warps per CTA leave fewer idle warps
+// A bin holds ~15 atoms at r_cut 6 A (SiO2 density): 4 warps per CTA leave fewer idle warps
 // waiting for a bin's last atom than 8 do, and more CTAs (bins) fit per SM.
 constexpr int kCnRing = 64;
 constexpr int kCnWarps = 4;

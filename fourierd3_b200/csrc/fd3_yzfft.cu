@@ -674,6 +674,7 @@ int launch_yz(const void* kern, int which, int threads, size_t smem, void** args
     set_error(what, "launch of the (y, z) transform failed");
     return FD3_ECUDA;
   }
+  count_launch();
   return FD3_OK;
 }
 

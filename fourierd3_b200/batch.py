@@ -393,6 +393,9 @@ class HostPipeline:
         # no reference back to the batch: a batch <-> pipeline cycle would leave the graphs to
         # the cycle collector, which may free them in the middle of a later capture
         self.device = dev = batch.device
+        # ... but the memory its graphs read stays alive with the pipeline: the workspace, the
+        # species and cells, and the plans (none of them refers to the batch)
+        self._keep = (batch._work, batch.species, batch.cells, dict(batch._engines))
         self.host = [batch._pinned_io() for _ in range(2)]
         self.dev_pos = [batch.positions.clone() for _ in range(2)]
         self.dev_out = [torch.zeros_like(batch._out) for _ in range(2)]

@@ -75,3 +75,40 @@ def test_two_rank_shards_cover_the_batch():
         assert p.exitcode == 0
     assert sorted(got[0] + got[1]) == list(range(40))
     assert not set(got[0]) & set(got[1])
+
+
+def test_lpt_split_more_parts_than_items_and_ties():
+    from fourierd3_b200.batch import lpt_split
+
+    bins = lpt_split([3.0, 1.0], 4)
+    assert bins == [[0], [1], [], []]
+    # equal costs: heaviest-first order breaks ties by index, bins by their own index
+    assert lpt_split([1.0, 1.0, 1.0, 1.0], 2) == [[0, 2], [1, 3]]
+
+
+def test_shard_covers_the_batch_and_checks_the_rank():
+    import pytest
+
+    from fourierd3_b200 import structures as st
+    from fourierd3_b200.batch import shard
+
+    structs = [st.random_box(k, 24 + 8 * k, z_max=18) for k in range(7)]
+    for world in (1, 2, 3):
+        parts = [shard(structs, r, world) for r in range(world)]
+        assert sorted(i for p in parts for i in p) == list(range(len(structs)))
+        assert all(p == sorted(p) for p in parts)
+    for bad in (-1, 3):
+        with pytest.raises(ValueError):
+            shard(structs, bad, 3)
+
+
+def test_batch_refuses_empty_input_and_non_cuda_devices():
+    import pytest
+
+    from fourierd3_b200 import structures as st
+    from fourierd3_b200.batch import D3Batch
+
+    with pytest.raises(ValueError):
+        D3Batch([])
+    with pytest.raises(RuntimeError):
+        D3Batch([st.random_box(0, 24, z_max=18)], device="cpu")
